@@ -1,0 +1,97 @@
+"""Shared test helpers: load the golden fixtures and rebuild the same device
+for the oracle (CPU) or for the GPU product from the stored definition."""
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    with np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False) as f:
+        return {k: f[k] for k in f.files}
+
+
+def coords(g):
+    return (g["x"], g["y"]) if int(g["dim"]) == 2 else (g["x"], g["y"], g["z"])
+
+
+def bcs(g):
+    """[(name, kind, flat node idx, vals)] in the fixture's insertion order."""
+    out = []
+    ptr = g["bc_ptr"]
+    for b, name in enumerate(g["bc_names"]):
+        out.append((str(name), str(g["bc_kinds"][b]),
+                    g["bc_idx"][ptr[b]:ptr[b + 1]], g["bc_vals"][b]))
+    return out
+
+
+def unflat(g, k):
+    nx, ny = g["x"].size, g["y"].size
+    i = k % nx
+    j = (k // nx) % ny
+    if int(g["dim"]) == 2:
+        return (i, j)
+    return (i, j, k // (nx * ny))
+
+
+def oracle_device(g, material=None):
+    from oracle import OracleDevice, OracleModels, SILICON_PARAMS
+    m = g["models"]
+    mat = dict(SILICON_PARAMS)
+    if material:
+        mat.update(material)
+    dev = OracleDevice(coords(g), g["doping"], Ntotal=g["Ntot"], T=float(g["T"]),
+                       models=OracleModels(*[bool(v) for v in m]), material=mat)
+    for name, kind, k, v in bcs(g):
+        ijk = unflat(g, k)
+        if kind == "contact":
+            dev.add_contact(name, *ijk, V=v[0])
+        else:
+            dev.gates[name] = None
+            _add_gate_kappa(dev, name, ijk, v)
+    return dev
+
+
+def _add_gate_kappa(dev, name, ijk, v):
+    """Gate from the stored kappa (the reference stores kappa, not t_ox)."""
+    kappa, Vfb, Vg, ax = v
+    idx = [np.asarray(a, dtype=np.int64) for a in ijk]
+    dv = dev.dv
+    if dev.dim == 2:
+        w = dv[0][idx[0]]
+    else:
+        axis = "xyz"[int(ax)]
+        if axis == "z":
+            w = dv[0][idx[0]] * dv[1][idx[1]]
+        elif axis == "y":
+            w = dv[0][idx[0]] * dv[2][idx[2]]
+        else:
+            w = dv[1][idx[1]] * dv[2][idx[2]]
+    dev.gates[name] = [dev.flat(*ijk), float(kappa), float(Vfb), float(Vg), w]
+
+
+def csr(g, prefix=""):
+    import scipy.sparse as sp
+    n = g[prefix + "J_indptr"].size - 1
+    return sp.csr_matrix((g[prefix + "J_data"], g[prefix + "J_indices"],
+                          g[prefix + "J_indptr"]), shape=(n, n))
+
+
+def rownorm_err(A, B):
+    """max over rows of ||A_r - B_r||_1 / ||B_r||_1 (normwise per row)."""
+    D = (A - B).tocsr()
+    Bc = B.tocsr()
+    num = np.asarray(abs(D).sum(axis=1)).ravel()
+    den = np.asarray(abs(Bc).sum(axis=1)).ravel()
+    den = np.where(den == 0, 1.0, den)
+    return float((num / den).max())
+
+
+def vec_err(a, b, scale=None):
+    """max |a-b| / max(|b|, scale) -- scale guards entries that cancel."""
+    a = np.asarray(a, dtype=float)
+    b = np.asarray(b, dtype=float)
+    s = np.abs(b) if scale is None else np.maximum(np.abs(b), scale)
+    s = np.where(s == 0, 1.0, s)
+    return float((np.abs(a - b) / s).max())
