@@ -1,0 +1,243 @@
+/*
+ * tcad_b200 -- C ABI of the sm_100a drift-diffusion solve path.
+ *
+ * Every entry point takes plain device pointers and sizes, launches on the
+ * given CUDA stream and returns a status code (TCAD_OK or a TCAD_ERR_*
+ * value); nothing throws across this boundary.  A host binding maps the
+ * codes onto the reference's error classes the way the reference's own
+ * binding does (core/bindings/module.cpp:100-127): TCAD_ERR_ARG -> ValueError,
+ * TCAD_ERR_SINGULAR / _NONFINITE / _NOCONV / _BREAKDOWN -> LinearSolveError
+ * (pytcad/linsolve.py:344), TCAD_ERR_CUDA -> RuntimeError.
+ *
+ * Data model ("pack"): one or more devices (instances) of one dimension are
+ * packed back to back.  Node arrays are structure-of-arrays of length
+ * n_nodes, node k of instance i sitting at node_off[i] + k with
+ * k = (kz*Ny + j)*Nx + i_x (x fastest), the reference's flat order
+ * (pytcad/mesh2d.py:1-7, pytcad/mesh3d.py:1-10).  Edge coefficients live at
+ * the edge's low ("owner") node.  Vectors of the coupled system are
+ * component-major: [psi(n_nodes) | n(n_nodes) | p(n_nodes)].
+ *
+ * Coupled Jacobian ("node-block" layout), TCAD_NE2 = 29 (2D) or
+ * TCAD_NE3 = 39 (3D) doubles per node, entry-major (J[e*n_nodes + k]):
+ *   e = 0..8            diagonal 3x3 block, row-major (row, col) over (psi,n,p)
+ *   e = 9 + 5*d + m     neighbour d = W,E,S,N,D,U (-x,+x,-y,+y,-z,+z);
+ *                       m = (psi<-psi), (n<-psi), (n<-n), (p<-psi), (p<-p)
+ * which is exactly the structural pattern of the reference's COO stamps
+ * (pytcad/device2d.py:1534-1621, core/src/device3d/kernels.cpp:40-168).
+ * Equilibrium Poisson Jacobian: 1 + 2*dim doubles per node (diag, then the
+ * neighbours in the same W,E,S,N,D,U order).
+ */
+#ifndef TCAD_B200_H
+#define TCAD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCAD_OK 0
+#define TCAD_ERR_ARG 1
+#define TCAD_ERR_SINGULAR 2
+#define TCAD_ERR_NONFINITE 3
+#define TCAD_ERR_NOCONV 4
+#define TCAD_ERR_CUDA 5
+#define TCAD_ERR_BREAKDOWN 6
+
+#define TCAD_NE2 29
+#define TCAD_NE3 39
+#define TCAD_FLAT_NODES 1024 /* nodes per flat (vector-kernel) block */
+#define TCAD_TILE_X 32       /* stencil tile: 32 x 8 nodes (x, y) */
+#define TCAD_TILE_Y 8
+#define TCAD_TILE_Z 16       /* z planes marched by one 3D stencil tile */
+
+/* per-instance scalar parameters: par[i*TCAD_NPAR + TCAD_P_*] */
+#define TCAD_NPAR 8
+#define TCAD_P_NS 0    /* reference concentration Ns [cm^-3] */
+#define TCAD_P_R0 1    /* recombination scale D0 Ns / LD^2 */
+#define TCAD_P_CN 2    /* Auger Cn [cm^6/s] */
+#define TCAD_P_CP 3    /* Auger Cp [cm^6/s] */
+#define TCAD_P_SRH 4   /* 1.0: recombination on (Models.srh) */
+#define TCAD_P_AUGER 5 /* 1.0: Auger on (Models.auger) */
+
+/* assembly modes */
+#define TCAD_MODE_RAW 0        /* reference _residual_jacobian rows, BC rows stamped */
+#define TCAD_MODE_ELIMINATE 1  /* + symmetric Dirichlet elimination (pytcad/dirichlet.py:270) */
+
+/* bcflag bits */
+#define TCAD_BC_CONTACT 1
+#define TCAD_BC_GATE 2
+
+typedef struct tcad_pack {
+  int32_t dim;           /* 2 or 3 */
+  int32_t n_inst;        /* packed instances */
+  int64_t n_nodes;       /* total nodes */
+  int64_t n_flat;        /* flat blocks (TCAD_FLAT_NODES nodes, never straddling instances) */
+  int64_t n_tiles;       /* stencil tiles */
+  /* per-instance tables (device memory) */
+  const int32_t* shape;    /* [3*n_inst] Nx, Ny, Nz (Nz = 1 in 2D) */
+  const int64_t* node_off; /* [n_inst+1] */
+  const int64_t* flat_off; /* [n_inst+1] first flat block of each instance */
+  const int32_t* flat_inst;/* [n_flat] instance of each flat block */
+  const int64_t* axis_off; /* [3*n_inst] start of the instance's x/y/z entries in h[]/dv[] */
+  const int32_t* tile;     /* [4*n_tiles] inst, i0, j0, k0 */
+  const double* par;       /* [TCAD_NPAR*n_inst] */
+  /* packed axis geometry, scaled by LD; h has the same count as dv (last unused) */
+  const double* h[3];
+  const double* dv[3];
+  /* node data (device memory, n_nodes each) */
+  const double* C;       /* net doping / Ns */
+  const double* nie;     /* effective intrinsic density [cm^-3] */
+  const double* nie_s;   /* nie / Ns */
+  const double* tau_n;   /* SRH lifetimes [s] */
+  const double* tau_p;
+  const double* an[3];   /* electron edge coefficient D_edge/h at the edge's low node */
+  const double* ap[3];   /* hole edge coefficient */
+  const double* dl[3];   /* ln(nie_s[high]/nie_s[low]) */
+  const uint8_t* bcflag; /* TCAD_BC_* bits */
+  const double* bc_psi0; /* contact targets at the current bias (read where CONTACT) */
+  const double* bc_n0;
+  const double* bc_p0;
+  const double* bc_psi0_eq; /* contact psi target of the zero-bias equilibrium */
+  const double* gate_k;  /* kappa*w summed over the node's gates (read where GATE) */
+  const double* gate_v;  /* Vg/VT - Vfb/VT */
+  const double* gate_veq;/* 0 - Vfb/VT (equilibrium: gate at zero bias) */
+  const double* gate_b;  /* local neutral-bulk potential psi_b */
+} tcad_pack_t;
+
+/* ABI guard: sizeof(tcad_pack_t) as compiled into the library. */
+size_t tcad_pack_sizeof(void);
+/* "tcad_b200 <version> sm_100a" */
+const char* tcad_version(void);
+
+/* ---- assembly ------------------------------------------------------------
+ * Coupled SG residual/Jacobian at (psi, n, p) [scaled, n_nodes each].
+ * Replaces Device2D._residual_jacobian (pytcad/device2d.py:1402-1920) and
+ * Device3D._residual_jacobian with its compiled stamps (pytcad/device3d.py:
+ * 1485-1978, core/src/device3d/kernels.cpp:40-168).  F is [3][n_nodes],
+ * J is [NE][n_nodes].  RAW: contact rows become (x - x0) with unit blocks;
+ * ELIMINATE: in addition the contact columns are folded into F, so that
+ * -F is the eliminated right-hand side of pytcad/dirichlet.py:270-300. */
+int tcad_sg_assemble(const tcad_pack_t* pk, const double* psi, const double* n,
+                     const double* p, double* F, double* J, int mode, void* stream);
+
+/* Raw continuity residual F_n + F_p at a node list (before the contact rows
+ * are stamped) -- the terminal-current kernel of Device2D/3D.terminal_current
+ * (pytcad/device2d.py:2194-2227, pytcad/device3d.py:2274-2306).  Writes the
+ * deterministic sum over the list to out_sum[0]. */
+int tcad_contact_current(const tcad_pack_t* pk, const double* psi, const double* n,
+                         const double* p, const int64_t* nodes, int64_t count,
+                         double* partial, int64_t partial_len, double* out_sum,
+                         void* stream);
+/* (partial must hold 2*count doubles: F_n of the listed nodes, then F_p.) */
+
+/* Edge current densities Jn, Jp of one axis at their low nodes (scaled;
+ * Device2D/3D.Jn_x.. attributes, pytcad/device2d.py:2188-2190). */
+int tcad_edge_currents(const tcad_pack_t* pk, int axis, const double* psi,
+                       const double* n, const double* p, double* Jn, double* Jp,
+                       void* stream);
+
+/* Equilibrium Poisson residual/Jacobian with slaved Boltzmann densities,
+ * Device2D._residual_jacobian_poisson (pytcad/device2d.py:844-942) and
+ * Device3D's (pytcad/device3d.py:952-1020, core/src/device3d/poisson_eq.cpp:
+ * 5-129).  F [n_nodes], J [(1+2*dim)][n_nodes]. */
+int tcad_poisson_assemble(const tcad_pack_t* pk, const double* psi, double* F,
+                          double* J, int mode, void* stream);
+
+/* ---- boundary conditions -------------------------------------------------
+ * Contact targets at the current bias (contacts.ohmic_values,
+ * pytcad/contacts.py:21-38, with psi0 = V/VT + ln(n0/nie)): for each listed
+ * contact node t, contact id cid[t] with vv[cid] = V/VT:
+ *   bc_psi0[node] = vv[cid[t]] + L[t],  bc_n0[node] = n0[t],  bc_p0[node] = p0[t]. */
+int tcad_set_contacts(const tcad_pack_t* pk, const int64_t* nodes, int64_t count,
+                      const int32_t* cid, const double* vv, const double* L,
+                      const double* n0, const double* p0, double* bc_psi0,
+                      double* bc_n0, double* bc_p0, void* stream);
+
+/* Warm start at a new bias (pytcad/device2d.py:1949-1953): psi, n, p of the
+ * listed contact nodes take their targets. */
+int tcad_stamp_contacts(const tcad_pack_t* pk, const int64_t* nodes, int64_t count,
+                        double* psi, double* n, double* p, void* stream);
+
+/* ---- linear algebra on the node-block layout ---------------------------
+ * Workspace size in bytes for tcad_block_krylov / tcad_newton_solve. */
+size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart);
+
+/* Node-block-Jacobi set-up (pytcad/linsolve.py:363-427): inverts every
+ * diagonal 3x3 block of J in place and replaces F by the block-scaled
+ * right-hand side b^ = D^-1 (-F).  status[inst] gets TCAD_ERR_SINGULAR for a
+ * block with |det| < 1e-300 or a non-finite entry. */
+int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
+                            int32_t* status, void* stream);
+
+/* y = A^ x with A^ = I + D^-1 (off-diagonal blocks), J prepared by
+ * tcad_block_jacobi_setup; x, y are [3][n_nodes]. */
+int tcad_block_spmv(const tcad_pack_t* pk, const double* J, const double* x,
+                    double* y, void* stream);
+
+/* Krylov solve of A^ x = b^ for every instance of the pack (BiCGStab:
+ * method 0, GMRES(restart): method 1), x starting at zero, per-instance
+ * convergence ||b^ - A^ x|| <= rtol ||b^||.  iters/status/relres are
+ * per-instance host arrays.  Replaces the gmres/bicgstab + block-Jacobi
+ * branch of linsolve.solve_linear (pytcad/linsolve.py:941-985). */
+int tcad_block_krylov(const tcad_pack_t* pk, const double* J, const double* b,
+                      double* x, int method, double rtol, int maxiter, int restart,
+                      void* work, size_t work_bytes, int32_t* iters,
+                      int32_t* status, double* relres, void* stream);
+
+/* ---- Newton --------------------------------------------------------------
+ * Damped update of the coupled Newton loop (pytcad/device2d.py:2079-2160):
+ * clip dpsi to +-max_dpsi, n/p to [0.1x, 10x], err = max(|dpsi|,
+ * |dn|/max(n,floor), |dp|/max(p,floor)) per instance into err[inst]. */
+int tcad_newton_update(const tcad_pack_t* pk, double* psi, double* n, double* p,
+                       const double* du, double max_dpsi, double dens_floor,
+                       const uint8_t* active, double* partial, double* err,
+                       void* stream);
+
+/* Options of one Newton solve (the NewtonOptions of pytcad/device.py:539-627). */
+typedef struct tcad_newton_opts {
+  int32_t max_iter;      /* 100 */
+  int32_t method;        /* 0 BiCGStab, 1 GMRES */
+  int32_t krylov_maxiter;
+  int32_t restart;
+  double tol_update;     /* 1e-8 */
+  double max_dpsi;       /* 5 */
+  double rtol;           /* Krylov relative tolerance (1e-10) */
+  double dens_floor;     /* 1e-10 */
+  int32_t verbose;
+  int32_t pad;
+} tcad_newton_opts_t;
+
+/* Per-instance result of a Newton solve (host memory). */
+typedef struct tcad_newton_result {
+  int32_t iters;         /* Newton iterations taken */
+  int32_t converged;     /* 1 when err < tol_update with a converged linear solve */
+  int32_t krylov_iters;  /* total Krylov iterations */
+  int32_t status;        /* last linear-solve status */
+  double err;            /* last update norm */
+  double relres;         /* last scaled linear residual */
+} tcad_newton_result_t;
+
+/* Full coupled Newton solve at the contact targets stored in the pack
+ * (Device2D/3D.solve_bias inner loop, pytcad/device2d.py:2020-2160,
+ * pytcad/device3d.py:2091-2239) for every instance whose active[inst] is
+ * non-zero.  psi/n/p are updated in place.  J, F are assembly buffers
+ * ([NE][n], [3][n]); du is [3][n]; work is tcad_block_workspace_bytes. */
+int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, double* p,
+                      double* F, double* J, double* du, const tcad_newton_opts_t* opts,
+                      uint8_t* active, void* work, size_t work_bytes,
+                      tcad_newton_result_t* result, void* stream);
+
+/* Equilibrium Poisson Newton solve (Device2D/3D.solve_equilibrium,
+ * pytcad/device2d.py:1308-1373, pytcad/device3d.py:1311-1454) from the psi
+ * given; on return n, p hold the slaved densities. */
+int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double* n, double* p,
+                           double* F, double* J, double* d, const tcad_newton_opts_t* opts,
+                           void* work, size_t work_bytes, tcad_newton_result_t* result,
+                           void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TCAD_B200_H */

@@ -1,0 +1,537 @@
+// Fused SG residual/Jacobian assembly (coupled psi/n/p) and the equilibrium
+// Poisson assembly, written straight into the fixed node-block layout of
+// include/tcad_b200.h.  Built with -fmad=false (see sg_edge.cuh).
+//
+// One CTA owns a 32 x 8 tile of nodes (x fastest, so a warp is one row of 32
+// consecutive nodes and every node-array access is a coalesced 256-byte
+// line).  The tile's plane values plus a one-node halo are staged in shared
+// memory; every x- and y-edge touching the tile is evaluated ONCE (Bernoulli
+// functions included) into shared memory and read by both endpoint nodes.
+// In 3D the CTA marches up to TCAD_TILE_Z planes in z, carrying the z-edge
+// between consecutive planes in registers (the up-edge of plane k is the
+// down-edge of plane k+1), so z-edges are also evaluated once.
+#include "sg_edge.cuh"
+
+namespace tcad {
+
+constexpr int TX = TCAD_TILE_X, TY = TCAD_TILE_Y;
+
+struct NodeVals {
+  double psi, n, p;
+};
+
+// Neighbour-block entry offsets: 9 + 5*d + m.
+__device__ __forceinline__ int nb(int d, int m) { return 9 + 5 * d + m; }
+
+template <int DIM>
+__global__ void __launch_bounds__(kTileThreads)
+k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
+              const double* __restrict__ nn, const double* __restrict__ pp,
+              double* __restrict__ F, double* __restrict__ J, int mode) {
+  constexpr int NE = DIM == 2 ? TCAD_NE2 : TCAD_NE3;
+  __shared__ double s_psi[TY + 2][TX + 2], s_n[TY + 2][TX + 2], s_p[TY + 2][TX + 2];
+  __shared__ uint8_t s_flag[TY + 2][TX + 2];
+  __shared__ Edge s_ex[TY][TX + 1];  // x-edge slot a: nodes (i0-1+a, i0+a)
+  __shared__ Edge s_ey[TY + 1][TX];  // y-edge slot b: nodes (j0-1+b, j0+b)
+
+  const int64_t t = blockIdx.x;
+  const int inst = pk.tile[4 * t + 0], i0 = pk.tile[4 * t + 1];
+  const int j0 = pk.tile[4 * t + 2], k0 = pk.tile[4 * t + 3];
+  const Inst g = load_inst(pk, inst);
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i < g.nx) && (j < g.ny);
+  const int64_t ax0 = pk.axis_off[3 * inst], ay0 = pk.axis_off[3 * inst + 1];
+  const int64_t az0 = pk.axis_off[3 * inst + 2];
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  const int64_t NN = pk.n_nodes;
+  const double* par = pk.par + TCAD_NPAR * inst;
+  const int kend = DIM == 3 ? min(k0 + TCAD_TILE_Z, g.nz) : 1;
+
+  // z-march registers (3D): own node values of the current / next plane
+  NodeVals cur{0.0, 0.0, 0.0}, nxt{0.0, 0.0, 0.0};
+  Edge eD, eU;
+  zero_edge(eD);
+  zero_edge(eU);
+  if (own) {
+    const int64_t q = g.off + (int64_t)k0 * sxy + (int64_t)j * g.nx + i;
+    cur = NodeVals{psi[q], nn[q], pp[q]};
+  }
+  if (DIM == 3 && own && k0 > 0) {  // down-edge into the first plane
+    const int64_t q = g.off + (int64_t)k0 * sxy + (int64_t)j * g.nx + i;
+    const int64_t ql = q - sxy;
+    sg_edge(psi[ql], cur.psi, nn[ql], cur.n, pp[ql], cur.p, pk.an[2][ql], pk.ap[2][ql],
+            pk.dl[2][ql], pk.h[2][az0 + k0 - 1], eD);
+  }
+
+  for (int kz = k0; kz < kend; ++kz) {
+    const int64_t plane = g.off + (int64_t)kz * sxy;
+    // ---- stage the plane (tile + 1-node halo, no corners) in shared memory
+    s_psi[ty + 1][tx + 1] = cur.psi;
+    s_n[ty + 1][tx + 1] = cur.n;
+    s_p[ty + 1][tx + 1] = cur.p;
+    s_flag[ty + 1][tx + 1] = own ? pk.bcflag[plane + (int64_t)j * g.nx + i] : 0;
+    if (tid < 2 * TY + 2 * TX) {
+      int r, c, hi, hj;
+      if (tid < 2 * TY) {  // x halo: columns 0 and TX+1
+        r = 1 + (tid >> 1);
+        c = (tid & 1) ? TX + 1 : 0;
+      } else {             // y halo: rows 0 and TY+1
+        const int u = tid - 2 * TY;
+        c = 1 + (u >> 1);
+        r = (u & 1) ? TY + 1 : 0;
+      }
+      hi = i0 - 1 + c;
+      hj = j0 - 1 + r;
+      double a = 0.0, b = 0.0, d = 0.0;
+      uint8_t f = 0;
+      if (hi >= 0 && hi < g.nx && hj >= 0 && hj < g.ny) {
+        const int64_t q = plane + (int64_t)hj * g.nx + hi;
+        a = psi[q]; b = nn[q]; d = pp[q]; f = pk.bcflag[q];
+      }
+      s_psi[r][c] = a; s_n[r][c] = b; s_p[r][c] = d; s_flag[r][c] = f;
+    }
+    if (DIM == 3 && own && kz + 1 < g.nz) {
+      const int64_t q = plane + sxy + (int64_t)j * g.nx + i;
+      nxt = NodeVals{psi[q], nn[q], pp[q]};
+    }
+    __syncthreads();
+
+    // ---- evaluate every edge touching the tile once
+    auto xedge = [&](int row, int a) {
+      const int ilo = i0 - 1 + a, jj = j0 + row;
+      Edge e;
+      if (ilo >= 0 && ilo + 1 < g.nx && jj < g.ny) {
+        const int64_t q = plane + (int64_t)jj * g.nx + ilo;
+        sg_edge(s_psi[row + 1][a], s_psi[row + 1][a + 1], s_n[row + 1][a],
+                s_n[row + 1][a + 1], s_p[row + 1][a], s_p[row + 1][a + 1], pk.an[0][q],
+                pk.ap[0][q], pk.dl[0][q], pk.h[0][ax0 + ilo], e);
+      } else {
+        zero_edge(e);
+      }
+      s_ex[row][a] = e;
+    };
+    auto yedge = [&](int col, int b) {
+      const int jlo = j0 - 1 + b, ii = i0 + col;
+      Edge e;
+      if (jlo >= 0 && jlo + 1 < g.ny && ii < g.nx) {
+        const int64_t q = plane + (int64_t)jlo * g.nx + ii;
+        sg_edge(s_psi[b][col + 1], s_psi[b + 1][col + 1], s_n[b][col + 1],
+                s_n[b + 1][col + 1], s_p[b][col + 1], s_p[b + 1][col + 1], pk.an[1][q],
+                pk.ap[1][q], pk.dl[1][q], pk.h[1][ay0 + jlo], e);
+      } else {
+        zero_edge(e);
+      }
+      s_ey[b][col] = e;
+    };
+    xedge(ty, tx + 1);  // own E edge
+    yedge(tx, ty + 1);  // own N edge
+    if (tid < TY) xedge(tid, 0);                        // tile's west halo edges
+    else if (tid < TY + TX) yedge(tid - TY, 0);         // tile's south halo edges
+    if (DIM == 3) {
+      if (own && kz + 1 < g.nz) {
+        const int64_t q = plane + (int64_t)j * g.nx + i;
+        sg_edge(cur.psi, nxt.psi, cur.n, nxt.n, cur.p, nxt.p, pk.an[2][q], pk.ap[2][q],
+                pk.dl[2][q], pk.h[2][az0 + kz], eU);
+      } else {
+        zero_edge(eU);
+      }
+    }
+    __syncthreads();
+
+    // ---- assemble the own node's row block
+    if (own) {
+      const int64_t k = plane + (int64_t)j * g.nx + i;
+      const uint8_t flag = s_flag[ty + 1][tx + 1];
+      double Fv[3];
+      double Jv[NE];
+#pragma unroll
+      for (int e = 0; e < NE; ++e) Jv[e] = 0.0;
+      if (flag & TCAD_BC_CONTACT) {
+        Fv[0] = cur.psi - pk.bc_psi0[k];
+        Fv[1] = cur.n - pk.bc_n0[k];
+        Fv[2] = cur.p - pk.bc_p0[k];
+        Jv[0] = 1.0; Jv[4] = 1.0; Jv[8] = 1.0;
+      } else {
+        const double dvx = pk.dv[0][ax0 + i], dvy = pk.dv[1][ay0 + j];
+        const double dvz = DIM == 3 ? pk.dv[2][az0 + kz] : 1.0;
+        const double fx = DIM == 2 ? dvy : dvy * dvz;   // x-edge face
+        const double fy = DIM == 2 ? dvx : dvx * dvz;   // y-edge face
+        const double fz = dvx * dvy;                    // z-edge face
+        const double dV = DIM == 2 ? dvy * dvx : (dvz * dvy) * dvx;
+        const bool vW = i >= 1, vE = i + 1 < g.nx, vS = j >= 1, vN = j + 1 < g.ny;
+        const bool vD = DIM == 3 && kz >= 1, vU = DIM == 3 && kz + 1 < g.nz;
+        const Edge& W = s_ex[ty][tx];
+        const Edge& E = s_ex[ty][tx + 1];
+        const Edge& S = s_ey[ty][tx];
+        const Edge& N = s_ey[ty + 1][tx];
+        // divergences: div[lo] += f; div[hi] -= f  (device2d.py:1512-1525)
+        double dx0 = 0.0, dx1 = 0.0, dx2 = 0.0, dy0 = 0.0, dy1 = 0.0, dy2 = 0.0;
+        double dz0 = 0.0, dz1 = 0.0, dz2 = 0.0;
+        if (vE) { dx0 = dx0 + E.f; dx1 = dx1 + E.Jn; dx2 = dx2 + E.Jp; }
+        if (vW) { dx0 = dx0 - W.f; dx1 = dx1 - W.Jn; dx2 = dx2 - W.Jp; }
+        if (vN) { dy0 = dy0 + N.f; dy1 = dy1 + N.Jn; dy2 = dy2 + N.Jp; }
+        if (vS) { dy0 = dy0 - S.f; dy1 = dy1 - S.Jn; dy2 = dy2 - S.Jp; }
+        if (vU) { dz0 = dz0 + eU.f; dz1 = dz1 + eU.Jn; dz2 = dz2 + eU.Jp; }
+        if (vD) { dz0 = dz0 - eD.f; dz1 = dz1 - eD.Jn; dz2 = dz2 - eD.Jp; }
+        double Rs, dRsn, dRsp;
+        recomb(cur.n, cur.p, pk.nie[k], pk.tau_n[k], pk.tau_p[k], par, Rs, dRsn, dRsp);
+        double f0 = fx * dx0 + fy * dy0;
+        double f1 = fx * dx1 + fy * dy1;
+        double f2 = fx * dx2 + fy * dy2;
+        if (DIM == 3) { f0 = f0 + fz * dz0; f1 = f1 + fz * dz1; f2 = f2 + fz * dz2; }
+        Fv[0] = f0 - dV * (cur.n - cur.p - pk.C[k]);
+        Fv[1] = f1 - Rs * dV;
+        Fv[2] = f2 + Rs * dV;
+        // diagonal block, summed in the reference's stamp order per axis
+        // (low-role edge first, then high-role edge)
+        double d00 = 0.0, d10 = 0.0, d11 = 0.0, d20 = 0.0, d22 = 0.0;
+        auto lo_role = [&](const Edge& e, double face, double h) {  // node = low end
+          d00 = d00 + (-(face / h));
+          d10 = d10 + (-(face * e.npsi));
+          d11 = d11 + face * e.nlo;
+          d20 = d20 + (-(face * e.ppsi));
+          d22 = d22 + face * e.plo;
+        };
+        auto hi_role = [&](const Edge& e, double face, double h) {  // node = high end
+          d00 = d00 + (-(face / h));
+          d10 = d10 + (-(face * e.npsi));
+          d11 = d11 + (-face) * e.nhi;
+          d20 = d20 + (-(face * e.ppsi));
+          d22 = d22 + (-face) * e.phi;
+        };
+        // Poisson row entries come first in the COO (x then y then z), the
+        // continuity rows interleave psi/n stamps per axis; each diagonal
+        // entry only collects one kind, so per-entry order is axis by axis.
+        if (vE) lo_role(E, fx, pk.h[0][ax0 + i]);
+        if (vW) hi_role(W, fx, pk.h[0][ax0 + i - 1]);
+        if (vN) lo_role(N, fy, pk.h[1][ay0 + j]);
+        if (vS) hi_role(S, fy, pk.h[1][ay0 + j - 1]);
+        if (vU) lo_role(eU, fz, pk.h[2][az0 + kz]);
+        if (vD) hi_role(eD, fz, pk.h[2][az0 + kz - 1]);
+        d11 = d11 + (-dRsn) * dV;
+        d22 = d22 + dRsp * dV;
+        Jv[0] = d00; Jv[1] = -dV; Jv[2] = dV;
+        Jv[3] = d10; Jv[4] = d11; Jv[5] = (-dRsp) * dV;
+        Jv[6] = d20; Jv[7] = dRsn * dV; Jv[8] = d22;
+        // off-diagonal blocks
+        auto put_lo = [&](int d, const Edge& e, double face, double h) {  // nbr = high end
+          Jv[nb(d, 0)] = face / h;
+          Jv[nb(d, 1)] = face * e.npsi;
+          Jv[nb(d, 2)] = face * e.nhi;
+          Jv[nb(d, 3)] = face * e.ppsi;
+          Jv[nb(d, 4)] = face * e.phi;
+        };
+        auto put_hi = [&](int d, const Edge& e, double face, double h) {  // nbr = low end
+          Jv[nb(d, 0)] = face / h;
+          Jv[nb(d, 1)] = face * e.npsi;
+          Jv[nb(d, 2)] = (-face) * e.nlo;
+          Jv[nb(d, 3)] = face * e.ppsi;
+          Jv[nb(d, 4)] = (-face) * e.plo;
+        };
+        if (vW) put_hi(0, W, fx, pk.h[0][ax0 + i - 1]);
+        if (vE) put_lo(1, E, fx, pk.h[0][ax0 + i]);
+        if (vS) put_hi(2, S, fy, pk.h[1][ay0 + j - 1]);
+        if (vN) put_lo(3, N, fy, pk.h[1][ay0 + j]);
+        if (DIM == 3) {
+          if (vD) put_hi(4, eD, fz, pk.h[2][az0 + kz - 1]);
+          if (vU) put_lo(5, eU, fz, pk.h[2][az0 + kz]);
+        }
+        if (flag & TCAD_BC_GATE) {  // oxide Robin term (device2d.py:1624-1637)
+          const double gk = pk.gate_k[k];
+          Fv[0] = Fv[0] + gk * (pk.gate_v[k] - (cur.psi - pk.gate_b[k]));
+          Jv[0] = Jv[0] + (-gk);
+        }
+        if (mode == TCAD_MODE_ELIMINATE) {
+          // fold contact neighbours' known updates into F, empty the column
+          auto fold = [&](int d, bool valid, uint8_t nflag, int64_t m) {
+            if (!valid || !(nflag & TCAD_BC_CONTACT)) return;
+            const double g0 = psi[m] - pk.bc_psi0[m];
+            const double g1 = nn[m] - pk.bc_n0[m];
+            const double g2 = pp[m] - pk.bc_p0[m];
+            Fv[0] = Fv[0] - Jv[nb(d, 0)] * g0;
+            Fv[1] = Fv[1] - (Jv[nb(d, 1)] * g0 + Jv[nb(d, 2)] * g1);
+            Fv[2] = Fv[2] - (Jv[nb(d, 3)] * g0 + Jv[nb(d, 4)] * g2);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) Jv[nb(d, q)] = 0.0;
+          };
+          fold(0, vW, s_flag[ty + 1][tx], k - 1);
+          fold(1, vE, s_flag[ty + 1][tx + 2], k + 1);
+          fold(2, vS, s_flag[ty][tx + 1], k - g.nx);
+          fold(3, vN, s_flag[ty + 2][tx + 1], k + g.nx);
+          if (DIM == 3) {
+            fold(4, vD, vD ? pk.bcflag[k - sxy] : 0, k - sxy);
+            fold(5, vU, vU ? pk.bcflag[k + sxy] : 0, k + sxy);
+          }
+        }
+      }
+      F[k] = Fv[0];
+      F[NN + k] = Fv[1];
+      F[2 * NN + k] = Fv[2];
+#pragma unroll
+      for (int e = 0; e < NE; ++e) J[(int64_t)e * NN + k] = Jv[e];
+    }
+    __syncthreads();
+    if (DIM == 3) {
+      cur = nxt;
+      eD = eU;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// raw continuity residual F_n + F_p at listed nodes (terminal currents)
+template <int DIM>
+__global__ void k_contact_current(const tcad_pack_t pk, const double* __restrict__ psi,
+                                  const double* __restrict__ nn,
+                                  const double* __restrict__ pp,
+                                  const int64_t* __restrict__ nodes, int64_t count,
+                                  double* __restrict__ out) {
+  // out[t] = raw F_n, out[count + t] = raw F_p of node nodes[t]
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const int64_t k = nodes[t];
+  // locate the instance by a binary search on node_off
+  int lo = 0, hi = pk.n_inst;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pk.node_off[mid] <= k) lo = mid; else hi = mid;
+  }
+  const Inst g = load_inst(pk, lo);
+  const int64_t loc = k - g.off;
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  const int i = (int)(loc % g.nx), j = (int)((loc / g.nx) % g.ny);
+  const int kz = DIM == 3 ? (int)(loc / sxy) : 0;
+  const int64_t ax0 = pk.axis_off[3 * lo], ay0 = pk.axis_off[3 * lo + 1];
+  const int64_t az0 = pk.axis_off[3 * lo + 2];
+  const double* par = pk.par + TCAD_NPAR * lo;
+  const double dvx = pk.dv[0][ax0 + i], dvy = pk.dv[1][ay0 + j];
+  const double dvz = DIM == 3 ? pk.dv[2][az0 + kz] : 1.0;
+  const double face[3] = {DIM == 2 ? dvy : dvy * dvz, DIM == 2 ? dvx : dvx * dvz, dvx * dvy};
+  const double dV = DIM == 2 ? dvy * dvx : (dvz * dvy) * dvx;
+  const int coord[3] = {i, j, kz};
+  const int extent[3] = {g.nx, g.ny, g.nz};
+  const int64_t stride[3] = {1, g.nx, sxy};
+  const int64_t aoff[3] = {ax0, ay0, az0};
+  double tn = 0.0, tp = 0.0;
+  for (int a = 0; a < DIM; ++a) {
+    double dn = 0.0, dp = 0.0;
+    if (coord[a] + 1 < extent[a]) {  // edge to the high neighbour (node = low end)
+      const int64_t m = k + stride[a];
+      Edge e;
+      sg_edge(psi[k], psi[m], nn[k], nn[m], pp[k], pp[m], pk.an[a][k], pk.ap[a][k],
+              pk.dl[a][k], pk.h[a][aoff[a] + coord[a]], e);
+      dn = dn + e.Jn; dp = dp + e.Jp;
+    }
+    if (coord[a] >= 1) {             // edge from the low neighbour (node = high end)
+      const int64_t m = k - stride[a];
+      Edge e;
+      sg_edge(psi[m], psi[k], nn[m], nn[k], pp[m], pp[k], pk.an[a][m], pk.ap[a][m],
+              pk.dl[a][m], pk.h[a][aoff[a] + coord[a] - 1], e);
+      dn = dn - e.Jn; dp = dp - e.Jp;
+    }
+    tn = a == 0 ? face[a] * dn : tn + face[a] * dn;
+    tp = a == 0 ? face[a] * dp : tp + face[a] * dp;
+  }
+  double Rs, dRsn, dRsp;
+  recomb(nn[k], pp[k], pk.nie[k], pk.tau_n[k], pk.tau_p[k], par, Rs, dRsn, dRsp);
+  out[t] = tn - Rs * dV;
+  out[count + t] = tp + Rs * dV;
+}
+
+// fixed-order sum of vals[0..count) by one block
+__global__ void k_sum_list(const double* __restrict__ vals, int64_t count,
+                           double* __restrict__ out) {
+  __shared__ double sm[32];
+  double s = 0.0;
+  for (int64_t q = threadIdx.x; q < count; q += blockDim.x) s += vals[q] + vals[count + q];
+  const double r = block_sum<256>(s, sm);
+  if (threadIdx.x == 0) out[0] = r;
+}
+
+template <int DIM>
+__global__ void k_edge_currents(const tcad_pack_t pk, int axis,
+                                const double* __restrict__ psi,
+                                const double* __restrict__ nn,
+                                const double* __restrict__ pp, double* __restrict__ Jn,
+                                double* __restrict__ Jp) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const Inst g = load_inst(pk, fb.inst);
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  const int64_t stride = axis == 0 ? 1 : (axis == 1 ? g.nx : sxy);
+  const int extent = axis == 0 ? g.nx : (axis == 1 ? g.ny : g.nz);
+  const int64_t aoff = pk.axis_off[3 * fb.inst + axis];
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += blockDim.x) {
+    const int64_t loc = k - fb.ioff;
+    const int c = axis == 0 ? (int)(loc % g.nx)
+                            : (axis == 1 ? (int)((loc / g.nx) % g.ny) : (int)(loc / sxy));
+    double a = 0.0, b = 0.0;
+    if (c + 1 < extent) {
+      const int64_t m = k + stride;
+      Edge e;
+      sg_edge(psi[k], psi[m], nn[k], nn[m], pp[k], pp[m], pk.an[axis][k], pk.ap[axis][k],
+              pk.dl[axis][k], pk.h[axis][aoff + c], e);
+      a = e.Jn; b = e.Jp;
+    }
+    Jn[k] = a;
+    Jp[k] = b;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// equilibrium Poisson (slaved Boltzmann densities), node-centric
+template <int DIM>
+__global__ void __launch_bounds__(kFlatThreads)
+k_poisson_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
+                   double* __restrict__ F, double* __restrict__ J, int mode) {
+  constexpr int NP = 1 + 2 * DIM;
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const Inst g = load_inst(pk, fb.inst);
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  const int64_t ax0 = pk.axis_off[3 * fb.inst], ay0 = pk.axis_off[3 * fb.inst + 1];
+  const int64_t az0 = pk.axis_off[3 * fb.inst + 2];
+  const int64_t NN = pk.n_nodes;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += blockDim.x) {
+    const int64_t loc = k - fb.ioff;
+    const int i = (int)(loc % g.nx), j = (int)((loc / g.nx) % g.ny);
+    const int kz = DIM == 3 ? (int)(loc / sxy) : 0;
+    const uint8_t flag = pk.bcflag[k];
+    double Fv;
+    double Jv[NP];
+#pragma unroll
+    for (int e = 0; e < NP; ++e) Jv[e] = 0.0;
+    const double ps = psi[k];
+    if (flag & TCAD_BC_CONTACT) {
+      Fv = ps - pk.bc_psi0_eq[k];
+      Jv[0] = 1.0;
+    } else {
+      const double ns = pk.nie_s[k] * exp(clip700(ps));
+      const double ps_ = pk.nie_s[k] * exp(clip700(-ps));
+      const double dnp = ns + ps_;
+      const double dvx = pk.dv[0][ax0 + i], dvy = pk.dv[1][ay0 + j];
+      const double dvz = DIM == 3 ? pk.dv[2][az0 + kz] : 1.0;
+      const double face[3] = {DIM == 2 ? dvy : dvy * dvz, DIM == 2 ? dvx : dvx * dvz,
+                              dvx * dvy};
+      const double dV = DIM == 2 ? dvy * dvx : (dvz * dvy) * dvx;
+      const int coord[3] = {i, j, kz};
+      const int extent[3] = {g.nx, g.ny, g.nz};
+      const int64_t stride[3] = {1, g.nx, sxy};
+      const int64_t aoff[3] = {ax0, ay0, az0};
+      double Ft = 0.0, dg = 0.0;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        double dv = 0.0;
+        const bool hiv = coord[a] + 1 < extent[a], lov = coord[a] >= 1;
+        if (hiv) {
+          const double h = pk.h[a][aoff[a] + coord[a]];
+          dv = dv + (psi[k + stride[a]] - ps) / h;
+          const double w = face[a] / h;
+          dg = dg + (-w);
+          Jv[2 + 2 * a] = w;
+        }
+        if (lov) {
+          const double h = pk.h[a][aoff[a] + coord[a] - 1];
+          dv = dv - (ps - psi[k - stride[a]]) / h;
+          const double w = face[a] / h;
+          dg = dg + (-w);
+          Jv[1 + 2 * a] = w;
+        }
+        Ft = a == 0 ? face[a] * dv : Ft + face[a] * dv;
+      }
+      Fv = Ft - dV * (ns - ps_ - pk.C[k]);
+      dg = dg + (-dV) * dnp;
+      if (flag & TCAD_BC_GATE) {
+        const double gk = pk.gate_k[k];
+        Fv = Fv + gk * (pk.gate_veq[k] - (ps - pk.gate_b[k]));
+        dg = dg + (-gk);
+      }
+      Jv[0] = dg;
+      if (mode == TCAD_MODE_ELIMINATE) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          if (coord[a] >= 1) {
+            const int64_t m = k - stride[a];
+            if (pk.bcflag[m] & TCAD_BC_CONTACT) {
+              Fv = Fv - Jv[1 + 2 * a] * (psi[m] - pk.bc_psi0_eq[m]);
+              Jv[1 + 2 * a] = 0.0;
+            }
+          }
+          if (coord[a] + 1 < extent[a]) {
+            const int64_t m = k + stride[a];
+            if (pk.bcflag[m] & TCAD_BC_CONTACT) {
+              Fv = Fv - Jv[2 + 2 * a] * (psi[m] - pk.bc_psi0_eq[m]);
+              Jv[2 + 2 * a] = 0.0;
+            }
+          }
+        }
+      }
+    }
+    F[k] = Fv;
+#pragma unroll
+    for (int e = 0; e < NP; ++e) J[(int64_t)e * NN + k] = Jv[e];
+  }
+}
+
+}  // namespace tcad
+
+using namespace tcad;
+
+extern "C" int tcad_sg_assemble(const tcad_pack_t* pk, const double* psi, const double* n,
+                                const double* p, double* F, double* J, int mode,
+                                void* stream) {
+  if (!pk || (pk->dim != 2 && pk->dim != 3) || pk->n_tiles <= 0) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned nt = (unsigned)pk->n_tiles;
+  if (pk->dim == 2)
+    k_sg_assemble<2><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode);
+  else
+    k_sg_assemble<3><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode);
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_contact_current(const tcad_pack_t* pk, const double* psi,
+                                    const double* n, const double* p,
+                                    const int64_t* nodes, int64_t count, double* partial,
+                                    int64_t partial_len, double* out_sum, void* stream) {
+  if (!pk || count < 0 || partial_len < 2 * count) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (count > 0) {
+    const unsigned nb_ = (unsigned)((count + 255) / 256);
+    if (pk->dim == 2)
+      k_contact_current<2><<<nb_, 256, 0, s>>>(*pk, psi, n, p, nodes, count, partial);
+    else
+      k_contact_current<3><<<nb_, 256, 0, s>>>(*pk, psi, n, p, nodes, count, partial);
+    TCAD_LAUNCH_CHECK();
+  }
+  k_sum_list<<<1, 256, 0, s>>>(partial, count, out_sum);
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_edge_currents(const tcad_pack_t* pk, int axis, const double* psi,
+                                  const double* n, const double* p, double* Jn,
+                                  double* Jp, void* stream) {
+  if (!pk || axis < 0 || axis >= pk->dim) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned nb_ = (unsigned)pk->n_flat;
+  if (pk->dim == 2)
+    k_edge_currents<2><<<nb_, kFlatThreads, 0, s>>>(*pk, axis, psi, n, p, Jn, Jp);
+  else
+    k_edge_currents<3><<<nb_, kFlatThreads, 0, s>>>(*pk, axis, psi, n, p, Jn, Jp);
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_poisson_assemble(const tcad_pack_t* pk, const double* psi, double* F,
+                                     double* J, int mode, void* stream) {
+  if (!pk || (pk->dim != 2 && pk->dim != 3)) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned nb_ = (unsigned)pk->n_flat;
+  if (pk->dim == 2)
+    k_poisson_assemble<2><<<nb_, kFlatThreads, 0, s>>>(*pk, psi, F, J, mode);
+  else
+    k_poisson_assemble<3><<<nb_, kFlatThreads, 0, s>>>(*pk, psi, F, J, mode);
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}

@@ -1,0 +1,95 @@
+// Shared device helpers of the tcad_b200 kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/tcad_b200.h"
+
+#define TCAD_CUDA_CHECK(expr)                        \
+  do {                                               \
+    cudaError_t e_ = (expr);                         \
+    if (e_ != cudaSuccess) return TCAD_ERR_CUDA;     \
+  } while (0)
+
+#define TCAD_LAUNCH_CHECK() TCAD_CUDA_CHECK(cudaGetLastError())
+
+namespace tcad {
+
+constexpr int kFlatThreads = 256;
+constexpr int kFlatPerThread = TCAD_FLAT_NODES / kFlatThreads;  // 4
+constexpr int kTileThreads = TCAD_TILE_X * TCAD_TILE_Y;           // 256
+
+// Geometry of one instance as seen by a kernel.
+struct Inst {
+  int nx, ny, nz;
+  int64_t off;  // first node
+  int64_t n;    // node count
+};
+
+__device__ __forceinline__ Inst load_inst(const tcad_pack_t& pk, int inst) {
+  Inst g;
+  g.nx = pk.shape[3 * inst + 0];
+  g.ny = pk.shape[3 * inst + 1];
+  g.nz = pk.shape[3 * inst + 2];
+  g.off = pk.node_off[inst];
+  g.n = pk.node_off[inst + 1] - g.off;
+  return g;
+}
+
+// Deterministic block reduction (fixed tree order) of one double per thread.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* smem) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) smem[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (warp == 0) {
+    r = lane < NT / 32 ? smem[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* smem) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) smem[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (warp == 0) {
+    r = lane < NT / 32 ? smem[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+  }
+  __syncthreads();
+  return r;
+}
+
+// Flat-block addressing: block b of the pack covers TCAD_FLAT_NODES nodes of
+// exactly one instance.  Returns the instance, the first node of the block
+// and the instance's end node.
+struct FlatBlock {
+  int inst;
+  int64_t begin, end;  // packed node range [begin, end) handled by this block
+  int64_t ioff, iend;  // instance node range
+};
+
+__device__ __forceinline__ FlatBlock flat_block(const tcad_pack_t& pk, int64_t b) {
+  FlatBlock fb;
+  fb.inst = pk.flat_inst[b];
+  fb.ioff = pk.node_off[fb.inst];
+  fb.iend = pk.node_off[fb.inst + 1];
+  const int64_t local = b - pk.flat_off[fb.inst];
+  fb.begin = fb.ioff + local * TCAD_FLAT_NODES;
+  fb.end = fb.begin + TCAD_FLAT_NODES < fb.iend ? fb.begin + TCAD_FLAT_NODES : fb.iend;
+  return fb;
+}
+
+}  // namespace tcad

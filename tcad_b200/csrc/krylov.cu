@@ -1,0 +1,935 @@
+// Node-block linear algebra, Krylov solvers and the Newton drivers.
+//
+// All kernels are "flat": block b owns TCAD_FLAT_NODES consecutive nodes of
+// one instance (flat_block()).  Reductions are per instance and
+// deterministic: each block writes its partial sums, and the LAST block of
+// the instance to finish (atomic ticket) sums the partials in block order and
+// updates the instance's scalar state (alpha, omega, ...).  The host only
+// looks at the per-instance state every few iterations, so the iteration
+// itself runs without host round trips; blocks of finished instances return
+// immediately, which is the per-instance convergence mask of a packed batch.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace tcad {
+
+constexpr int NT = kFlatThreads;
+
+// Per-instance Krylov state (device memory, mirrored to the host).
+struct KState {
+  double rho, rho_prev, alpha, omega, beta;
+  double rr, bb, tol2, r0n2, rv, ss;
+  int32_t it, maxit, status, active, restart, early, pad0, pad1;
+};
+
+template <int DIM>
+struct Stencil {
+  static constexpr int NE = DIM == 2 ? TCAD_NE2 : TCAD_NE3;
+  static constexpr int ND = 2 * DIM;
+};
+
+__device__ __forceinline__ int64_t clampi(int64_t m, int64_t lo, int64_t hi) {
+  return m < lo ? lo : (m >= hi ? hi - 1 : m);
+}
+
+__device__ __forceinline__ void nbr_offsets(const Inst& g, int64_t* off) {
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  off[0] = -1; off[1] = 1; off[2] = -(int64_t)g.nx; off[3] = g.nx;
+  off[4] = -sxy; off[5] = sxy;
+}
+
+// --------------------------------------------------------------------------
+// partial sums -> per-instance totals (last block finalizes)
+template <int NS>
+struct Reduce {
+  // returns true in every thread of the block that must finalize
+  __device__ static bool run(const tcad_pack_t& pk, int64_t b, int inst, double (&v)[NS],
+                             double* partial, unsigned* ticket, double* tot) {
+    __shared__ double sm[32];
+    __shared__ double st[NS];
+    __shared__ int last;
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      const double r = block_sum<NT>(v[q], sm);
+      if (threadIdx.x == 0) st[q] = r;
+    }
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int q = 0; q < NS; ++q) partial[b * 4 + q] = st[q];
+      __threadfence();
+      const int64_t nb = pk.flat_off[inst + 1] - pk.flat_off[inst];
+      const unsigned prev = atomicAdd(&ticket[inst], 1u);
+      last = (prev == (unsigned)(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    const int64_t b0 = pk.flat_off[inst], b1 = pk.flat_off[inst + 1];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      double s = 0.0;
+      for (int64_t bb = b0 + threadIdx.x; bb < b1; bb += NT) s += __ldcg(&partial[bb * 4 + q]);
+      const double r = block_sum<NT>(s, sm);
+      if (threadIdx.x == 0) tot[q] = r;
+    }
+    if (threadIdx.x == 0) ticket[inst] = 0u;
+    return true;
+  }
+};
+
+// --------------------------------------------------------------------------
+// block-Jacobi set-up: invert the 3x3 diagonal blocks, scale the rhs
+__global__ void __launch_bounds__(NT)
+k_bj_setup(const tcad_pack_t pk, double* __restrict__ J, double* __restrict__ F,
+           int32_t* __restrict__ status) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const int64_t NN = pk.n_nodes;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    double a[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) a[e] = J[(int64_t)e * NN + k];
+    const double c00 = a[4] * a[8] - a[5] * a[7];
+    const double c01 = a[5] * a[6] - a[3] * a[8];
+    const double c02 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    bool ok = isfinite(det) && fabs(det) >= 1e-300;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) ok = ok && isfinite(a[e]);
+    double inv[9];
+    if (ok) {
+      const double id = 1.0 / det;
+      inv[0] = c00 * id;
+      inv[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+      inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+      inv[3] = c01 * id;
+      inv[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+      inv[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+      inv[6] = c02 * id;
+      inv[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+      inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    } else {
+      atomicExch(&status[fb.inst], TCAD_ERR_SINGULAR);
+#pragma unroll
+      for (int e = 0; e < 9; ++e) inv[e] = (e % 4 == 0) ? 1.0 : 0.0;
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) J[(int64_t)e * NN + k] = inv[e];
+    const double r0 = -F[k], r1 = -F[NN + k], r2 = -F[2 * NN + k];
+    if (!(isfinite(r0) && isfinite(r1) && isfinite(r2)))
+      atomicExch(&status[fb.inst], TCAD_ERR_NONFINITE);
+    F[k] = inv[0] * r0 + inv[1] * r1 + inv[2] * r2;
+    F[NN + k] = inv[3] * r0 + inv[4] * r1 + inv[5] * r2;
+    F[2 * NN + k] = inv[6] * r0 + inv[7] * r1 + inv[8] * r2;
+  }
+}
+
+// y = x + Dinv * (sum_d A_d x_nbr(d))      (SCALED)
+// y = D x + sum_d A_d x_nbr(d)             (raw J, !SCALED)
+template <int DIM, bool SCALED>
+__device__ __forceinline__ void spmv_node(const double* __restrict__ J,
+                                          const double* __restrict__ x, int64_t k,
+                                          int64_t NN, const int64_t* off, int64_t lo,
+                                          int64_t hi, double& y0, double& y1, double& y2) {
+  double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < 2 * DIM; ++d) {
+    const int64_t m = clampi(k + off[d], lo, hi);
+    const int e = 9 + 5 * d;
+    const double xs = x[m], xn = x[NN + m], xp = x[2 * NN + m];
+    t0 += J[(int64_t)e * NN + k] * xs;
+    t1 += J[(int64_t)(e + 1) * NN + k] * xs + J[(int64_t)(e + 2) * NN + k] * xn;
+    t2 += J[(int64_t)(e + 3) * NN + k] * xs + J[(int64_t)(e + 4) * NN + k] * xp;
+  }
+  const double x0 = x[k], x1 = x[NN + k], x2 = x[2 * NN + k];
+  double d[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) d[e] = J[(int64_t)e * NN + k];
+  if (SCALED) {
+    y0 = x0 + (d[0] * t0 + d[1] * t1 + d[2] * t2);
+    y1 = x1 + (d[3] * t0 + d[4] * t1 + d[5] * t2);
+    y2 = x2 + (d[6] * t0 + d[7] * t1 + d[8] * t2);
+  } else {
+    y0 = d[0] * x0 + d[1] * x1 + d[2] * x2 + t0;
+    y1 = d[3] * x0 + d[4] * x1 + d[5] * x2 + t1;
+    y2 = d[6] * x0 + d[7] * x1 + d[8] * x2 + t2;
+  }
+}
+
+template <int DIM, bool SCALED>
+__global__ void __launch_bounds__(NT)
+k_spmv(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ x,
+       double* __restrict__ y) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const Inst g = load_inst(pk, fb.inst);
+  int64_t off[6];
+  nbr_offsets(g, off);
+  const int64_t NN = pk.n_nodes;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    double y0, y1, y2;
+    spmv_node<DIM, SCALED>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    y[k] = y0; y[NN + k] = y1; y[2 * NN + k] = y2;
+  }
+}
+
+// --------------------------------------------------------------------------
+// BiCGStab on A^ (per instance).  Vectors: r, rh (shadow), p, v, s, t; x.
+struct BiVec {
+  double *r, *rh, *p, *v, *s, *t;
+};
+
+__global__ void __launch_bounds__(NT)
+k_bi_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict__ x,
+          BiVec w, KState* ks, double* partial, unsigned* ticket, double rtol, int maxit,
+          const int32_t* __restrict__ pre_status) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const int64_t NN = pk.n_nodes;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t q = c * NN + k;
+      const double bv = b[q];
+      x[q] = 0.0; w.r[q] = bv; w.rh[q] = bv; w.p[q] = 0.0; w.v[q] = 0.0;
+      v[0] += bv * bv;
+    }
+  }
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.bb = tot[0]; s.rr = tot[0]; s.r0n2 = tot[0];
+    s.tol2 = rtol * rtol * tot[0];
+    s.rho = tot[0]; s.rho_prev = 1.0; s.alpha = 1.0; s.omega = 1.0;
+    s.beta = 0.0; s.it = 0; s.maxit = maxit; s.restart = 0; s.early = 0;
+    s.status = pre_status ? pre_status[fb.inst] : TCAD_OK;
+    const bool done = s.status != TCAD_OK || !(tot[0] > 0.0) || !isfinite(tot[0]);
+    if (s.status == TCAD_OK && !isfinite(tot[0])) s.status = TCAD_ERR_NONFINITE;
+    s.active = done ? 0 : 1;
+  }
+}
+
+// p = r + beta (p - omega v)   (restart: rh = r, p = r)
+__global__ void __launch_bounds__(NT)
+k_bi_p(const tcad_pack_t pk, BiVec w, const KState* ks) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const KState s = ks[fb.inst];
+  if (!s.active) return;
+  const int64_t NN = pk.n_nodes;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t q = c * NN + k;
+      const double r = w.r[q];
+      if (s.restart) {
+        w.rh[q] = r;
+        w.p[q] = r;
+      } else {
+        w.p[q] = r + s.beta * (w.p[q] - s.omega * w.v[q]);
+      }
+    }
+  }
+}
+
+// v = A^ p, alpha = rho / (rh, v)
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_bi_v(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
+       double* partial, unsigned* ticket) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  if (!ks[fb.inst].active) return;
+  const Inst g = load_inst(pk, fb.inst);
+  int64_t off[6];
+  nbr_offsets(g, off);
+  const int64_t NN = pk.n_nodes;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    double y0, y1, y2;
+    spmv_node<DIM, true>(J, w.p, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    w.v[k] = y0; w.v[NN + k] = y1; w.v[2 * NN + k] = y2;
+    v[0] += w.rh[k] * y0 + w.rh[NN + k] * y1 + w.rh[2 * NN + k] * y2;
+  }
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.restart = 0;
+    s.rv = tot[0];
+    if (tot[0] == 0.0 || !isfinite(tot[0])) {
+      s.status = TCAD_ERR_BREAKDOWN;
+      s.active = 0;
+    } else {
+      s.alpha = s.rho / tot[0];
+    }
+  }
+}
+
+// s = r - alpha v, (s, s)
+__global__ void __launch_bounds__(NT)
+k_bi_s(const tcad_pack_t pk, BiVec w, KState* ks, double* partial, unsigned* ticket) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const KState s0 = ks[fb.inst];
+  if (!s0.active) return;
+  const int64_t NN = pk.n_nodes;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t q = c * NN + k;
+      const double sv = w.r[q] - s0.alpha * w.v[q];
+      w.s[q] = sv;
+      v[0] += sv * sv;
+    }
+  }
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.ss = tot[0];
+    s.early = tot[0] <= s.tol2 ? 1 : 0;
+  }
+}
+
+// t = A^ s, omega = (t, s) / (t, t)
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_bi_t(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
+       double* partial, unsigned* ticket) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  if (!ks[fb.inst].active) return;
+  const Inst g = load_inst(pk, fb.inst);
+  int64_t off[6];
+  nbr_offsets(g, off);
+  const int64_t NN = pk.n_nodes;
+  double v[2] = {0.0, 0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    double y0, y1, y2;
+    spmv_node<DIM, true>(J, w.s, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    w.t[k] = y0; w.t[NN + k] = y1; w.t[2 * NN + k] = y2;
+    v[0] += y0 * w.s[k] + y1 * w.s[NN + k] + y2 * w.s[2 * NN + k];
+    v[1] += y0 * y0 + y1 * y1 + y2 * y2;
+  }
+  double tot[2];
+  if (Reduce<2>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.omega = (s.early || !(tot[1] > 0.0)) ? 0.0 : tot[0] / tot[1];
+  }
+}
+
+// x += alpha p + omega s; r = s - omega t; rho = (rh, r); (r, r)
+__global__ void __launch_bounds__(NT)
+k_bi_x(const tcad_pack_t pk, double* __restrict__ x, BiVec w, KState* ks, double* partial,
+       unsigned* ticket) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const KState s0 = ks[fb.inst];
+  if (!s0.active) return;
+  const int64_t NN = pk.n_nodes;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t q = c * NN + k;
+      x[q] = x[q] + s0.alpha * w.p[q] + s0.omega * w.s[q];
+      const double r = w.s[q] - s0.omega * w.t[q];
+      w.r[q] = r;
+      const double rh = w.rh[q];
+      v[0] += rh * r;
+      v[1] += r * r;
+      v[2] += rh * rh;
+    }
+  }
+  double tot[3];
+  if (Reduce<3>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.it += 1;
+    s.rr = tot[1];
+    s.rho_prev = s.rho;
+    s.rho = tot[0];
+    if (!isfinite(tot[1])) {
+      s.status = TCAD_ERR_NONFINITE;
+      s.active = 0;
+    } else if (tot[1] <= s.tol2) {
+      s.active = 0;                     // converged (true residual checked by the host)
+    } else if (s.it >= s.maxit) {
+      s.status = TCAD_ERR_NOCONV;
+      s.active = 0;
+    } else if (s.omega == 0.0 || fabs(tot[0]) <= 1e-14 * sqrt(tot[1] * tot[2])) {
+      s.restart = 1;                    // shadow residual lost: restart from r
+      s.rho = tot[1];
+      s.r0n2 = tot[1];
+      s.beta = 0.0;
+    } else {
+      s.beta = (s.rho / s.rho_prev) * (s.alpha / s.omega);
+    }
+  }
+}
+
+// true scaled residual r = b - A^ x, its norm into the state; re-arm a restart
+// when it is not within the tolerance the recursive residual claimed
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_true_resid(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ b,
+             const double* __restrict__ x, double* __restrict__ r, KState* ks,
+             double* partial, unsigned* ticket, int rearm) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const Inst g = load_inst(pk, fb.inst);
+  int64_t off[6];
+  nbr_offsets(g, off);
+  const int64_t NN = pk.n_nodes;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    double y0, y1, y2;
+    spmv_node<DIM, true>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    const double a0 = b[k] - y0, a1 = b[NN + k] - y1, a2 = b[2 * NN + k] - y2;
+    r[k] = a0; r[NN + k] = a1; r[2 * NN + k] = a2;
+    v[0] += a0 * a0 + a1 * a1 + a2 * a2;
+  }
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.rr = tot[0];
+    if (rearm && s.status == TCAD_OK && s.bb > 0.0 && tot[0] > 4.0 * s.tol2 &&
+        s.it < s.maxit && isfinite(tot[0])) {
+      s.active = 1;
+      s.restart = 1;
+      s.rho = tot[0];
+      s.r0n2 = tot[0];
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// Newton update (device2d.py:2079-2100): per-instance max update into err
+__global__ void __launch_bounds__(NT)
+k_newton_update(const tcad_pack_t pk, double* __restrict__ psi, double* __restrict__ nn,
+                double* __restrict__ pp, const double* __restrict__ du, double max_dpsi,
+                double floor_, const uint8_t* __restrict__ active,
+                unsigned long long* __restrict__ err) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  if (active && !active[fb.inst]) return;
+  __shared__ double sm[32];
+  const int64_t NN = pk.n_nodes;
+  double e = 0.0;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    const double u0 = du[k], u1 = du[NN + k], u2 = du[2 * NN + k];
+    const bool finite = isfinite(u0) && isfinite(u1) && isfinite(u2);
+    double dpsi = u0 < -max_dpsi ? -max_dpsi : (u0 > max_dpsi ? max_dpsi : u0);
+    const double n0 = nn[k], p0 = pp[k];
+    double n1 = n0 + u1, p1 = p0 + u2;
+    // numpy.clip(a, lo, hi) = minimum(maximum(a, lo), hi)
+    n1 = fmin(fmax(n1, 0.1 * n0), 10.0 * n0);
+    p1 = fmin(fmax(p1, 0.1 * p0), 10.0 * p0);
+    const double rn = fabs(n1 - n0) / fmax(n0, floor_);
+    const double rp = fabs(p1 - p0) / fmax(p0, floor_);
+    double ek = fmax(fabs(dpsi), fmax(rn, rp));
+    if (!finite || !(ek == ek)) ek = INFINITY;  // NaN update: never "converged"
+    e = fmax(e, ek);
+    psi[k] = psi[k] + dpsi;
+    nn[k] = n1;
+    pp[k] = p1;
+  }
+  const double m = block_max<NT>(e, sm);
+  if (threadIdx.x == 0) atomicMax(&err[fb.inst], (unsigned long long)__double_as_longlong(m));
+}
+
+// --------------------------------------------------------------------------
+// equilibrium Poisson: PCG on A = -J (symmetric positive definite after the
+// symmetric elimination), Jacobi preconditioner, energy-norm stopping test
+struct CgVec {
+  double *r, *z, *p, *q;
+};
+
+template <int DIM>
+__device__ __forceinline__ double pspmv(const double* __restrict__ J,
+                                        const double* __restrict__ x, int64_t k, int64_t NN,
+                                        const int64_t* off, int64_t lo, int64_t hi) {
+  double y = J[k] * x[k];
+#pragma unroll
+  for (int d = 0; d < 2 * DIM; ++d) {
+    const int64_t m = clampi(k + off[d], lo, hi);
+    y += J[(int64_t)(1 + d) * NN + k] * x[m];
+  }
+  return -y;
+}
+
+__global__ void __launch_bounds__(NT)
+k_cg_init(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ b,
+          double* __restrict__ x, CgVec w, KState* ks, double* partial, unsigned* ticket,
+          double rtol, int maxit, const uint8_t* __restrict__ active) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const int64_t NN = pk.n_nodes;
+  double v[2] = {0.0, 0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    const double bv = b[k];
+    const double z = bv / (-J[k]);
+    x[k] = 0.0; w.r[k] = bv; w.z[k] = z; w.p[k] = z;
+    v[0] += bv * z;
+    v[1] += bv * bv;
+  }
+  (void)NN;
+  double tot[2];
+  if (Reduce<2>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.bb = tot[0]; s.rho = tot[0]; s.rr = tot[0];
+    s.tol2 = rtol * rtol * tot[0];
+    s.it = 0; s.maxit = maxit; s.status = TCAD_OK; s.restart = 0; s.early = 0;
+    if (!isfinite(tot[0]) || !isfinite(tot[1])) s.status = TCAD_ERR_NONFINITE;
+    s.active = (s.status == TCAD_OK && tot[0] > 0.0 && (!active || active[fb.inst])) ? 1 : 0;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_cg_q(const tcad_pack_t pk, const double* __restrict__ J, CgVec w, KState* ks,
+       double* partial, unsigned* ticket) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  if (!ks[fb.inst].active) return;
+  const Inst g = load_inst(pk, fb.inst);
+  int64_t off[6];
+  nbr_offsets(g, off);
+  const int64_t NN = pk.n_nodes;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    const double q = pspmv<DIM>(J, w.p, k, NN, off, fb.ioff, fb.iend);
+    w.q[k] = q;
+    v[0] += w.p[k] * q;
+  }
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    if (!(tot[0] > 0.0) || !isfinite(tot[0])) {
+      s.status = TCAD_ERR_BREAKDOWN;
+      s.active = 0;
+    } else {
+      s.alpha = s.rho / tot[0];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+k_cg_x(const tcad_pack_t pk, const double* __restrict__ J, double* __restrict__ x, CgVec w,
+       KState* ks, double* partial, unsigned* ticket) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const KState s0 = ks[fb.inst];
+  if (!s0.active) return;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    x[k] = x[k] + s0.alpha * w.p[k];
+    const double r = w.r[k] - s0.alpha * w.q[k];
+    w.r[k] = r;
+    const double z = r / (-J[k]);
+    w.z[k] = z;
+    v[0] += r * z;
+  }
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.it += 1;
+    s.rho_prev = s.rho;
+    s.rho = tot[0];
+    s.rr = tot[0];
+    if (!isfinite(tot[0])) {
+      s.status = TCAD_ERR_NONFINITE;
+      s.active = 0;
+    } else if (tot[0] <= s.tol2) {
+      s.active = 0;
+    } else if (s.it >= s.maxit) {
+      s.status = TCAD_ERR_NOCONV;
+      s.active = 0;
+    } else {
+      s.beta = s.rho / s.rho_prev;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+k_cg_p(const tcad_pack_t pk, CgVec w, const KState* ks) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const KState s = ks[fb.inst];
+  if (!s.active) return;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) w.p[k] = w.z[k] + s.beta * w.p[k];
+}
+
+// equilibrium update: clip to +-max_dpsi, psi += d, err = max |d|
+__global__ void __launch_bounds__(NT)
+k_eq_update(const tcad_pack_t pk, double* __restrict__ psi, const double* __restrict__ d,
+            double max_dpsi, const uint8_t* __restrict__ active,
+            unsigned long long* __restrict__ err) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  if (active && !active[fb.inst]) return;
+  __shared__ double sm[32];
+  double e = 0.0;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    double v = d[k];
+    v = v < -max_dpsi ? -max_dpsi : (v > max_dpsi ? max_dpsi : v);
+    psi[k] = psi[k] + v;
+    double a = fabs(v);
+    if (!(a == a)) a = INFINITY;
+    e = fmax(e, a);
+  }
+  const double m = block_max<NT>(e, sm);
+  if (threadIdx.x == 0) atomicMax(&err[fb.inst], (unsigned long long)__double_as_longlong(m));
+}
+
+// slaved Boltzmann densities n = nie_s e^psi, p = nie_s e^-psi
+__global__ void __launch_bounds__(NT)
+k_slaved(const tcad_pack_t pk, const double* __restrict__ psi, double* __restrict__ nn,
+         double* __restrict__ pp) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    const double ps = psi[k];
+    const double c = ps < -700.0 ? -700.0 : (ps > 700.0 ? 700.0 : ps);
+    nn[k] = pk.nie_s[k] * exp(c);
+    pp[k] = pk.nie_s[k] * exp(-c);
+  }
+}
+
+// --------------------------------------------------------------------------
+// workspace carving
+struct Carve {
+  char* base;
+  size_t used;
+  size_t cap;
+  template <class T>
+  T* take(size_t count) {
+    const size_t bytes = (count * sizeof(T) + 255) & ~(size_t)255;
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+struct Work {
+  BiVec bi;
+  CgVec cg;
+  double* partial;
+  KState* ks;
+  unsigned* ticket;
+  int32_t* status;
+  unsigned long long* err;
+  size_t bytes;
+};
+
+static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
+  Carve c{reinterpret_cast<char*>(base), 0, cap};
+  Work w;
+  const size_t v3 = 3 * (size_t)pk->n_nodes;
+  w.bi.r = c.take<double>(v3);
+  w.bi.rh = c.take<double>(v3);
+  w.bi.p = c.take<double>(v3);
+  w.bi.v = c.take<double>(v3);
+  w.bi.s = c.take<double>(v3);
+  w.bi.t = c.take<double>(v3);
+  // the scalar PCG reuses the first vector's storage (3 x n_nodes)
+  w.cg.r = w.bi.r;
+  w.cg.z = w.bi.r + pk->n_nodes;
+  w.cg.p = w.bi.r + 2 * pk->n_nodes;
+  w.cg.q = w.bi.rh;
+  w.partial = c.take<double>(4 * (size_t)pk->n_flat);
+  w.ks = c.take<KState>(pk->n_inst);
+  w.ticket = c.take<unsigned>(pk->n_inst);
+  w.status = c.take<int32_t>(pk->n_inst);
+  w.err = c.take<unsigned long long>(pk->n_inst);
+  w.bytes = c.used;
+  return w;
+}
+
+static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double* b,
+                           double* x, double rtol, int maxiter, const Work& w,
+                           const int32_t* pre_status, std::vector<KState>& hks,
+                           cudaStream_t s) {
+  const unsigned nb = (unsigned)pk->n_flat;
+  const int ni = pk->n_inst;
+  TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
+  k_bi_init<<<nb, NT, 0, s>>>(*pk, b, x, w.bi, w.ks, w.partial, w.ticket, rtol, maxiter,
+                              pre_status);
+  TCAD_LAUNCH_CHECK();
+  hks.resize(ni);
+  int check = 4;
+  int done_iters = 0;
+  int rechecks = 0;
+  for (;;) {
+    for (int q = 0; q < check; ++q) {
+      k_bi_p<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks);
+      if (pk->dim == 2)
+        k_bi_v<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      else
+        k_bi_v<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      k_bi_s<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks, w.partial, w.ticket);
+      if (pk->dim == 2)
+        k_bi_t<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      else
+        k_bi_t<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      k_bi_x<<<nb, NT, 0, s>>>(*pk, x, w.bi, w.ks, w.partial, w.ticket);
+    }
+    TCAD_LAUNCH_CHECK();
+    done_iters += check;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState) * ni,
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+    if (!any) {
+      // true-residual check; instances whose recursive residual drifted are
+      // re-armed from the true residual (bounded number of re-checks)
+      const int rearm = rechecks < 8 ? 1 : 0;
+      if (pk->dim == 2)
+        k_true_resid<2><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w.ks, w.partial, w.ticket, rearm);
+      else
+        k_true_resid<3><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w.ks, w.partial, w.ticket, rearm);
+      TCAD_LAUNCH_CHECK();
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState) * ni,
+                                      cudaMemcpyDeviceToHost, s));
+      TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+      for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+      ++rechecks;
+      if (!any) break;
+    }
+    if (done_iters > 64) check = 16;
+    if (done_iters > 1024) check = 32;
+  }
+  return TCAD_OK;
+}
+
+static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, double* x,
+                     double rtol, int maxiter, const Work& w, const uint8_t* active,
+                     std::vector<KState>& hks, cudaStream_t s) {
+  const unsigned nb = (unsigned)pk->n_flat;
+  const int ni = pk->n_inst;
+  TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
+  k_cg_init<<<nb, NT, 0, s>>>(*pk, J, b, x, w.cg, w.ks, w.partial, w.ticket, rtol, maxiter,
+                              active);
+  TCAD_LAUNCH_CHECK();
+  hks.resize(ni);
+  int check = 8;
+  int done_iters = 0;
+  for (;;) {
+    for (int q = 0; q < check; ++q) {
+      if (pk->dim == 2)
+        k_cg_q<2><<<nb, NT, 0, s>>>(*pk, J, w.cg, w.ks, w.partial, w.ticket);
+      else
+        k_cg_q<3><<<nb, NT, 0, s>>>(*pk, J, w.cg, w.ks, w.partial, w.ticket);
+      k_cg_x<<<nb, NT, 0, s>>>(*pk, J, x, w.cg, w.ks, w.partial, w.ticket);
+      k_cg_p<<<nb, NT, 0, s>>>(*pk, w.cg, w.ks);
+    }
+    TCAD_LAUNCH_CHECK();
+    done_iters += check;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState) * ni,
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+    if (!any) break;
+    if (done_iters > 64) check = 32;
+  }
+  return TCAD_OK;
+}
+
+}  // namespace tcad
+
+using namespace tcad;
+
+extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart) {
+  if (!pk) return 0;
+  (void)method; (void)restart;
+  Work w = carve(pk, nullptr, 0);
+  return w.bytes + 256;
+}
+
+extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
+                                       int32_t* status, void* stream) {
+  if (!pk || !J || !F || !status) return TCAD_ERR_ARG;
+  k_bj_setup<<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status);
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_block_spmv(const tcad_pack_t* pk, const double* J, const double* x,
+                               double* y, void* stream) {
+  if (!pk) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (pk->dim == 2)
+    k_spmv<2, true><<<(unsigned)pk->n_flat, NT, 0, s>>>(*pk, J, x, y);
+  else
+    k_spmv<3, true><<<(unsigned)pk->n_flat, NT, 0, s>>>(*pk, J, x, y);
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_block_krylov(const tcad_pack_t* pk, const double* J, const double* b,
+                                 double* x, int method, double rtol, int maxiter,
+                                 int restart, void* work, size_t work_bytes, int32_t* iters,
+                                 int32_t* status, double* relres, void* stream) {
+  if (!pk || !work) return TCAD_ERR_ARG;
+  if (method != 0) return TCAD_ERR_ARG;  // GMRES on the block layout: not in this library
+  (void)restart;
+  Work w = carve(pk, work, work_bytes);
+  if (w.bytes > work_bytes) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<KState> hks;
+  const int rc = launch_bicgstab(pk, J, b, x, rtol, maxiter, w, nullptr, hks, s);
+  if (rc != TCAD_OK) return rc;
+  for (int i = 0; i < pk->n_inst; ++i) {
+    if (iters) iters[i] = hks[i].it;
+    if (status) status[i] = hks[i].status;
+    if (relres) relres[i] = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
+  }
+  return TCAD_OK;
+}
+
+extern "C" int tcad_newton_update(const tcad_pack_t* pk, double* psi, double* n, double* p,
+                                  const double* du, double max_dpsi, double dens_floor,
+                                  const uint8_t* active, double* partial, double* err,
+                                  void* stream) {
+  if (!pk) return TCAD_ERR_ARG;
+  (void)partial;
+  cudaStream_t s = (cudaStream_t)stream;
+  TCAD_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(double) * pk->n_inst, s));
+  k_newton_update<<<(unsigned)pk->n_flat, NT, 0, s>>>(
+      *pk, psi, n, p, du, max_dpsi, dens_floor, active,
+      reinterpret_cast<unsigned long long*>(err));
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, double* p,
+                                 double* F, double* J, double* du,
+                                 const tcad_newton_opts_t* opts, uint8_t* active,
+                                 void* work, size_t work_bytes,
+                                 tcad_newton_result_t* result, void* stream) {
+  if (!pk || !opts || !active || !result || !work) return TCAD_ERR_ARG;
+  if (opts->method != 0) return TCAD_ERR_ARG;
+  Work w = carve(pk, work, work_bytes);
+  if (w.bytes > work_bytes) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int ni = pk->n_inst;
+  const unsigned nb = (unsigned)pk->n_flat;
+  std::vector<uint8_t> hact(ni);
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(hact.data(), active, ni, cudaMemcpyDeviceToHost, s));
+  TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+  for (int i = 0; i < ni; ++i) {
+    result[i].iters = 0; result[i].converged = 0; result[i].krylov_iters = 0;
+    result[i].status = TCAD_OK; result[i].err = INFINITY; result[i].relres = 0.0;
+  }
+  std::vector<KState> hks;
+  std::vector<unsigned long long> herr(ni);
+  std::vector<int32_t> hstat(ni);
+  for (int it = 0; it < opts->max_iter; ++it) {
+    int rc = tcad_sg_assemble(pk, psi, n, p, F, J, TCAD_MODE_ELIMINATE, stream);
+    if (rc != TCAD_OK) return rc;
+    TCAD_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int32_t) * ni, s));
+    k_bj_setup<<<nb, NT, 0, s>>>(*pk, J, F, w.status);
+    TCAD_LAUNCH_CHECK();
+    // inactive instances: pre-mark so their Krylov stays idle
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(hstat.data(), w.status, sizeof(int32_t) * ni,
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    for (int i = 0; i < ni; ++i)
+      if (!hact[i] && hstat[i] == TCAD_OK) hstat[i] = -1;  // idle marker
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(w.status, hstat.data(), sizeof(int32_t) * ni,
+                                    cudaMemcpyHostToDevice, s));
+    rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s);
+    if (rc != TCAD_OK) return rc;
+    // instances whose linear solve broke down / diverged keep their state
+    for (int i = 0; i < ni; ++i) {
+      if (!hact[i]) continue;
+      result[i].krylov_iters += hks[i].it;
+      result[i].status = hks[i].status;
+      result[i].relres = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
+    }
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(active, hact.data(), ni, cudaMemcpyHostToDevice, s));
+    TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
+    k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
+                                      active, w.err);
+    TCAD_LAUNCH_CHECK();
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int i = 0; i < ni; ++i) {
+      if (!hact[i]) continue;
+      double e;
+      std::memcpy(&e, &herr[i], sizeof(double));
+      result[i].iters = it + 1;
+      result[i].err = e;
+      const bool lin_ok = result[i].status == TCAD_OK;
+      const bool hard = result[i].status == TCAD_ERR_SINGULAR ||
+                        result[i].status == TCAD_ERR_NONFINITE;
+      if (opts->verbose)
+        std::printf("    [gpu] inst %d it %2d  err=%.3e  krylov=%d relres=%.2e st=%d\n", i,
+                    it, e, hks[i].it, result[i].relres, result[i].status);
+      if (e < opts->tol_update && lin_ok) {
+        result[i].converged = 1;
+        hact[i] = 0;
+      } else if (hard || !(e == e) || e == INFINITY) {
+        hact[i] = 0;  // singular block / non-finite state: this instance failed
+      }
+      any = any || hact[i];
+    }
+    if (!any) break;
+  }
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(active, hact.data(), ni, cudaMemcpyHostToDevice, s));
+  TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+  return TCAD_OK;
+}
+
+extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double* n,
+                                      double* p, double* F, double* J, double* d,
+                                      const tcad_newton_opts_t* opts, void* work,
+                                      size_t work_bytes, tcad_newton_result_t* result,
+                                      void* stream) {
+  if (!pk || !opts || !result || !work) return TCAD_ERR_ARG;
+  Work w = carve(pk, work, work_bytes);
+  if (w.bytes > work_bytes) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int ni = pk->n_inst;
+  const unsigned nb = (unsigned)pk->n_flat;
+  std::vector<uint8_t> hact(ni, 1);
+  uint8_t* dact = reinterpret_cast<uint8_t*>(w.status);  // reuse: n_inst bytes
+  for (int i = 0; i < ni; ++i) {
+    result[i].iters = 0; result[i].converged = 0; result[i].krylov_iters = 0;
+    result[i].status = TCAD_OK; result[i].err = INFINITY; result[i].relres = 0.0;
+  }
+  std::vector<KState> hks;
+  std::vector<unsigned long long> herr(ni);
+  for (int it = 0; it < opts->max_iter; ++it) {
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(dact, hact.data(), ni, cudaMemcpyHostToDevice, s));
+    int rc = tcad_poisson_assemble(pk, psi, F, J, TCAD_MODE_ELIMINATE, stream);
+    if (rc != TCAD_OK) return rc;
+    rc = launch_cg(pk, J, F, d, opts->rtol, opts->krylov_maxiter, w, dact, hks, s);
+    if (rc != TCAD_OK) return rc;
+    TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
+    k_eq_update<<<nb, NT, 0, s>>>(*pk, psi, d, opts->max_dpsi, dact, w.err);
+    TCAD_LAUNCH_CHECK();
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int i = 0; i < ni; ++i) {
+      if (!hact[i]) continue;
+      double e;
+      std::memcpy(&e, &herr[i], sizeof(double));
+      result[i].iters = it + 1;
+      result[i].err = e;
+      result[i].krylov_iters += hks[i].it;
+      result[i].status = hks[i].status;
+      result[i].relres = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
+      if (opts->verbose)
+        std::printf("    [gpu] eq inst %d it %2d  |d|=%.3e  cg=%d st=%d\n", i, it, e,
+                    hks[i].it, hks[i].status);
+      if (e < opts->tol_update && result[i].status == TCAD_OK) {
+        result[i].converged = 1;
+        hact[i] = 0;
+      } else if (!(e == e) || e == INFINITY) {
+        hact[i] = 0;
+      }
+      any = any || hact[i];
+    }
+    if (!any) break;
+  }
+  k_slaved<<<nb, NT, 0, s>>>(*pk, psi, n, p);
+  TCAD_LAUNCH_CHECK();
+  TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+  return TCAD_OK;
+}

@@ -1,0 +1,115 @@
+// Scharfetter-Gummel edge quantities.  Compiled with -fmad=false so the
+// arithmetic rounds step by step in the reference's order
+// (pytcad/kernels.py:88-109, pytcad/device2d.py:1449-1479).
+#pragma once
+
+#include "common.cuh"
+
+namespace tcad {
+
+// Clip to [-700, 700] keeping NaN (numpy.clip semantics).
+__device__ __forceinline__ double clip700(double x) {
+  return x < -700.0 ? -700.0 : (x > 700.0 ? 700.0 : x);
+}
+
+// B(x) and B'(x) of the series branch |x| < 1e-4 (kernels.py:92-96,105-109).
+__device__ __forceinline__ void bern_series(double x, double& B, double& dB) {
+  B = (1.0 - x / 2.0) + (x * x) / 12.0;
+  dB = (-0.5 + x / 6.0) - (x * x * x) / 180.0;
+}
+
+// B(x), B(-x), B'(x), B'(-x) with B(x) = x / expm1(x) and
+// B'(x) = B(x) (1/x - 1/(1 - e^-x)); the two expm1 values serve all four.
+__device__ __forceinline__ void bern4(double x, double& Bp, double& Bm, double& dBp,
+                                      double& dBm) {
+  x = clip700(x);
+  if (fabs(x) < 1e-4) {
+    bern_series(x, Bp, dBp);
+    bern_series(-x, Bm, dBm);
+    return;
+  }
+  const double e1 = expm1(x);   // e^x - 1
+  const double e2 = expm1(-x);  // e^-x - 1
+  Bp = x / e1;
+  Bm = (-x) / e2;
+  double om = -e2;  // 1 - e^-x
+  if (fabs(om) < 1e-300) om = 1e-300;
+  dBp = Bp * (1.0 / x - 1.0 / om);
+  double om2 = -e1;  // 1 - e^x
+  if (fabs(om2) < 1e-300) om2 = 1e-300;
+  dBm = Bm * (1.0 / (-x) - 1.0 / om2);
+}
+
+// Everything the two endpoint rows need from one edge (low -> high node).
+struct Edge {
+  double f;     // Poisson flux (psi_hi - psi_lo) / h
+  double Jn;    // electron SG current an (n_hi B(d) - n_lo B(-d))
+  double Jp;    // hole SG current -ap (p_hi B(-d') - p_lo B(d'))
+  double npsi;  // dJn/dpsi_hi = an (n_hi B'(d) + n_lo B'(-d))
+  double nlo;   // dJn/dn_lo = -an B(-d)
+  double nhi;   // dJn/dn_hi = an B(d)
+  double ppsi;  // dJp/dpsi_hi = ap (p_hi B'(-d') + p_lo B'(d'))
+  double plo;   // dJp/dp_lo = ap B(d')
+  double phi;   // dJp/dp_hi = -ap B(-d')
+};
+
+__device__ __forceinline__ void zero_edge(Edge& e) {
+  e.f = e.Jn = e.Jp = e.npsi = e.nlo = e.nhi = e.ppsi = e.plo = e.phi = 0.0;
+}
+
+// d = dpsi + dlnnie (electrons), d' = dpsi - dlnnie (holes):
+// pytcad/device2d.py:1451-1479.
+__device__ __forceinline__ void sg_edge(double psi_lo, double psi_hi, double n_lo,
+                                        double n_hi, double p_lo, double p_hi, double an,
+                                        double ap, double dl, double h, Edge& e) {
+  const double dpsi = psi_hi - psi_lo;
+  e.f = dpsi / h;
+  double Bp, Bm, dBp, dBm, Bph, Bmh, dBph, dBmh;
+  bern4(dpsi + dl, Bp, Bm, dBp, dBm);
+  if (dl == 0.0) {
+    Bph = Bp; Bmh = Bm; dBph = dBp; dBmh = dBm;
+  } else {
+    bern4(dpsi - dl, Bph, Bmh, dBph, dBmh);
+  }
+  e.Jn = an * (n_hi * Bp - n_lo * Bm);
+  e.Jp = -ap * (p_hi * Bmh - p_lo * Bph);
+  const double Sn = n_hi * dBp + n_lo * dBm;
+  const double Sp = p_hi * dBmh + p_lo * dBph;
+  e.npsi = an * Sn;
+  e.nlo = -an * Bm;
+  e.nhi = an * Bp;
+  e.ppsi = ap * Sp;
+  e.plo = ap * Bph;
+  e.phi = -ap * Bmh;
+}
+
+// SRH + Auger recombination, scaled (materials.py:474-518 with the
+// device's R0/Ns scaling, pytcad/device2d.py:1482-1508).
+__device__ __forceinline__ void recomb(double n, double p, double nie, double taun,
+                                       double taup, const double* par, double& Rs,
+                                       double& dRsn, double& dRsp) {
+  const double Ns = par[TCAD_P_NS], R0 = par[TCAD_P_R0];
+  if (par[TCAD_P_SRH] == 0.0) {
+    Rs = dRsn = dRsp = 0.0;
+    return;
+  }
+  const double nph = n * Ns, pph = p * Ns;
+  const double excess = nph * pph - nie * nie;
+  const double den = taup * (nph + nie) + taun * (pph + nie);
+  double R = excess / den;
+  const double den2 = den * den;
+  double dRdn = (pph * den - excess * taup) / den2;
+  double dRdp = (nph * den - excess * taun) / den2;
+  if (par[TCAD_P_AUGER] != 0.0) {
+    const double Cn = par[TCAD_P_CN], Cp = par[TCAD_P_CP];
+    const double cc = Cn * nph + Cp * pph;
+    R = R + cc * excess;
+    dRdn = dRdn + Cn * excess + cc * pph;
+    dRdp = dRdp + Cp * excess + cc * nph;
+  }
+  Rs = R / R0;
+  dRsn = dRdn * Ns / R0;
+  dRsp = dRdp * Ns / R0;
+}
+
+}  // namespace tcad

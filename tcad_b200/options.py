@@ -1,0 +1,90 @@
+"""Models and NewtonOptions, the reference's option contract
+(pytcad/device.py:373-535, 539-627), restricted to what the GPU path
+implements.  A physics flag the path does not implement is refused loudly
+instead of being ignored, the reference's own rule for unimplemented
+compositions (e.g. pytcad/device2d.py:224-232)."""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+
+@dataclass
+class Models:
+    doping_mobility: bool = True
+    field_mobility: bool = False
+    srh: bool = True
+    tat: bool = False
+    trap_et_rel: float = 0.5
+    fd: bool = False
+    incomplete_ion: bool = False
+    impact: bool = False
+    impact_nonlocal: bool = False
+    impact_lambda_n: float = 6.5e-6   # ii_nonlocal.py:61
+    impact_lambda_p: float = 6.5e-6
+    btbt: bool = False
+    btbt_nonlocal: bool = False
+    dg: bool = False
+    dg_gamma: float = 1.0
+    auger: bool = True
+    bgn: bool = True
+    surface_mobility: bool = False
+    driving_force: str = "field"
+    band_offset: str = "nie"
+    thermionic: bool = False
+    S_n: float = 0.0
+    S_p: float = 0.0
+    energy_balance: bool = False
+
+    _GPU_UNIMPLEMENTED = ("field_mobility", "tat", "fd", "incomplete_ion", "impact",
+                          "impact_nonlocal", "btbt", "btbt_nonlocal", "dg",
+                          "surface_mobility", "thermionic", "energy_balance")
+
+    def __post_init__(self):
+        if self.band_offset not in ("nie", "affinity"):
+            raise ValueError(f"Models.band_offset={self.band_offset!r} is not recognised")
+        if self.driving_force != "field":
+            raise NotImplementedError(
+                f"Models.driving_force={self.driving_force!r} is not implemented")
+
+    def require_gpu_path(self):
+        """Raise NotImplementedError for flags outside the GPU path."""
+        on = [f for f in self._GPU_UNIMPLEMENTED if getattr(self, f)]
+        if self.band_offset != "nie":
+            on.append("band_offset='affinity'")
+        if self.S_n != 0.0 or self.S_p != 0.0:
+            on.append("S_n/S_p")
+        if on:
+            raise NotImplementedError(
+                "tcad_b200 implements the plain drift-diffusion path (Boltzmann, "
+                "full ionisation, SRH/Auger, doping mobility, BGN); refusing "
+                f"Models({', '.join(on)}) rather than silently ignoring it")
+
+
+@dataclass
+class NewtonOptions:
+    max_iter: int = 100
+    tol_update: float = 1e-8
+    tol_residual: float = 1e-10
+    max_dpsi: float = 5.0
+    verbose: bool = False
+    linsolve: str = "auto"
+    linsolve_rtol: float = 1e-10
+    precond: str = "auto"
+    block_size: int | None = 3
+    direct_ordering: str | None = None
+    # GPU-only: Krylov iteration budget per Newton step (the reference's
+    # solve_linear caps at 500 and falls back to a CPU direct solve, which
+    # the GPU path does not have)
+    linsolve_maxiter: int = 4000
+
+    def __post_init__(self):
+        if self.precond not in ("auto", "block_jacobi", "schur"):
+            raise ValueError(f"NewtonOptions.precond={self.precond!r} is not a known "
+                             "preconditioner flavor")
+        if self.block_size is not None and (
+                not isinstance(self.block_size, int) or self.block_size <= 0):
+            raise ValueError(f"NewtonOptions.block_size={self.block_size!r} must be "
+                             "a positive int or None.")
+        if self.linsolve not in ("auto", "direct", "gmres", "bicgstab", "gpu_direct",
+                                 "petsc", "mumps"):
+            raise ValueError(f"unknown linsolve {self.linsolve!r}")

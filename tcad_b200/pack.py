@@ -1,0 +1,499 @@
+"""Host set-up of one device instance and the HBM-resident pack of one or more
+instances (the layout of include/tcad_b200.h).
+
+``Setup`` is the once-per-device part of Device2D/Device3D.__init__
+(pytcad/device2d.py:168-453, pytcad/device3d.py:437-724) for the plain path:
+scaling, per-node coefficients and per-edge SG coefficients, evaluated in
+numpy with the reference's formulas so the kernels receive bit-identical
+inputs.  ``Pack`` uploads a list of set-ups back to back into device
+memory and owns the state, Jacobian and Krylov workspace buffers.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .physics import (D0_REF, EPS0, EPS_OX_R, Q, SILICON, Semiconductor,
+                      control_volume_widths, lifetime_scharfetter,
+                      mobility_caughey_thomas, nie_effective, ohmic_values,
+                      thermal_voltage)
+from .options import Models
+
+
+def _hmean(lo, hi):
+    return 2.0 * lo * hi / (lo + hi)
+
+
+class Contact:
+    """Ohmic contact (pytcad/device2d.py:64-71 DirichletBC)."""
+    kind = "contact"
+
+    def __init__(self, nodes, V):
+        self.nodes = np.asarray(nodes, dtype=np.int64).ravel()
+        self.V = float(V)
+
+
+class Gate:
+    """Oxide gate, Robin on psi (pytcad/device2d.py:74-83, device3d.py:111-125)."""
+    kind = "gate"
+
+    def __init__(self, nodes, kappa, Vfb, Vg, w, normal_axis=None):
+        self.nodes = np.asarray(nodes, dtype=np.int64).ravel()
+        self.kappa = float(kappa)
+        self.Vfb = float(Vfb)
+        self.Vg = float(Vg)
+        self.w = np.broadcast_to(np.asarray(w, dtype=float), self.nodes.shape).copy()
+        self.normal_axis = normal_axis
+
+
+class Setup:
+    """Scaled geometry and coefficients of one device (host numpy)."""
+
+    def __init__(self, coords, doping, Ntotal=None, T=300.0, material=SILICON,
+                 models=None, Ns_override=None):
+        self.dim = len(coords)
+        self.models = models or Models()
+        self.models.require_gpu_path()
+        if not isinstance(material, Semiconductor):
+            raise NotImplementedError(
+                "tcad_b200: heterostructures (per-node material lists) are not on "
+                "the GPU path; pass one Semiconductor")
+        self.mat = material
+        self.coords = [np.asarray(c, dtype=float) for c in coords]
+        self.nax = [c.size for c in self.coords]               # Nx, Ny(, Nz)
+        if min(self.nax) < 2:
+            raise ValueError("every mesh axis needs at least 2 nodes")
+        self.shape = tuple(reversed(self.nax))
+        self.N = int(np.prod(self.nax))
+        self.doping = np.asarray(doping, dtype=float).reshape(self.shape)
+        self.Ntot = (np.abs(self.doping) if Ntotal is None
+                     else np.asarray(Ntotal, dtype=float).reshape(self.shape))
+        self.T = T
+        mat = material
+        # scaling (pytcad/device2d.py:319-347)
+        self.VT = thermal_voltage(T)
+        self.eps = mat.eps_r * EPS0
+        self.ni = mat.ni(T)
+        self.Ns = (max(float(np.abs(self.doping).max()), self.ni)
+                   if Ns_override is None else float(Ns_override))
+        self.LD = np.sqrt(self.eps * self.VT / (Q * self.Ns))
+        self.J0 = Q * D0_REF * self.Ns / self.LD
+        self.R0 = D0_REF * self.Ns / self.LD ** 2
+        self.h = [np.diff(c / self.LD) for c in self.coords]
+        self.dv = [control_volume_widths(h) for h in self.h]
+        self.C = self.doping / self.Ns
+        # per-node coefficients (pytcad/device2d.py:361-407)
+        nt = self.Ntot
+        self.nie = nie_effective(nt, mat, T, self.models.bgn)
+        self.nie_s = self.nie / self.Ns
+        if self.models.doping_mobility:
+            mu_n = mobility_caughey_thomas(nt, mat, T, "n")
+            mu_p = mobility_caughey_thomas(nt, mat, T, "p")
+        else:
+            mu_n = np.full(self.shape, mat.mu_n_max)
+            mu_p = np.full(self.shape, mat.mu_p_max)
+        self.tau_n = lifetime_scharfetter(nt, mat.tau_n0, mat.tau_Nref)
+        self.tau_p = lifetime_scharfetter(nt, mat.tau_p0, mat.tau_Nref)
+        # per-edge SG coefficients at the low node (pytcad/device2d.py:442-450)
+        self.an, self.ap, self.dl = [], [], []
+        for ax in range(self.dim):
+            lo, hi = self.lo(ax), self.hi(ax)
+            hb = self.bcast(self.h[ax], ax)
+            dn = _hmean(mu_n[lo], mu_n[hi]) * self.VT / D0_REF
+            dp = _hmean(mu_p[lo], mu_p[hi]) * self.VT / D0_REF
+            an = np.zeros(self.shape); ap = np.zeros(self.shape); dl = np.zeros(self.shape)
+            an[lo] = dn / hb
+            ap[lo] = dp / hb
+            dl[lo] = np.log(self.nie_s[hi] / self.nie_s[lo])
+            self.an.append(an); self.ap.append(ap); self.dl.append(dl)
+        self.bcs = {}
+
+    # ---- axis helpers (axis 0 = x is the last array axis)
+    def arr_axis(self, ax):
+        return self.dim - 1 - ax
+
+    def lo(self, ax):
+        s = [slice(None)] * self.dim
+        s[self.arr_axis(ax)] = slice(None, -1)
+        return tuple(s)
+
+    def hi(self, ax):
+        s = [slice(None)] * self.dim
+        s[self.arr_axis(ax)] = slice(1, None)
+        return tuple(s)
+
+    def bcast(self, v, ax):
+        shp = [1] * self.dim
+        shp[self.arr_axis(ax)] = v.size
+        return v.reshape(shp)
+
+    def flat(self, *ijk):
+        out = np.atleast_1d(np.asarray(ijk[0], dtype=np.int64))
+        stride = 1
+        for a in range(1, self.dim):
+            stride *= self.nax[a - 1]
+            out = out + np.atleast_1d(np.asarray(ijk[a], dtype=np.int64)) * stride
+        return out
+
+    def bulk_guess(self):
+        """Neutral-bulk potential (pytcad/device2d.py:744-759)."""
+        return np.arcsinh(self.C / (2.0 * self.nie_s))
+
+    def gate_kappa(self, tox_cm):
+        """pytcad/device2d.py:676-680."""
+        return EPS_OX_R * EPS0 * self.LD / (self.eps * tox_cm)
+
+    def gate_weight(self, idx, normal_axis):
+        """Face length (2D) or face area normal to `normal_axis` (3D,
+        pytcad/device3d.py:939-947) the gate flux crosses."""
+        dv = self.dv
+        if self.dim == 2:
+            return dv[0][idx[0]]
+        if normal_axis == "z":
+            return dv[0][idx[0]] * dv[1][idx[1]]
+        if normal_axis == "y":
+            return dv[0][idx[0]] * dv[2][idx[2]]
+        return dv[1][idx[1]] * dv[2][idx[2]]
+
+    # ---- boundary-condition arrays
+    def contact_table(self):
+        """Unique contact nodes (a later contact wins a shared node, as the
+        reference's row stamping does), their contact index, ln(n0/nie),
+        n0 and p0 (pytcad/contacts.py:21-38)."""
+        names = [n for n, b in self.bcs.items() if b.kind == "contact"]
+        owner = {}
+        for ci, name in enumerate(names):
+            for k in self.bcs[name].nodes:
+                owner[int(k)] = ci
+        nodes = np.array(sorted(owner), dtype=np.int64)
+        cid = np.array([owner[int(k)] for k in nodes], dtype=np.int32)
+        L, n0, p0 = ohmic_values(self.C.ravel()[nodes], self.nie_s.ravel()[nodes], 0.0,
+                                 self.VT)
+        return names, nodes, cid, L, n0, p0
+
+    def gate_arrays(self):
+        """Per-node kappa*w, V/VT - Vfb/VT (bias and equilibrium) and psi_b
+        for every gate node (pytcad/device2d.py:1624-1637)."""
+        gk = np.zeros(self.N); gv = np.zeros(self.N); gveq = np.zeros(self.N)
+        gb = np.zeros(self.N); cnt = np.zeros(self.N, dtype=np.int64)
+        acc_v = np.zeros(self.N); acc_veq = np.zeros(self.N)
+        Cf, nief = self.C.ravel(), self.nie_s.ravel()
+        for b in self.bcs.values():
+            if b.kind != "gate":
+                continue
+            k = b.nodes
+            kw = b.kappa * b.w
+            v = b.Vg / self.VT - b.Vfb / self.VT
+            veq = 0.0 - b.Vfb / self.VT
+            first = cnt[k] == 0
+            gk[k] = np.where(first, kw, gk[k] + kw)
+            gv[k] = np.where(first, v, gv[k]); gveq[k] = np.where(first, veq, gveq[k])
+            acc_v[k] += kw * v; acc_veq[k] += kw * veq
+            gb[k] = np.arcsinh(Cf[k] / (2.0 * nief[k]))
+            cnt[k] += 1
+        multi = cnt > 1   # several gates on a node: kappa*w-weighted mean
+        gv[multi] = acc_v[multi] / gk[multi]
+        gveq[multi] = acc_veq[multi] / gk[multi]
+        return cnt > 0, gk, gv, gveq, gb
+
+
+class Pack:
+    """Device-memory image of a list of Setups of one dimension."""
+
+    def __init__(self, setups, device="cuda"):
+        import torch
+        self.torch = torch
+        self.setups = list(setups)
+        dims = {s.dim for s in self.setups}
+        if len(dims) != 1:
+            raise ValueError("a pack holds instances of one dimension")
+        self.dim = dims.pop()
+        self.lib = _lib.load()
+        self.device = torch.device(device)
+        dim = self.dim
+        ni = len(self.setups)
+        sizes = [s.N for s in self.setups]
+        self.node_off = np.concatenate(([0], np.cumsum(sizes))).astype(np.int64)
+        self.N = int(self.node_off[-1])
+        nflat = [-(-n // _lib.FLAT_NODES) for n in sizes]
+        self.flat_off = np.concatenate(([0], np.cumsum(nflat))).astype(np.int64)
+        flat_inst = np.repeat(np.arange(ni, dtype=np.int32), nflat)
+        shape = np.ones((ni, 3), dtype=np.int32)
+        axis_off = np.zeros((ni, 3), dtype=np.int64)
+        hs = [[], [], []]; dvs = [[], [], []]
+        cur = [0, 0, 0]
+        for i, s in enumerate(self.setups):
+            for a in range(3):
+                if a < dim:
+                    shape[i, a] = s.nax[a]
+                    hh = np.concatenate([s.h[a], [0.0]])
+                    dd = s.dv[a]
+                else:
+                    hh, dd = np.zeros(1), np.ones(1)
+                axis_off[i, a] = cur[a]
+                cur[a] += hh.size
+                hs[a].append(hh); dvs[a].append(dd)
+        tiles = []
+        for i, s in enumerate(self.setups):
+            nz = s.nax[2] if dim == 3 else 1
+            kstep = _lib.TILE_Z if dim == 3 else 1
+            for k0 in range(0, nz, kstep):
+                for j0 in range(0, s.nax[1], _lib.TILE_Y):
+                    for i0 in range(0, s.nax[0], _lib.TILE_X):
+                        tiles.append((i, i0, j0, k0))
+        tiles = np.asarray(tiles, dtype=np.int32).ravel()
+        par = np.zeros((ni, _lib.NPAR))
+        for i, s in enumerate(self.setups):
+            par[i, 0] = s.Ns
+            par[i, 1] = s.R0
+            par[i, 2] = s.mat.Cn_auger
+            par[i, 3] = s.mat.Cp_auger
+            par[i, 4] = 1.0 if s.models.srh else 0.0
+            par[i, 5] = 1.0 if s.models.auger else 0.0
+        self.n_tiles = tiles.size // 4
+        self.n_flat = int(self.flat_off[-1])
+
+        def cat(attr):
+            return np.concatenate([getattr(s, attr).ravel() for s in self.setups])
+
+        def up(a, dtype=torch.float64):
+            return torch.from_numpy(np.ascontiguousarray(a)).to(self.device, dtype)
+
+        t = {}
+        t["shape"] = up(shape.ravel(), torch.int32)
+        t["node_off"] = up(self.node_off, torch.int64)
+        t["flat_off"] = up(self.flat_off, torch.int64)
+        t["flat_inst"] = up(flat_inst, torch.int32)
+        t["axis_off"] = up(axis_off.ravel(), torch.int64)
+        t["tile"] = up(tiles, torch.int32)
+        t["par"] = up(par.ravel())
+        for a in range(3):
+            t[f"h{a}"] = up(np.concatenate(hs[a]))
+            t[f"dv{a}"] = up(np.concatenate(dvs[a]))
+        for name in ("C", "nie", "nie_s", "tau_n", "tau_p"):
+            t[name] = up(cat(name))
+        for a in range(dim):
+            for name in ("an", "ap", "dl"):
+                t[f"{name}{a}"] = up(np.concatenate([getattr(s, name)[a].ravel()
+                                                     for s in self.setups]))
+        for name in ("bc_psi0", "bc_n0", "bc_p0", "bc_psi0_eq", "gate_k", "gate_v",
+                     "gate_veq", "gate_b"):
+            t[name] = torch.zeros(self.N, dtype=torch.float64, device=self.device)
+        t["bcflag"] = torch.zeros(self.N, dtype=torch.uint8, device=self.device)
+        self.t = t
+        P = _lib.TcadPack()
+        P.dim = dim; P.n_inst = ni; P.n_nodes = self.N
+        P.n_flat = self.n_flat; P.n_tiles = self.n_tiles
+        for f in ("shape", "node_off", "flat_off", "flat_inst", "axis_off", "tile", "par",
+                  "C", "nie", "nie_s", "tau_n", "tau_p", "bcflag", "bc_psi0", "bc_n0",
+                  "bc_p0", "bc_psi0_eq", "gate_k", "gate_v", "gate_veq", "gate_b"):
+            setattr(P, f, t[f].data_ptr())
+        for a in range(3):
+            P.h[a] = t[f"h{a}"].data_ptr()
+            P.dv[a] = t[f"dv{a}"].data_ptr()
+            src = a if a < dim else 0
+            P.an[a] = t[f"an{src}"].data_ptr()
+            P.ap[a] = t[f"ap{src}"].data_ptr()
+            P.dl[a] = t[f"dl{src}"].data_ptr()
+        self.P = P
+        self.pref = ctypes.byref(P)
+        # state and solver buffers
+        z = lambda n: torch.zeros(n, dtype=torch.float64, device=self.device)  # noqa: E731
+        self.psi, self.n, self.p = z(self.N), z(self.N), z(self.N)
+        self.F = z(3 * self.N)
+        self.J = z(_lib.NE[dim] * self.N)
+        self.du = z(3 * self.N)
+        wb = int(self.lib.tcad_block_workspace_bytes(self.pref, 0, 0))
+        self.work = torch.empty(wb, dtype=torch.uint8, device=self.device)
+        self.active = torch.ones(ni, dtype=torch.uint8, device=self.device)
+        self.contact_nodes = [None] * ni
+        self.refresh_bcs()
+
+    # ---------------------------------------------------------------------
+    def sp(self):
+        return _lib.stream_ptr()
+
+    def refresh_bcs(self):
+        """(Re)build the boundary-condition arrays from every instance's BCs."""
+        torch = self.torch
+        N = self.N
+        flag = np.zeros(N, dtype=np.uint8)
+        psi0eq = np.zeros(N)
+        gk = np.zeros(N); gv = np.zeros(N); gveq = np.zeros(N); gb = np.zeros(N)
+        c_nodes, c_cid, c_L, c_n0, c_p0 = [], [], [], [], []
+        self.contact_names = []
+        self.cid_base = []
+        base = 0
+        for i, s in enumerate(self.setups):
+            off = int(self.node_off[i])
+            names, nodes, cid, L, n0, p0 = s.contact_table()
+            self.contact_names.append(names)
+            self.cid_base.append(base)
+            g_on, g_k, g_v, g_veq, g_b = s.gate_arrays()
+            sl = slice(off, off + s.N)
+            flag[sl][g_on] |= _lib.BC_GATE
+            gk[sl] = g_k; gv[sl] = g_v; gveq[sl] = g_veq; gb[sl] = g_b
+            flag[off + nodes] |= _lib.BC_CONTACT
+            psi0eq[off + nodes] = 0.0 / s.VT + L
+            c_nodes.append(off + nodes); c_cid.append(base + cid)
+            c_L.append(L); c_n0.append(n0); c_p0.append(p0)
+            base += len(names)
+        self.n_contacts_total = base
+        up = lambda a, dt=torch.float64: torch.from_numpy(  # noqa: E731
+            np.ascontiguousarray(a)).to(self.device, dt)
+        self.t["bcflag"].copy_(up(flag, torch.uint8))
+        self.t["bc_psi0_eq"].copy_(up(psi0eq))
+        self.t["gate_k"].copy_(up(gk)); self.t["gate_v"].copy_(up(gv))
+        self.t["gate_veq"].copy_(up(gveq)); self.t["gate_b"].copy_(up(gb))
+        self.c_nodes = up(np.concatenate(c_nodes) if c_nodes else np.zeros(0), torch.int64)
+        self.c_cid = up(np.concatenate(c_cid) if c_cid else np.zeros(0), torch.int32)
+        self.c_L = up(np.concatenate(c_L) if c_L else np.zeros(0))
+        self.c_n0 = up(np.concatenate(c_n0) if c_n0 else np.zeros(0))
+        self.c_p0 = up(np.concatenate(c_p0) if c_p0 else np.zeros(0))
+        self._gate_host = gv
+        # per contact: device node list (for terminal currents)
+        self.contact_lists = {}
+        for i, s in enumerate(self.setups):
+            off = int(self.node_off[i])
+            for name, b in s.bcs.items():
+                if b.kind == "contact":
+                    self.contact_lists[(i, name)] = up(off + np.unique(b.nodes), torch.int64)
+        maxc = max([v.numel() for v in self.contact_lists.values()] + [1])
+        self.cur_partial = torch.zeros(2 * maxc, dtype=torch.float64, device=self.device)
+        self.cur_out = torch.zeros(max(len(self.contact_lists), 1), dtype=torch.float64,
+                                   device=self.device)
+        self.set_bias()
+
+    def set_bias(self, voltages=None):
+        """Contact targets at each contact's voltage and the gates' Vg terms.
+        voltages: optional per-instance {name: V} overriding the stored V."""
+        torch = self.torch
+        vv = np.zeros(max(self.n_contacts_total, 1))
+        for i, s in enumerate(self.setups):
+            over = voltages[i] if voltages else {}
+            for ci, name in enumerate(self.contact_names[i]):
+                V = over.get(name, s.bcs[name].V) if over else s.bcs[name].V
+                vv[self.cid_base[i] + ci] = V / s.VT
+        vvt = torch.from_numpy(vv).to(self.device)
+        rc = self.lib.tcad_set_contacts(
+            self.pref, _lib.ptr(self.c_nodes), self.c_nodes.numel(), _lib.ptr(self.c_cid),
+            _lib.ptr(vvt), _lib.ptr(self.c_L), _lib.ptr(self.c_n0), _lib.ptr(self.c_p0),
+            _lib.ptr(self.t["bc_psi0"]), _lib.ptr(self.t["bc_n0"]), _lib.ptr(self.t["bc_p0"]),
+            self.sp())
+        _lib.check(rc, "tcad_set_contacts")
+        # gate V/VT - Vfb/VT at the current Vg (host recompute: gate sets are small
+        # relative to the mesh, the upload is one node array)
+        gv = np.zeros(self.N)
+        changed = False
+        for i, s in enumerate(self.setups):
+            if any(b.kind == "gate" for b in s.bcs.values()):
+                off = int(self.node_off[i])
+                gv[off:off + s.N] = s.gate_arrays()[2]
+                changed = True
+        if changed:
+            self.t["gate_v"].copy_(torch.from_numpy(gv).to(self.device))
+        self._vvt = vvt  # keep alive until the kernel ran
+
+    def stamp_contacts(self):
+        rc = self.lib.tcad_stamp_contacts(self.pref, _lib.ptr(self.c_nodes),
+                                          self.c_nodes.numel(), _lib.ptr(self.psi),
+                                          _lib.ptr(self.n), _lib.ptr(self.p), self.sp())
+        _lib.check(rc, "tcad_stamp_contacts")
+
+    # ---- kernels -----------------------------------------------------------
+    def assemble(self, mode, psi=None, n=None, p=None):
+        rc = self.lib.tcad_sg_assemble(
+            self.pref, _lib.ptr(self.psi if psi is None else psi),
+            _lib.ptr(self.n if n is None else n), _lib.ptr(self.p if p is None else p),
+            _lib.ptr(self.F), _lib.ptr(self.J), mode, self.sp())
+        _lib.check(rc, "tcad_sg_assemble")
+
+    def assemble_poisson(self, mode, psi=None, F=None, J=None):
+        rc = self.lib.tcad_poisson_assemble(
+            self.pref, _lib.ptr(self.psi if psi is None else psi),
+            _lib.ptr(self.F if F is None else F), _lib.ptr(self.J if J is None else J),
+            mode, self.sp())
+        _lib.check(rc, "tcad_poisson_assemble")
+
+    def contact_current(self, inst, name, psi=None, n=None, p=None, out_slot=0):
+        """Deterministic sum of raw F_n + F_p over a contact's nodes (scaled)."""
+        nodes = self.contact_lists[(inst, name)]
+        rc = self.lib.tcad_contact_current(
+            self.pref, _lib.ptr(self.psi if psi is None else psi),
+            _lib.ptr(self.n if n is None else n), _lib.ptr(self.p if p is None else p),
+            _lib.ptr(nodes), nodes.numel(), _lib.ptr(self.cur_partial),
+            self.cur_partial.numel(), _lib.ptr(self.cur_out[out_slot:]), self.sp())
+        _lib.check(rc, "tcad_contact_current")
+        return self.cur_out[out_slot]
+
+    def raw_continuity(self, nodes_dev, psi, n, p):
+        """Raw (F_n, F_p) at a device node list."""
+        torch = self.torch
+        cnt = nodes_dev.numel()
+        part = torch.zeros(2 * max(cnt, 1), dtype=torch.float64, device=self.device)
+        out = torch.zeros(1, dtype=torch.float64, device=self.device)
+        rc = self.lib.tcad_contact_current(self.pref, _lib.ptr(psi), _lib.ptr(n),
+                                           _lib.ptr(p), _lib.ptr(nodes_dev), cnt,
+                                           _lib.ptr(part), part.numel(), _lib.ptr(out),
+                                           self.sp())
+        _lib.check(rc, "tcad_contact_current")
+        return part[:cnt], part[cnt:2 * cnt]
+
+    def edge_currents(self, axis, psi=None, n=None, p=None):
+        torch = self.torch
+        Jn = torch.empty(self.N, dtype=torch.float64, device=self.device)
+        Jp = torch.empty(self.N, dtype=torch.float64, device=self.device)
+        rc = self.lib.tcad_edge_currents(
+            self.pref, axis, _lib.ptr(self.psi if psi is None else psi),
+            _lib.ptr(self.n if n is None else n), _lib.ptr(self.p if p is None else p),
+            _lib.ptr(Jn), _lib.ptr(Jp), self.sp())
+        _lib.check(rc, "tcad_edge_currents")
+        return Jn, Jp
+
+    def newton_opts(self, opts, equilibrium=False):
+        o = _lib.NewtonOpts()
+        o.max_iter = int(opts.max_iter)
+        o.method = 1 if opts.linsolve == "gmres" and not equilibrium else 0
+        o.method = 0  # the node-block path runs BiCGStab (GMRES: see linsolve.py)
+        o.krylov_maxiter = int(getattr(opts, "linsolve_maxiter", 4000))
+        o.restart = 0
+        o.tol_update = float(opts.tol_update)
+        o.max_dpsi = float(opts.max_dpsi)
+        o.rtol = float(opts.linsolve_rtol)
+        o.dens_floor = 1e-10
+        o.verbose = 1 if opts.verbose else 0
+        return o
+
+    def newton(self, opts, active=None):
+        ni = len(self.setups)
+        if active is None:
+            self.active.fill_(1)
+        else:
+            self.active.copy_(self.torch.as_tensor(np.asarray(active, np.uint8)))
+        o = self.newton_opts(opts)
+        res = (_lib.NewtonResult * ni)()
+        rc = self.lib.tcad_newton_solve(
+            self.pref, _lib.ptr(self.psi), _lib.ptr(self.n), _lib.ptr(self.p),
+            _lib.ptr(self.F), _lib.ptr(self.J), _lib.ptr(self.du), ctypes.byref(o),
+            _lib.ptr(self.active), _lib.ptr(self.work), self.work.numel(), res, self.sp())
+        _lib.check(rc, "tcad_newton_solve")
+        return [dict(iters=r.iters, converged=bool(r.converged),
+                     krylov_iters=r.krylov_iters, status=r.status, err=r.err,
+                     relres=r.relres) for r in res]
+
+    def equilibrium(self, opts):
+        ni = len(self.setups)
+        o = self.newton_opts(opts, equilibrium=True)
+        o.krylov_maxiter = max(o.krylov_maxiter, 20000)
+        res = (_lib.NewtonResult * ni)()
+        d = self.du[: self.N]
+        rc = self.lib.tcad_equilibrium_solve(
+            self.pref, _lib.ptr(self.psi), _lib.ptr(self.n), _lib.ptr(self.p),
+            _lib.ptr(self.F), _lib.ptr(self.J), _lib.ptr(d), ctypes.byref(o),
+            _lib.ptr(self.work), self.work.numel(), res, self.sp())
+        _lib.check(rc, "tcad_equilibrium_solve")
+        return [dict(iters=r.iters, converged=bool(r.converged),
+                     krylov_iters=r.krylov_iters, status=r.status, err=r.err,
+                     relres=r.relres) for r in res]

@@ -95,3 +95,29 @@ def vec_err(a, b, scale=None):
     s = np.abs(b) if scale is None else np.maximum(np.abs(b), scale)
     s = np.where(s == 0, 1.0, s)
     return float((np.abs(a - b) / s).max())
+
+
+def gpu_device(g, material=None):
+    """The same device on the GPU path (tcad_b200), BCs with the stored kappa."""
+    import tcad_b200 as tb
+    from tcad_b200.pack import Contact, Gate
+    m = g["models"]
+    mat = tb.Semiconductor(**(material or {}))
+    models = tb.Models(doping_mobility=bool(m[0]), srh=bool(m[1]), auger=bool(m[2]),
+                       bgn=bool(m[3]))
+    if int(g["dim"]) == 2:
+        dev = tb.Device2D(tb.Mesh2D(g["x"], g["y"]), g["doping"], Ntotal=g["Ntot"],
+                          T=float(g["T"]), material=mat, models=models)
+    else:
+        dev = tb.Device3D(tb.Mesh3D(g["x"], g["y"], g["z"]), g["doping"],
+                          Ntotal=g["Ntot"], T=float(g["T"]), material=mat, models=models)
+    s = dev.setup
+    for name, kind, k, v in bcs(g):
+        if kind == "contact":
+            dev.bcs[name] = Contact(k, v[0])
+        else:
+            idx = [np.asarray(a, dtype=np.int64) for a in unflat(g, k)]
+            axis = "xyz"[int(v[3])] if int(g["dim"]) == 3 else None
+            dev.bcs[name] = Gate(k, v[0], v[1], v[2], s.gate_weight(idx, axis), axis)
+    dev._bcs_changed()
+    return dev

@@ -1,0 +1,92 @@
+"""CPU tests: host-side set-up and the C ABI (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import fixtures as fx
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize("name", ["asm2d", "asm3d", "trigate_small", "mosfet_small"])
+def test_setup_matches_oracle_bitwise(name):
+    """The coefficient arrays handed to the kernels equal the oracle's (and
+    hence the reference's) bit for bit."""
+    from tcad_b200.pack import Setup
+    import tcad_b200 as tb
+    g = fx.load(name)
+    ora = fx.oracle_device(g)
+    m = g["models"]
+    s = Setup(fx.coords(g), g["doping"], Ntotal=g["Ntot"], T=float(g["T"]),
+              models=tb.Models(doping_mobility=bool(m[0]), srh=bool(m[1]),
+                               auger=bool(m[2]), bgn=bool(m[3])))
+    for a in ("Ns", "LD", "J0", "R0", "VT"):
+        assert getattr(s, a) == getattr(ora, a), a
+    for a in ("C", "nie", "nie_s", "tau_n", "tau_p"):
+        assert np.array_equal(getattr(s, a), getattr(ora, a)), a
+    for ax in range(s.dim):
+        assert np.array_equal(s.h[ax], ora.h[ax]) and np.array_equal(s.dv[ax], ora.dv[ax])
+        lo = s.lo(ax)
+        assert np.array_equal(s.an[ax][lo], ora.an[ax])
+        assert np.array_equal(s.ap[ax][lo], ora.ap[ax])
+        assert np.array_equal(s.dl[ax][lo], ora.dlnnie[ax])
+        hi_edge = [slice(None)] * s.dim
+        hi_edge[s.arr_axis(ax)] = -1
+        assert not s.an[ax][tuple(hi_edge)].any()
+
+
+def test_contact_table_matches_ohmic_values():
+    from tcad_b200.pack import Setup
+    import tcad_b200 as tb
+    from oracle import ohmic_values
+    g = fx.load("trigate_small")
+    s = Setup(fx.coords(g), g["doping"], Ntotal=g["Ntot"], models=tb.Models())
+    from tcad_b200.pack import Contact
+    for name, kind, k, v in fx.bcs(g):
+        if kind == "contact":
+            s.bcs[name] = Contact(k, 0.3)
+    names, nodes, cid, L, n0, p0 = s.contact_table()
+    psi0, on0, op0 = ohmic_values(s.C.ravel()[nodes], s.nie_s.ravel()[nodes], 0.3, s.VT)
+    assert np.array_equal(0.3 / s.VT + L, psi0)
+    assert np.array_equal(n0, on0) and np.array_equal(p0, op0)
+
+
+def test_refuses_unimplemented_models():
+    import tcad_b200 as tb
+    with pytest.raises(NotImplementedError):
+        tb.Models(fd=True).require_gpu_path()
+    with pytest.raises(NotImplementedError):
+        tb.Models(S_n=1e3).require_gpu_path()
+
+
+def _header_functions():
+    src = open(os.path.join(ROOT, "include", "tcad_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tcad_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_header_symbol():
+    """The .so loads (no GPU needed to dlopen) and exports every function the
+    header declares; the ctypes binding covers the same set."""
+    from tcad_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        import __graft_entry__
+        __graft_entry__.build()
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    names = _header_functions()
+    assert len(names) >= 12
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) <= set(_lib.exported_names()) | {"tcad_pack_sizeof", "tcad_version"}
+    assert lib.tcad_pack_sizeof() == ctypes.sizeof(_lib.TcadPack)
+
+
+def test_product_does_not_import_oracle():
+    for dirpath, _, files in os.walk(os.path.join(ROOT, "tcad_b200")):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cuh")):
+                txt = open(os.path.join(dirpath, f)).read()
+                assert "import oracle" not in txt and "from oracle" not in txt, f
