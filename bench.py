@@ -1,0 +1,478 @@
+#!/usr/bin/env python
+"""Converged bias points per second of the drift-diffusion solve on B200.
+
+Workload (default): the 3D n-channel tri-gate on a 160 x 96 x 64 tensor mesh
+(983,040 nodes, 2,949,120 unknowns): p-body 1e18, Gaussian S/D implants of
+peak 1e20 cm^-3 (sigma 10 nm), 40 nm gate, 1 nm oxide Robin gates on three
+faces; Id-Vg sweep Vg = 0..1.0 V in 21 steps at Vd = 0.05 V and at 0.7 V,
+each sweep warm-started from equilibrium.  Synthetic device (no dataset).
+
+One step = one bias point (warm-started Newton + terminal current).  A point
+counts only when Newton converged (update < 1e-8 plus the polishing step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--workload trigate3d|diode2d] [--small]
+
+N > 1: one process per GPU under torchrun, each an independent replica of the
+sweep (the path does not shard: replicas only); value = all ranks' points /
+max-over-ranks time.  --impl reference: the oracle's CPU implementation of
+the same path on the host cores (rank 0 only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "converged bias pts/s at <=1e-6 rel current err, chosen vs plain GPU; p50/p99"
+UNIT = "bias_pts/s"
+
+# Algorithmic bytes per node (one launch touches every node once):
+#  block SpMV (scaled, 3D): J 39 doubles + x 3 + y 3             = 360 B
+#  coupled SG assembly (3D): 16 doubles in (psi,n,p,C,nie,tau_n,tau_p,
+#     an/ap/dl x 3 axes) + bcflag byte + 42 doubles out (F 3, J 39) = 465 B
+BYTES_SPMV = {2: (29 + 3 + 3) * 8, 3: (39 + 3 + 3) * 8}
+BYTES_ASM = {2: (13 + 32) * 8 + 1, 3: (16 + 42) * 8 + 1}
+
+# Newton iterations / BiCGStab iterations per bias point of the plain FP64
+# path on this workload, from its own bench runs; used only to scale the
+# CPU oracle's measured per-iteration costs to a bias point.
+TRIGATE_ITERS = {"newton_per_point": 4.0, "krylov_per_newton": 250.0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="trigate3d", choices=["trigate3d", "diode2d"])
+    ap.add_argument("--small", action="store_true", help="down-scaled mesh (testing)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(name):
+    """Bytes per launch of a kernel from its committed ncu summary
+    (profiles/<name>.md, line 'traffic_bytes_per_launch: <int>'), else None."""
+    p = os.path.join(ROOT, "profiles", name + ".md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(float(line.split(":")[1]))
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def build_workload(name, small, dev_cls_2d, dev_cls_3d):
+    from tcad_b200 import workloads as W
+    if name == "diode2d":
+        nx, ny = (41, 11) if small else (201, 101)
+        dev = W.diode2d(dev_cls_2d, nx, ny)
+        sched = [({"anode": v}, i == 0) for i, v in enumerate(W.DIODE_SWEEP)]
+        desc = f"diode2d {nx}x{ny} ({nx * ny} nodes) 0..0.7 V step 0.05"
+        contact = "anode"
+    else:
+        dims = (40, 24, 16) if small else (160, 96, 64)
+        dev = W.trigate3d(dev_cls_3d, *dims)
+        sched = [(W.trigate_bias(vd, vg), first) for vd, vg, first in W.trigate_schedule()]
+        desc = (f"trigate3d {dims[0]}x{dims[1]}x{dims[2]} ({np.prod(dims):,} nodes) "
+                "Id-Vg Vg 0..1.0 V step 0.05 at Vd 0.05 V and 0.7 V")
+        contact = "drain"
+    return dev, sched, desc, contact
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import tcad_b200 as tb
+    from tcad_b200 import _lib
+    lib = _lib.load()
+    dev, sched, desc, contact = build_workload(args.workload, args.small, tb.Device2D,
+                                               tb.Device3D)
+    opts = tb.NewtonOptions(verbose=bool(args.verbose))
+    dim = dev.dim
+    N = dev.N
+    state = {"q": 0}
+    newton_log = []
+
+    def one_point(e2e):
+        volts, first = sched[state["q"] % len(sched)]
+        state["q"] += 1
+        if first:
+            dev.solve_equilibrium(opts)
+        dev.solve_bias(volts, opts)
+        I = dev.terminal_current(contact)
+        h2d = 8 * (len(volts) + 3) + (8 * N if any(k.startswith("gate") for k in volts) else 0)
+        d2h = 8
+        if e2e:
+            _ = dev.psi          # the step's field result back on the host
+            d2h += 8 * N
+        newton_log.append(dict(dev.last_newton, first=first))
+        if args.verbose:
+            r = dev.last_newton
+            sys.stderr.write(f"  point {state['q']:3d} {volts} first={first} conv={r['converged']}"
+                             f" newton={r['iters']} krylov={r['krylov_iters']} "
+                             f"relres={r['relres']:.1e} I={I:.6e}\n")
+            sys.stderr.flush()
+        return I, dev.last_converged, h2d, d2h
+
+    for _ in range(args.warmup):
+        one_point(True)
+    newton_log.clear()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 2)]
+    L0 = lib.tcad_launch_count()
+    lat_dev, lat_e2e, conv, h2d_tot, d2h_tot = [], [], 0, 0, 0
+    with Clocks(local) as clk:
+        t_wall = time.perf_counter()
+        ev[0].record()
+        for q in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c = torch.cuda.Event(enable_timing=True)
+            a.record()
+            I, ok, h2d, d2h = one_point(False)
+            b.record()
+            _ = dev.psi                 # host read of the field (e2e leg)
+            c.record()
+            torch.cuda.synchronize()
+            lat_dev.append(a.elapsed_time(b))
+            lat_e2e.append(a.elapsed_time(c))
+            conv += int(ok)
+            h2d_tot += h2d
+            d2h_tot += d2h + 8 * N
+        ev[1].record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t_wall
+    launches = lib.tcad_launch_count() - L0
+    t_dev = sum(lat_dev) / 1e3
+    t_e2e = ev[0].elapsed_time(ev[1]) / 1e3
+    if world > 1:
+        tt = torch.tensor([t_dev, t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = float(tt[0]), float(tt[1])
+        cc = torch.tensor([conv], device="cuda", dtype=torch.float64)
+        dist.all_reduce(cc, op=dist.ReduceOp.SUM)
+        conv_all = int(cc.item())
+    else:
+        conv_all = conv
+
+    # ---- live roofline of the dominant kernel (block SpMV on the last J) and
+    # of the assembly, CUDA events on the launching stream
+    pk = dev.pack
+    sp = _lib.stream_ptr()
+    y = torch.empty_like(pk.du)
+    x = torch.randn(3 * pk.N, dtype=torch.float64, device=pk.device)
+
+    def time_kernel(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    # the scaled operator needs D^-1 blocks: re-assemble and set up once
+    pk.assemble(_lib.MODE_ELIMINATE)
+    st = torch.zeros(1, dtype=torch.int32, device=pk.device)
+    lib.tcad_block_jacobi_setup(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(st), sp)
+    t_spmv = time_kernel(lambda: lib.tcad_block_spmv(pk.pref, _lib.ptr(pk.J), _lib.ptr(x),
+                                                     _lib.ptr(y), sp), 50)
+    Fa = torch.empty_like(pk.F)
+    Ja = torch.empty_like(pk.J)
+    t_asm = time_kernel(lambda: lib.tcad_sg_assemble(pk.pref, _lib.ptr(pk.psi), _lib.ptr(pk.n),
+                                                     _lib.ptr(pk.p), _lib.ptr(Fa), _lib.ptr(Ja),
+                                                     _lib.MODE_ELIMINATE, sp), 20)
+    peak, peak_kind = load_peaks()
+    ach_spmv = BYTES_SPMV[dim] * N / t_spmv / 1e9
+    ach_asm = BYTES_ASM[dim] * N / t_asm / 1e9
+    tr = load_traffic(f"spmv{dim}d_{args.workload}")
+
+    res = {}
+    if rank == 0:
+        pts = [r for r in newton_log]
+        nn = [r["iters"] for r in pts]
+        kk = [r["krylov_iters"] for r in pts]
+        value = conv_all / t_dev
+        res = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic device (analytic doping profiles, explicit mesh)",
+            "config": {"workload": desc, "method": "plain FP64 GPU path: fused SG assembly, "
+                       "node-block-scaled BiCGStab, damped Newton (+1 polishing step)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (J alone is "
+                             f"{8 * _lib.NE[dim] * N / 1e6:.0f} MB)"},
+            "p50_ms": statistics.median(lat_dev),
+            "p99_ms": float(np.percentile(lat_dev, 99)),
+            "converged_points": conv_all, "points": args.steps * world,
+            "newton_iters_mean": float(np.mean(nn)), "krylov_iters_mean": float(np.mean(kk)),
+            "e2e": {"value": conv_all / t_e2e, "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d_tot / args.steps),
+                    "d2h_bytes_per_step": int(d2h_tot / args.steps),
+                    "p50_ms": statistics.median(lat_e2e),
+                    "p99_ms": float(np.percentile(lat_e2e, 99))},
+            "roofline": {"kernel": "k_bi_v/k_bi_t/k_spmv (node-block SpMV, FP64)",
+                         "bound": "hbm", "achieved": ach_spmv, "peak": peak,
+                         "unit": "GB/s", "frac": ach_spmv / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "bytes_per_launch": BYTES_SPMV[dim] * N,
+                         "launch_ms": t_spmv * 1e3, "traffic": tr},
+            "roofline_assembly": {"kernel": "k_sg_assemble", "bound": "hbm",
+                                  "achieved": ach_asm, "peak": peak, "unit": "GB/s",
+                                  "frac": ach_asm / peak,
+                                  "bytes_per_launch": BYTES_ASM[dim] * N,
+                                  "launch_ms": t_asm * 1e3,
+                                  "traffic": load_traffic(f"assemble{dim}d_{args.workload}")},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "wall_s": wall,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline(dev, args, nn, kk)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return res
+
+
+def oracle_from(dev):
+    """The same device, state and BCs for the CPU oracle."""
+    from oracle import OracleDevice, OracleModels
+    s = dev.setup
+    m = s.models
+    mat = {k: getattr(s.mat, k) for k in s.mat.__dataclass_fields__ if k != "name"}
+    ora = OracleDevice(s.coords, s.doping, Ntotal=s.Ntot, T=s.T,
+                       models=OracleModels(m.doping_mobility, m.srh, m.auger, m.bgn),
+                       material=mat)
+    for name, b in dev.bcs.items():
+        if b.kind == "contact":
+            ora.contacts[name] = [b.nodes.copy(), b.V]
+        else:
+            ora.gates[name] = [b.nodes.copy(), b.kappa, b.Vfb, b.Vg, b.w.copy()]
+    return ora
+
+
+def cpu_costs(ora, psi, n, p, krylov_iters=10):
+    """Time one full-mesh oracle Newton iteration's pieces on the host:
+    assembly + Dirichlet elimination, node-block-Jacobi set-up, and the cost
+    of one BiCGStab iteration (right block-Jacobi, scipy)."""
+    from oracle import eliminate_csr, build_block_jacobi
+    from scipy.sparse.linalg import LinearOperator, bicgstab
+    t0 = time.perf_counter()
+    F, J, _, _ = ora.residual_jacobian(psi, n, p)
+    Jd, rhs = eliminate_csr(J, -F, ora.fixed)
+    t_asm = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    inv = build_block_jacobi(Jd, 3)
+    t_bj = time.perf_counter() - t0
+    nb = Jd.shape[0] // 3
+    M = LinearOperator(Jd.shape, lambda v: np.einsum("nij,nj->ni", inv,
+                                                     v.reshape(nb, 3)).ravel())
+    t0 = time.perf_counter()
+    bicgstab(Jd, rhs, rtol=1e-30, atol=0.0, maxiter=krylov_iters, M=M)
+    t_it = (time.perf_counter() - t0) / krylov_iters
+    return t_asm, t_bj, t_it
+
+
+def cpu_baseline(dev, args, newton_iters, krylov_iters):
+    """Oracle on the host cores, one full-mesh sample scaled to a bias point
+    with the GPU run's own Newton and Krylov iteration counts."""
+    try:
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+        ora = oracle_from(dev)
+        t_asm, t_bj, t_it = cpu_costs(ora, dev.psi, dev.n, dev.p)
+        per_point = [nw * (t_asm + t_bj) + kr * t_it
+                     for nw, kr in zip(newton_iters, krylov_iters)]
+        sec = float(np.mean(per_point))
+        return {"value": 1.0 / sec, "unit": UNIT, "cores": 1, "kind": "port",
+                "sample": ("oracle (numpy/scipy) on the full mesh: one assembly + "
+                           f"elimination ({t_asm:.2f} s), one node-block-Jacobi set-up "
+                           f"({t_bj:.2f} s), 10 scipy BiCGStab iterations "
+                           f"({t_it:.3f} s each); scaled to a bias point with the GPU "
+                           "run's per-point Newton and BiCGStab iteration counts"),
+                "sec_per_point": sec}
+    except Exception as exc:      # the baseline is reported, never required
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "port",
+                "sample": f"failed: {exc!r}"}
+
+
+def run_reference(args):
+    """The oracle's CPU implementation on the host cores (rank 0 only)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return None
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count() or 1))
+    from tcad_b200 import workloads as W
+    from tcad_b200.pack import Setup, Contact, Gate
+    import tcad_b200 as tb
+
+    class HostOnly:
+        """Device-shaped host set-up (no GPU touched): the workload builders
+        fill its BCs, then the oracle takes it over."""
+        dim = 3
+
+        def __init__(self, mesh, doping, Ntotal=None, models=None, **kw):
+            coords = (mesh.x, mesh.y) if not hasattr(mesh, "z") else (mesh.x, mesh.y, mesh.z)
+            self.dim = len(coords)
+            self.setup = Setup(coords, doping, Ntotal=Ntotal, models=models or tb.Models(),
+                               **kw)
+            self.bcs = self.setup.bcs
+
+        def add_contact(self, name, *ijk, V=0.0):
+            self.bcs[name] = Contact(self.setup.flat(*ijk), V)
+
+        def add_gate(self, name, *ijk, tox_cm, Vfb, Vg=0.0, normal_axis="z"):
+            idx = [np.atleast_1d(np.asarray(a, dtype=np.int64)) for a in ijk]
+            self.bcs[name] = Gate(self.setup.flat(*ijk), self.setup.gate_kappa(tox_cm), Vfb,
+                                  Vg, self.setup.gate_weight(idx, normal_axis), normal_axis)
+
+    dev, sched, desc, contact = build_workload(args.workload, args.small, HostOnly, HostOnly)
+    ora = oracle_from(dev)
+    ora.solve_equilibrium() if args.workload == "diode2d" else None
+    if args.workload == "diode2d":
+        # full solves: every step is one real warm-started bias point
+        lat = []
+        pts = [v for v, _ in sched]
+        for q in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            ora.solve_bias(pts[q % len(pts)])
+            ora.terminal_current(contact)
+            if q >= args.warmup:
+                lat.append(time.perf_counter() - t0)
+        sample = "full oracle bias points (scipy SuperLU), warm-started sweep"
+    else:
+        # bounded sample: one full-mesh Newton-iteration cost per step, at the
+        # bulk-guess state, scaled with the plain GPU path's iteration counts
+        psi = ora.bulk_guess()
+        n = ora.nie_s * np.exp(psi)
+        p = ora.nie_s * np.exp(-psi)
+        lat = []
+        for q in range(args.warmup + args.steps):
+            t_asm, t_bj, t_it = cpu_costs(ora, psi, n, p, krylov_iters=5)
+            sec = (TRIGATE_ITERS["newton_per_point"] * (t_asm + t_bj)
+                   + TRIGATE_ITERS["newton_per_point"] * TRIGATE_ITERS["krylov_per_newton"]
+                   * t_it)
+            if q >= args.warmup:
+                lat.append(sec)
+        sample = ("per step: one full-mesh oracle assembly + elimination + "
+                  "node-block-Jacobi set-up + 5 scipy BiCGStab iterations, scaled to a "
+                  f"bias point with {TRIGATE_ITERS['newton_per_point']} Newton x "
+                  f"{TRIGATE_ITERS['krylov_per_newton']} BiCGStab iterations")
+    sec = float(np.mean(lat))
+    value = 1.0 / sec
+    cores = int(os.environ.get("OPENBLAS_NUM_THREADS", "1"))
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic device",
+            "config": {"workload": desc, "method": "oracle CPU port (numpy/scipy)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        res = run_reference(args)
+    else:
+        res = run_ours(args)
+    if res:
+        print(json.dumps(res))
+        sys.stdout.flush()
+
+
+if __name__ == "__main__":
+    main()

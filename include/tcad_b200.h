@@ -110,6 +110,8 @@ typedef struct tcad_pack {
 size_t tcad_pack_sizeof(void);
 /* "tcad_b200 <version> sm_100a" */
 const char* tcad_version(void);
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t tcad_launch_count(void);
 
 /* ---- assembly ------------------------------------------------------------
  * Coupled SG residual/Jacobian at (psi, n, p) [scaled, n_nodes each].
@@ -186,6 +188,22 @@ int tcad_block_krylov(const tcad_pack_t* pk, const double* J, const double* b,
                       void* work, size_t work_bytes, int32_t* iters,
                       int32_t* status, double* relres, void* stream);
 
+/* ---- general CSR (linsolve.solve_linear drop-in) -------------------------
+ * Solve A x = b for one n x n CSR matrix (int32 indices, device memory),
+ * x holding the initial guess.  method 0: BiCGStab (maxiter iterations),
+ * 1: GMRES(restart) (maxiter restart cycles), both right-preconditioned by
+ * node-block-Jacobi when block_size == 3 divides n (point Jacobi otherwise or
+ * when a block is singular; *precond_out = 3, 1 or 0), stopping at
+ * ||b - A x|| <= max(atol, rtol ||b||) (pytcad/linsolve.py:941-985).
+ * *resid_out = true ||b - A x|| / ||b||.  Returns TCAD_ERR_NOCONV when the
+ * tolerance was not met (x then holds the last iterate). */
+size_t tcad_csr_workspace_bytes(int64_t n, int method, int restart);
+int tcad_csr_krylov(int64_t n, const int32_t* indptr, const int32_t* indices,
+                    const double* data, const double* b, double* x, int method,
+                    int block_size, double rtol, double atol, int maxiter, int restart,
+                    void* work, size_t work_bytes, int32_t* iters_out, double* resid_out,
+                    int32_t* precond_out, void* stream);
+
 /* ---- Newton --------------------------------------------------------------
  * Damped update of the coupled Newton loop (pytcad/device2d.py:2079-2160):
  * clip dpsi to +-max_dpsi, n/p to [0.1x, 10x], err = max(|dpsi|,
@@ -206,6 +224,9 @@ typedef struct tcad_newton_opts {
   double rtol;           /* Krylov relative tolerance (1e-10) */
   double dens_floor;     /* 1e-10 */
   int32_t verbose;
+  int32_t polish;        /* extra Newton steps after the update test passes */
+  double eta_max;        /* forcing: loosest Krylov tolerance of an early step */
+  int32_t forcing;       /* 0: every step at rtol; 1: eta_k = clamp(0.1 err_{k-1}, rtol, eta_max) */
   int32_t pad;
 } tcad_newton_opts_t;
 

@@ -8,7 +8,7 @@ solve methods raise when the library or a CUDA device is missing.
 from .options import Models, NewtonOptions  # noqa: F401
 from .physics import (SILICON, Semiconductor, Mesh2D, Mesh3D, graded_nodes,  # noqa: F401
                       flatband_voltage, thermal_voltage)
-from .linsolve import LinearSolveError  # noqa: F401
+from .linsolve import LinearSolveError, solve_linear  # noqa: F401
 from .device import Device2D, Device3D  # noqa: F401
 
 __version__ = "0.1"

@@ -53,7 +53,9 @@ class NewtonOpts(ctypes.Structure):
                 ("krylov_maxiter", ctypes.c_int32), ("restart", ctypes.c_int32),
                 ("tol_update", ctypes.c_double), ("max_dpsi", ctypes.c_double),
                 ("rtol", ctypes.c_double), ("dens_floor", ctypes.c_double),
-                ("verbose", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("verbose", ctypes.c_int32), ("polish", ctypes.c_int32),
+                ("eta_max", ctypes.c_double), ("forcing", ctypes.c_int32),
+                ("pad", ctypes.c_int32)]
 
 
 class NewtonResult(ctypes.Structure):
@@ -66,6 +68,7 @@ class NewtonResult(ctypes.Structure):
 _SIGS = {
     "tcad_pack_sizeof": (ctypes.c_size_t, []),
     "tcad_version": (ctypes.c_char_p, []),
+    "tcad_launch_count": (ctypes.c_uint64, []),
     "tcad_sg_assemble": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, ctypes.c_int, _p]),
     "tcad_contact_current": (ctypes.c_int, [_p, _p, _p, _p, _p, ctypes.c_int64, _p,
                                             ctypes.c_int64, _p, _p]),
@@ -86,6 +89,11 @@ _SIGS = {
     "tcad_set_contacts": (ctypes.c_int, [_p, _p, ctypes.c_int64, _p, _p, _p, _p, _p,
                                          _p, _p, _p, _p]),
     "tcad_stamp_contacts": (ctypes.c_int, [_p, _p, ctypes.c_int64, _p, _p, _p, _p]),
+    "tcad_csr_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
+    "tcad_csr_krylov": (ctypes.c_int, [ctypes.c_int64, _p, _p, _p, _p, _p, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int, ctypes.c_int, _p, ctypes.c_size_t,
+                                       _p, _p, _p, _p]),
 }
 
 _lib = None

@@ -24,6 +24,7 @@ UNITS = {
     "krylov.cu": [],
     "capi.cu": [],
     "bc.cu": [],
+    "csr.cu": [],
 }
 
 

@@ -486,6 +486,7 @@ extern "C" int tcad_sg_assemble(const tcad_pack_t* pk, const double* psi, const 
     k_sg_assemble<2><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode);
   else
     k_sg_assemble<3><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }
@@ -502,9 +503,11 @@ extern "C" int tcad_contact_current(const tcad_pack_t* pk, const double* psi,
       k_contact_current<2><<<nb_, 256, 0, s>>>(*pk, psi, n, p, nodes, count, partial);
     else
       k_contact_current<3><<<nb_, 256, 0, s>>>(*pk, psi, n, p, nodes, count, partial);
+    note_launch();
     TCAD_LAUNCH_CHECK();
   }
   k_sum_list<<<1, 256, 0, s>>>(partial, count, out_sum);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }
@@ -519,6 +522,7 @@ extern "C" int tcad_edge_currents(const tcad_pack_t* pk, int axis, const double*
     k_edge_currents<2><<<nb_, kFlatThreads, 0, s>>>(*pk, axis, psi, n, p, Jn, Jp);
   else
     k_edge_currents<3><<<nb_, kFlatThreads, 0, s>>>(*pk, axis, psi, n, p, Jn, Jp);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }
@@ -532,6 +536,7 @@ extern "C" int tcad_poisson_assemble(const tcad_pack_t* pk, const double* psi, d
     k_poisson_assemble<2><<<nb_, kFlatThreads, 0, s>>>(*pk, psi, F, J, mode);
   else
     k_poisson_assemble<3><<<nb_, kFlatThreads, 0, s>>>(*pk, psi, F, J, mode);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }

@@ -39,6 +39,7 @@ extern "C" int tcad_set_contacts(const tcad_pack_t* pk, const int64_t* nodes, in
   if (count == 0) return TCAD_OK;
   k_set_contacts<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       nodes, count, cid, vv, L, n0, p0, bc_psi0, bc_n0, bc_p0);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }
@@ -49,6 +50,7 @@ extern "C" int tcad_stamp_contacts(const tcad_pack_t* pk, const int64_t* nodes, 
   if (count == 0) return TCAD_OK;
   k_stamp_contacts<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       *pk, nodes, count, psi, n, p);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }

@@ -16,6 +16,9 @@
 
 namespace tcad {
 
+// Count of kernels this library launched (defined in capi.cu).
+void note_launch(uint64_t n = 1);
+
 constexpr int kFlatThreads = 256;
 constexpr int kFlatPerThread = TCAD_FLAT_NODES / kFlatThreads;  // 4
 constexpr int kTileThreads = TCAD_TILE_X * TCAD_TILE_Y;           // 256

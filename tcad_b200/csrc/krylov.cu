@@ -185,7 +185,7 @@ struct BiVec {
 __global__ void __launch_bounds__(NT)
 k_bi_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict__ x,
           BiVec w, KState* ks, double* partial, unsigned* ticket, double rtol, int maxit,
-          const int32_t* __restrict__ pre_status) {
+          const int32_t* __restrict__ pre_status, const double* __restrict__ rtol_inst) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const int64_t NN = pk.n_nodes;
   double v[1] = {0.0};
@@ -202,7 +202,8 @@ k_bi_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict
   if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     KState& s = ks[fb.inst];
     s.bb = tot[0]; s.rr = tot[0]; s.r0n2 = tot[0];
-    s.tol2 = rtol * rtol * tot[0];
+    const double rt = rtol_inst ? rtol_inst[fb.inst] : rtol;
+    s.tol2 = rt * rt * tot[0];
     s.rho = tot[0]; s.rho_prev = 1.0; s.alpha = 1.0; s.omega = 1.0;
     s.beta = 0.0; s.it = 0; s.maxit = maxit; s.restart = 0; s.early = 0;
     s.status = pre_status ? pre_status[fb.inst] : TCAD_OK;
@@ -608,6 +609,7 @@ struct Work {
   unsigned* ticket;
   int32_t* status;
   unsigned long long* err;
+  double* eta;
   size_t bytes;
 };
 
@@ -631,6 +633,7 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   w.ticket = c.take<unsigned>(pk->n_inst);
   w.status = c.take<int32_t>(pk->n_inst);
   w.err = c.take<unsigned long long>(pk->n_inst);
+  w.eta = c.take<double>(pk->n_inst);
   w.bytes = c.used;
   return w;
 }
@@ -638,12 +641,13 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
 static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double* b,
                            double* x, double rtol, int maxiter, const Work& w,
                            const int32_t* pre_status, std::vector<KState>& hks,
-                           cudaStream_t s) {
+                           cudaStream_t s, const double* rtol_inst = nullptr) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
   k_bi_init<<<nb, NT, 0, s>>>(*pk, b, x, w.bi, w.ks, w.partial, w.ticket, rtol, maxiter,
-                              pre_status);
+                              pre_status, rtol_inst);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   hks.resize(ni);
   int check = 4;
@@ -652,16 +656,21 @@ static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double*
   for (;;) {
     for (int q = 0; q < check; ++q) {
       k_bi_p<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks);
+      note_launch();
       if (pk->dim == 2)
         k_bi_v<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
       else
         k_bi_v<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      note_launch();
       k_bi_s<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks, w.partial, w.ticket);
+      note_launch();
       if (pk->dim == 2)
         k_bi_t<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
       else
         k_bi_t<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      note_launch();
       k_bi_x<<<nb, NT, 0, s>>>(*pk, x, w.bi, w.ks, w.partial, w.ticket);
+      note_launch();
     }
     TCAD_LAUNCH_CHECK();
     done_iters += check;
@@ -678,6 +687,7 @@ static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double*
         k_true_resid<2><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w.ks, w.partial, w.ticket, rearm);
       else
         k_true_resid<3><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w.ks, w.partial, w.ticket, rearm);
+      note_launch();
       TCAD_LAUNCH_CHECK();
       TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState) * ni,
                                       cudaMemcpyDeviceToHost, s));
@@ -700,6 +710,7 @@ static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, do
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
   k_cg_init<<<nb, NT, 0, s>>>(*pk, J, b, x, w.cg, w.ks, w.partial, w.ticket, rtol, maxiter,
                               active);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   hks.resize(ni);
   int check = 8;
@@ -710,8 +721,11 @@ static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, do
         k_cg_q<2><<<nb, NT, 0, s>>>(*pk, J, w.cg, w.ks, w.partial, w.ticket);
       else
         k_cg_q<3><<<nb, NT, 0, s>>>(*pk, J, w.cg, w.ks, w.partial, w.ticket);
+      note_launch();
       k_cg_x<<<nb, NT, 0, s>>>(*pk, J, x, w.cg, w.ks, w.partial, w.ticket);
+      note_launch();
       k_cg_p<<<nb, NT, 0, s>>>(*pk, w.cg, w.ks);
+      note_launch();
     }
     TCAD_LAUNCH_CHECK();
     done_iters += check;
@@ -741,6 +755,7 @@ extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double*
                                        int32_t* status, void* stream) {
   if (!pk || !J || !F || !status) return TCAD_ERR_ARG;
   k_bj_setup<<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }
@@ -753,6 +768,7 @@ extern "C" int tcad_block_spmv(const tcad_pack_t* pk, const double* J, const dou
     k_spmv<2, true><<<(unsigned)pk->n_flat, NT, 0, s>>>(*pk, J, x, y);
   else
     k_spmv<3, true><<<(unsigned)pk->n_flat, NT, 0, s>>>(*pk, J, x, y);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }
@@ -789,6 +805,7 @@ extern "C" int tcad_newton_update(const tcad_pack_t* pk, double* psi, double* n,
   k_newton_update<<<(unsigned)pk->n_flat, NT, 0, s>>>(
       *pk, psi, n, p, du, max_dpsi, dens_floor, active,
       reinterpret_cast<unsigned long long*>(err));
+  note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }
@@ -815,11 +832,14 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   std::vector<KState> hks;
   std::vector<unsigned long long> herr(ni);
   std::vector<int32_t> hstat(ni);
+  std::vector<int> polish_left(ni, -1);  // -1: not yet converged
+  std::vector<double> heta(ni, opts->forcing ? std::max(opts->eta_max, opts->rtol) : opts->rtol);
   for (int it = 0; it < opts->max_iter; ++it) {
     int rc = tcad_sg_assemble(pk, psi, n, p, F, J, TCAD_MODE_ELIMINATE, stream);
     if (rc != TCAD_OK) return rc;
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int32_t) * ni, s));
     k_bj_setup<<<nb, NT, 0, s>>>(*pk, J, F, w.status);
+    note_launch();
     TCAD_LAUNCH_CHECK();
     // inactive instances: pre-mark so their Krylov stays idle
     TCAD_CUDA_CHECK(cudaMemcpyAsync(hstat.data(), w.status, sizeof(int32_t) * ni,
@@ -829,7 +849,10 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       if (!hact[i] && hstat[i] == TCAD_OK) hstat[i] = -1;  // idle marker
     TCAD_CUDA_CHECK(cudaMemcpyAsync(w.status, hstat.data(), sizeof(int32_t) * ni,
                                     cudaMemcpyHostToDevice, s));
-    rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s);
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(w.eta, heta.data(), sizeof(double) * ni,
+                                    cudaMemcpyHostToDevice, s));
+    rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
+                         w.eta);
     if (rc != TCAD_OK) return rc;
     // instances whose linear solve broke down / diverged keep their state
     for (int i = 0; i < ni; ++i) {
@@ -842,6 +865,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
     k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
                                       active, w.err);
+    note_launch();
     TCAD_LAUNCH_CHECK();
     TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
                                     cudaMemcpyDeviceToHost, s));
@@ -857,11 +881,20 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       const bool hard = result[i].status == TCAD_ERR_SINGULAR ||
                         result[i].status == TCAD_ERR_NONFINITE;
       if (opts->verbose)
-        std::printf("    [gpu] inst %d it %2d  err=%.3e  krylov=%d relres=%.2e st=%d\n", i,
-                    it, e, hks[i].it, result[i].relres, result[i].status);
-      if (e < opts->tol_update && lin_ok) {
+        std::printf("    [gpu] inst %d it %2d  err=%.3e  krylov=%d relres=%.2e eta=%.1e st=%d\n",
+                    i, it, e, hks[i].it, result[i].relres, heta[i], result[i].status);
+      // forcing term of the next step (inexact Newton): quadratic convergence
+      // is kept while the linear tolerance tracks the update size
+      if (opts->forcing)
+        heta[i] = std::min(std::max(opts->eta_max, opts->rtol),
+                           std::max(opts->rtol, 0.1 * (std::isfinite(e) ? e : 1.0)));
+      if (polish_left[i] > 0) {
+        // post-convergence polishing step (already counted as converged)
+        if (--polish_left[i] == 0) hact[i] = 0;
+      } else if (e < opts->tol_update && lin_ok) {
         result[i].converged = 1;
-        hact[i] = 0;
+        polish_left[i] = opts->polish > 0 ? opts->polish : 0;
+        if (polish_left[i] == 0) hact[i] = 0;
       } else if (hard || !(e == e) || e == INFINITY) {
         hact[i] = 0;  // singular block / non-finite state: this instance failed
       }
@@ -901,6 +934,7 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
     if (rc != TCAD_OK) return rc;
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
     k_eq_update<<<nb, NT, 0, s>>>(*pk, psi, d, opts->max_dpsi, dact, w.err);
+    note_launch();
     TCAD_LAUNCH_CHECK();
     TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
                                     cudaMemcpyDeviceToHost, s));
@@ -929,6 +963,7 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
     if (!any) break;
   }
   k_slaved<<<nb, NT, 0, s>>>(*pk, psi, n, p);
+  note_launch();
   TCAD_LAUNCH_CHECK();
   TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
   return TCAD_OK;

@@ -76,6 +76,17 @@ class NewtonOptions:
     # solve_linear caps at 500 and falls back to a CPU direct solve, which
     # the GPU path does not have)
     linsolve_maxiter: int = 4000
+    # GPU-only: Newton steps taken after the update test passes.  The test
+    # saturates at the 1e-10 density floor, so sub-floor minority densities
+    # (and low-bias currents) are converged only to ~1e-5 when it first
+    # passes; one more quadratic step brings them to round-off.
+    polish: int = 1
+    # GPU-only: inexact-Newton forcing.  "adaptive" solves step k to
+    # eta_k = clamp(0.1 * update_{k-1}, linsolve_rtol, eta_max) (quadratic
+    # convergence is kept; the converged state is the same); "fixed" solves
+    # every step to linsolve_rtol like the reference's iterative branch.
+    forcing: str = "adaptive"
+    eta_max: float = 1e-3
 
     def __post_init__(self):
         if self.precond not in ("auto", "block_jacobi", "schur"):

@@ -464,6 +464,9 @@ class Pack:
         o.rtol = float(opts.linsolve_rtol)
         o.dens_floor = 1e-10
         o.verbose = 1 if opts.verbose else 0
+        o.polish = 0 if equilibrium else int(getattr(opts, "polish", 0))
+        o.forcing = 1 if getattr(opts, "forcing", "fixed") == "adaptive" else 0
+        o.eta_max = float(getattr(opts, "eta_max", 1e-3))
         return o
 
     def newton(self, opts, active=None):

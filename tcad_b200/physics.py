@@ -196,30 +196,33 @@ class Mesh3D:
 
 
 def graded_nodes(n, L, focus, ratio):
-    """Exactly `n` nodes on [0, L] whose spacing grows geometrically by
-    `ratio` per cell away from the nearest focus point (both sides).  Used by
-    the workload builders, which need explicit node counts."""
+    """Exactly `n` nodes on [0, L], spacing growing linearly with the distance
+    d to the nearest focus point, s(d) = h0 + (ratio - 1) d -- the target
+    size of pytcad/mesh.py:30-116 (graded_mesh), i.e. a geometric series of
+    cell sizes with the given ratio -- with h0 chosen so that the node count
+    is exactly n.  Used by the workload builders, which need explicit node
+    counts."""
     focus = np.sort(np.clip(np.atleast_1d(np.asarray(focus, dtype=float)), 0.0, L))
     if n < 2:
         raise ValueError("need at least 2 nodes")
-    # cell-size density s(x) = ratio^(d(x)/h0) integrated numerically, then
-    # equal-mass subdivision (the cell-to-cell ratio is ~ratio where it grows)
-    xs = np.linspace(0.0, L, 200001)
+    g = ratio - 1.0
+    xs = np.linspace(0.0, L, 400001)
     d = np.min(np.abs(xs[:, None] - focus[None, :]), axis=1)
-    lo, hi = 1e-12, L
-    for _ in range(200):          # find h0 so that the cell count is n-1
+
+    def cells(h0):
+        w = 1.0 / (h0 + g * d)
+        return np.concatenate(([0.0], np.cumsum(0.5 * (w[1:] + w[:-1]) * np.diff(xs))))
+
+    lo, hi = L * 1e-9, L
+    for _ in range(200):            # bisection on h0 (log scale)
         h0 = np.sqrt(lo * hi)
-        s = h0 * np.power(ratio, np.minimum(d / h0, 700.0 / np.log(ratio)))
-        s = np.minimum(s, L)
-        cells = np.trapezoid(1.0 / s, xs)
-        if cells > n - 1:
+        if cells(h0)[-1] > n - 1:
             lo = h0
         else:
             hi = h0
-        if hi / lo < 1 + 1e-12:
+        if hi / lo < 1.0 + 1e-13:
             break
-    w = 1.0 / s
-    cum = np.concatenate(([0.0], np.cumsum(0.5 * (w[1:] + w[:-1]) * np.diff(xs))))
+    cum = cells(np.sqrt(lo * hi))
     cum /= cum[-1]
     x = np.interp(np.linspace(0.0, 1.0, n), cum, xs)
     x[0], x[-1] = 0.0, L

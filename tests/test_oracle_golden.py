@@ -64,7 +64,7 @@ def test_equilibrium_matches_reference(name):
 def _sweep(g, volts_of, tags, dev):
     I = []
     for v, tag in zip(g[volts_of[0]], tags):
-        dev.solve_bias(volts_of[1](float(v)))
+        dev.solve_bias(volts_of[1](float(v)), tol=float(g["tol_update"]))
         assert dev.last_converged
         I.append(dev.terminal_current(volts_of[2]))
         if "psi_" + tag in g:
@@ -80,7 +80,7 @@ def test_diode_small_sweep():
     assert np.abs(dev.psi.ravel() - g["psi_eq"]).max() * dev.VT < 1e-9
     I = []
     for V in g["V"]:
-        dev.solve_bias({"anode": float(V)})
+        dev.solve_bias({"anode": float(V)}, tol=float(g["tol_update"]))
         assert dev.last_converged
         I.append(dev.terminal_current("anode"))
     I = np.array(I)
