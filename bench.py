@@ -19,6 +19,7 @@ max-over-ranks time.  --impl reference: the oracle's CPU implementation of
 the same path on the host cores (rank 0 only).
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -58,6 +59,9 @@ def parse():
     ap.add_argument("--small", action="store_true", help="down-scaled mesh (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--kernels", action="store_true",
+                    help="profiling mode: assembly, block-Jacobi set-up and 20 BiCGStab "
+                         "iterations on the full-size workload at its bulk-guess state")
     return ap.parse_args()
 
 
@@ -463,8 +467,50 @@ def run_reference(args):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_kernels(args):
+    """A short, representative launch sequence for ncu: 3 coupled assemblies,
+    one block-Jacobi set-up, 3 block SpMVs and one 20-iteration BiCGStab, on
+    the full workload at its neutral-bulk state (no Newton solve)."""
+    import torch
+    import tcad_b200 as tb
+    from tcad_b200 import _lib
+    lib = _lib.load()
+    dev, sched, desc, contact = build_workload(args.workload, args.small, tb.Device2D,
+                                               tb.Device3D)
+    pk = dev.pack
+    s = dev.setup
+    g = s.bulk_guess()
+    pk.psi.copy_(dev._to_dev(g))
+    pk.n.copy_(dev._to_dev(s.nie_s * np.exp(g)))
+    pk.p.copy_(dev._to_dev(s.nie_s * np.exp(-g)))
+    pk.set_bias()
+    sp = _lib.stream_ptr()
+    for _ in range(3):
+        _lib.check(lib.tcad_sg_assemble(pk.pref, _lib.ptr(pk.psi), _lib.ptr(pk.n),
+                                        _lib.ptr(pk.p), _lib.ptr(pk.F), _lib.ptr(pk.J),
+                                        _lib.MODE_ELIMINATE, sp), "assemble")
+    st = torch.zeros(max(1, len(pk.setups)), dtype=torch.int32, device=pk.device)
+    _lib.check(lib.tcad_block_jacobi_setup(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F),
+                                           _lib.ptr(st), sp), "bj")
+    y = torch.empty_like(pk.du)
+    for _ in range(3):
+        _lib.check(lib.tcad_block_spmv(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(y),
+                                       sp), "spmv")
+    it, stt, rr = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_double(0)
+    _lib.check(lib.tcad_block_krylov(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(pk.du),
+                                     0, 1e-30, 20, 0, _lib.ptr(pk.work), pk.work.numel(),
+                                     ctypes.byref(it), ctypes.byref(stt), ctypes.byref(rr),
+                                     sp), "krylov")
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "kernels", "workload": desc, "nodes": int(dev.N),
+                      "krylov_iters": it.value, "launches": int(lib.tcad_launch_count())}))
+
+
 def main():
     args = parse()
+    if args.kernels:
+        run_kernels(args)
+        return
     if args.impl == "reference":
         res = run_reference(args)
     else:

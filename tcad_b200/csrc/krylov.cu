@@ -881,7 +881,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       const bool hard = result[i].status == TCAD_ERR_SINGULAR ||
                         result[i].status == TCAD_ERR_NONFINITE;
       if (opts->verbose)
-        std::printf("    [gpu] inst %d it %2d  err=%.3e  krylov=%d relres=%.2e eta=%.1e st=%d\n",
+        std::fprintf(stderr, "    [gpu] inst %d it %2d  err=%.3e  krylov=%d relres=%.2e eta=%.1e st=%d\n",
                     i, it, e, hks[i].it, result[i].relres, heta[i], result[i].status);
       // forcing term of the next step (inexact Newton): quadratic convergence
       // is kept while the linear tolerance tracks the update size
@@ -950,7 +950,7 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
       result[i].status = hks[i].status;
       result[i].relres = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
       if (opts->verbose)
-        std::printf("    [gpu] eq inst %d it %2d  |d|=%.3e  cg=%d st=%d\n", i, it, e,
+        std::fprintf(stderr, "    [gpu] eq inst %d it %2d  |d|=%.3e  cg=%d st=%d\n", i, it, e,
                     hks[i].it, hks[i].status);
       if (e < opts->tol_update && result[i].status == TCAD_OK) {
         result[i].converged = 1;

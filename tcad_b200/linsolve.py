@@ -56,6 +56,8 @@ def solve_linear(A, b, *, method="direct", rtol=1e-10, atol=0.0, maxiter=500,
         raise LinearSolveError(f"solve_linear({method!r}): b contains non-finite values")
     if not np.all(np.isfinite(A.data)):
         raise LinearSolveError(f"solve_linear({method!r}): A contains non-finite values")
+    if A.nnz == 0 or np.any(np.diff(A.indptr) == 0):
+        raise LinearSolveError(f"solve_linear({method!r}): A has an empty row (singular)")
     if A.nnz >= 2 ** 31 or n >= 2 ** 31:
         raise ValueError("solve_linear: matrix too large for 32-bit CSR indices")
     dev = torch.device("cuda")
