@@ -204,6 +204,27 @@ int tcad_csr_krylov(int64_t n, const int32_t* indptr, const int32_t* indices,
                     void* work, size_t work_bytes, int32_t* iters_out, double* resid_out,
                     int32_t* precond_out, void* stream);
 
+/* ---- node-block BiCGStab that allocates nothing ---------------------------
+ * No counterpart in the reference.  The same solve as tcad_block_krylov
+ * (method 0), for callers that cannot allocate device memory on demand: a
+ * serving process whose HBM is already carved up by its own pool, a foreign-
+ * language host (cgo / JNI / N-API) with no device allocator, or a latency-
+ * critical loop that must not pay cudaMalloc's device-wide synchronisation.
+ * The Krylov scratch is a file-scope device array of TCAD_STATIC_SCRATCH_BYTES
+ * (5 MiB) that every GPU loading this library holds until exit; the entry
+ * point calls no cudaMalloc / cudaFree and no host heap.  Limits:
+ * n_nodes <= TCAD_STATIC_MAX_NODES (32768) and n_inst <= TCAD_STATIC_MAX_INST
+ * (32); larger packs get TCAD_ERR_ARG.  The first call on each device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device current;
+ * make it before any stream capture.  Calls share the array: each call clears
+ * what must start at zero, and calls whose work overlaps on the GPU race. */
+#define TCAD_STATIC_MAX_NODES 32768
+#define TCAD_STATIC_MAX_INST 32
+#define TCAD_STATIC_SCRATCH_BYTES (5u << 20)
+int tcad_block_krylov_noalloc(const tcad_pack_t* pk, const double* J, const double* b,
+                              double* x, double rtol, int maxiter, int32_t* iters,
+                              int32_t* status, double* relres, void* stream);
+
 /* ---- Newton --------------------------------------------------------------
  * Damped update of the coupled Newton loop (pytcad/device2d.py:2079-2160):
  * clip dpsi to +-max_dpsi, n/p to [0.1x, 10x], err = max(|dpsi|,

@@ -89,6 +89,8 @@ _SIGS = {
     "tcad_set_contacts": (ctypes.c_int, [_p, _p, ctypes.c_int64, _p, _p, _p, _p, _p,
                                          _p, _p, _p, _p]),
     "tcad_stamp_contacts": (ctypes.c_int, [_p, _p, ctypes.c_int64, _p, _p, _p, _p]),
+    "tcad_block_krylov_noalloc": (ctypes.c_int, [_p, _p, _p, _p, ctypes.c_double,
+                                                 ctypes.c_int, _p, _p, _p, _p]),
     "tcad_csr_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
     "tcad_csr_krylov": (ctypes.c_int, [ctypes.c_int64, _p, _p, _p, _p, _p, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_double, ctypes.c_double,

@@ -968,3 +968,115 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
   TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
   return TCAD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Node-block BiCGStab that allocates nothing.
+//
+// Some callers cannot allocate device memory on demand: a serving process
+// whose HBM is carved up by its own pool allocator up front, a foreign-
+// language host (cgo, JNI, N-API) that has no device allocator to hand over
+// scratch, or a latency-critical loop that must not pay cudaMalloc's implicit
+// device-wide synchronisation.  For them the Krylov scratch lives in the
+// file-scope device array below: TCAD_STATIC_SCRATCH_BYTES, which every GPU
+// that loads this library keeps reserved until the process exits.  The
+// caller passes only inputs (pack, prepared J, b) and outputs (x, per-
+// instance results).
+//
+// Set-up: the array's host-side name is only a stand-in for the symbol, not
+// a device address, so the first call on each device (with that device
+// current) looks the address up with cudaGetSymbolAddress and caches it; make
+// that first call before any stream capture.  All calls share the one array:
+// the solver clears what must start at zero (reduction tickets) and
+// initialises its vectors itself, and two calls whose work overlaps on the GPU
+// (different streams, or different host threads) race on the scratch.
+namespace tcad {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[TCAD_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+static void* g_noalloc_addr[kMaxDevices] = {nullptr};
+
+static int noalloc_scratch(void** out) {
+  int dev = -1;
+  TCAD_CUDA_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return TCAD_ERR_ARG;
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* p = nullptr;
+    TCAD_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return TCAD_OK;
+}
+
+}  // namespace tcad
+
+extern "C" int tcad_block_krylov_noalloc(const tcad_pack_t* pk, const double* J,
+                                         const double* b, double* x, double rtol,
+                                         int maxiter, int32_t* iters, int32_t* status,
+                                         double* relres, void* stream) {
+  if (!pk || !J || !b || !x) return TCAD_ERR_ARG;
+  if (pk->n_nodes > TCAD_STATIC_MAX_NODES || pk->n_inst > TCAD_STATIC_MAX_INST ||
+      pk->n_inst < 1)
+    return TCAD_ERR_ARG;  // beyond the static scratch: use tcad_block_krylov
+  void* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc != TCAD_OK) return rc;
+  Work w = carve(pk, base, TCAD_STATIC_SCRATCH_BYTES);
+  if (w.bytes > TCAD_STATIC_SCRATCH_BYTES) return TCAD_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned nb = (unsigned)pk->n_flat;
+  const int ni = pk->n_inst;
+  KState hks[TCAD_STATIC_MAX_INST];  // host mirror on the stack, no heap
+  TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
+  k_bi_init<<<nb, NT, 0, s>>>(*pk, b, x, w.bi, w.ks, w.partial, w.ticket, rtol, maxiter,
+                              nullptr, nullptr);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  int check = 4, done_iters = 0, rechecks = 0;
+  for (;;) {
+    for (int q = 0; q < check; ++q) {
+      k_bi_p<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks);
+      if (pk->dim == 2)
+        k_bi_v<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      else
+        k_bi_v<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      k_bi_s<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks, w.partial, w.ticket);
+      if (pk->dim == 2)
+        k_bi_t<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      else
+        k_bi_t<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+      k_bi_x<<<nb, NT, 0, s>>>(*pk, x, w.bi, w.ks, w.partial, w.ticket);
+      note_launch(5);
+    }
+    TCAD_LAUNCH_CHECK();
+    done_iters += check;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(hks, w.ks, sizeof(KState) * ni, cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+    if (!any) {
+      const int rearm = rechecks < 8 ? 1 : 0;
+      if (pk->dim == 2)
+        k_true_resid<2><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w.ks, w.partial, w.ticket, rearm);
+      else
+        k_true_resid<3><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w.ks, w.partial, w.ticket, rearm);
+      note_launch();
+      TCAD_LAUNCH_CHECK();
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(hks, w.ks, sizeof(KState) * ni, cudaMemcpyDeviceToHost,
+                                      s));
+      TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+      for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+      ++rechecks;
+      if (!any) break;
+    }
+    if (done_iters > 64) check = 16;
+    if (done_iters > 1024) check = 32;
+  }
+  for (int i = 0; i < ni; ++i) {
+    if (iters) iters[i] = hks[i].it;
+    if (status) status[i] = hks[i].status;
+    if (relres) relres[i] = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
+  }
+  return TCAD_OK;
+}
