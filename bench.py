@@ -58,6 +58,11 @@ def parse():
     ap.add_argument("--workload", default="trigate3d", choices=["trigate3d", "diode2d"])
     ap.add_argument("--small", action="store_true", help="down-scaled mesh (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"],
+                    help="the timed (chosen) path; the plain FP64 path is always run "
+                         "beside it on the same points for the current check")
+    ap.add_argument("--plain-steps", type=int, default=None,
+                    help="points of the plain FP64 comparison run (default: warmup+steps)")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--kernels", action="store_true",
                     help="profiling mode: assembly, block-Jacobi set-up and 20 BiCGStab "
@@ -162,6 +167,63 @@ def build_workload(name, small, dev_cls_2d, dev_cls_3d):
     return dev, sched, desc, contact
 
 
+class PointRunner:
+    """One device marching through the bias schedule with one Newton method."""
+
+    def __init__(self, args, method, dev_classes):
+        import tcad_b200 as tb
+        self.args = args
+        self.dev, self.sched, self.desc, self.contact = build_workload(
+            args.workload, args.small, *dev_classes)
+        self.opts = tb.NewtonOptions(verbose=bool(args.verbose),
+                                     precision="mixed" if method == "mixed" else "fp64")
+        self.method = method
+        self.q = 0
+        self.log = []
+
+    def point(self):
+        """Solve the next bias point; returns (current, converged, h2d, d2h)."""
+        dev = self.dev
+        volts, first = self.sched[self.q % len(self.sched)]
+        self.q += 1
+        if first:
+            dev.solve_equilibrium(self.opts)
+        dev.solve_bias(volts, self.opts)
+        I = dev.terminal_current(self.contact)
+        N = dev.N
+        h2d = 8 * (len(volts) + 3) + (8 * N if any(k.startswith("gate") for k in volts) else 0)
+        self.log.append(dict(dev.last_newton, first=first, I=I))
+        if self.args.verbose:
+            r = dev.last_newton
+            sys.stderr.write(f"  [{self.method}] point {self.q:3d} {volts} first={first} "
+                             f"conv={r['converged']} newton={r['iters']} krylov="
+                             f"{r['krylov_iters']} relres={r['relres']:.1e} I={I:.9e}\n")
+            sys.stderr.flush()
+        return I, dev.last_converged, h2d, 8
+
+
+def timed_points(torch, runner, steps, e2e):
+    """Per-point device latency (CUDA events on the launching stream) and, with
+    e2e, the latency including the host read of the potential field."""
+    lat, lat_e2e, conv, h2d, d2h = [], [], 0, 0, 0
+    for _ in range(steps):
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record()
+        I, ok, hb, db = runner.point()
+        b.record()
+        if e2e:
+            _ = runner.dev.psi
+            db += 8 * runner.dev.N
+        c.record()
+        torch.cuda.synchronize()
+        lat.append(a.elapsed_time(b))
+        lat_e2e.append(a.elapsed_time(c))
+        conv += int(ok)
+        h2d += hb
+        d2h += db
+    return lat, lat_e2e, conv, h2d, d2h
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -175,76 +237,54 @@ def run_ours(args):
     import tcad_b200 as tb
     from tcad_b200 import _lib
     lib = _lib.load()
-    dev, sched, desc, contact = build_workload(args.workload, args.small, tb.Device2D,
-                                               tb.Device3D)
-    opts = tb.NewtonOptions(verbose=bool(args.verbose))
-    dim = dev.dim
-    N = dev.N
-    state = {"q": 0}
-    newton_log = []
-
-    def one_point(e2e):
-        volts, first = sched[state["q"] % len(sched)]
-        state["q"] += 1
-        if first:
-            dev.solve_equilibrium(opts)
-        dev.solve_bias(volts, opts)
-        I = dev.terminal_current(contact)
-        h2d = 8 * (len(volts) + 3) + (8 * N if any(k.startswith("gate") for k in volts) else 0)
-        d2h = 8
-        if e2e:
-            _ = dev.psi          # the step's field result back on the host
-            d2h += 8 * N
-        newton_log.append(dict(dev.last_newton, first=first))
-        if args.verbose:
-            r = dev.last_newton
-            sys.stderr.write(f"  point {state['q']:3d} {volts} first={first} conv={r['converged']}"
-                             f" newton={r['iters']} krylov={r['krylov_iters']} "
-                             f"relres={r['relres']:.1e} I={I:.6e}\n")
-            sys.stderr.flush()
-        return I, dev.last_converged, h2d, d2h
+    classes = (tb.Device2D, tb.Device3D)
+    chosen = PointRunner(args, args.method, classes)
+    dev = chosen.dev
+    dim, N = dev.dim, dev.N
 
     for _ in range(args.warmup):
-        one_point(True)
-    newton_log.clear()
+        chosen.point()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 2)]
     L0 = lib.tcad_launch_count()
-    lat_dev, lat_e2e, conv, h2d_tot, d2h_tot = [], [], 0, 0, 0
     with Clocks(local) as clk:
         t_wall = time.perf_counter()
-        ev[0].record()
-        for q in range(args.steps):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            c = torch.cuda.Event(enable_timing=True)
-            a.record()
-            I, ok, h2d, d2h = one_point(False)
-            b.record()
-            _ = dev.psi                 # host read of the field (e2e leg)
-            c.record()
-            torch.cuda.synchronize()
-            lat_dev.append(a.elapsed_time(b))
-            lat_e2e.append(a.elapsed_time(c))
-            conv += int(ok)
-            h2d_tot += h2d
-            d2h_tot += d2h + 8 * N
-        ev[1].record()
+        lat, lat_e2e, conv, h2d_tot, d2h_tot = timed_points(torch, chosen, args.steps, True)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t_wall
     launches = lib.tcad_launch_count() - L0
-    t_dev = sum(lat_dev) / 1e3
-    t_e2e = ev[0].elapsed_time(ev[1]) / 1e3
+    t_dev = sum(lat) / 1e3
+    t_e2e = sum(lat_e2e) / 1e3
+    pts_chosen = chosen.log[args.warmup:]
+
+    # the plain FP64 path on the same points: its throughput, and the
+    # reference currents for the chosen path's 1e-6 check
+    plain_lat = None
+    if args.method != "fp64":
+        plain = PointRunner(args, "fp64", classes)
+        for _ in range(args.warmup):
+            plain.point()
+        plain_lat, _, plain_conv, _, _ = timed_points(torch, plain, args.steps, False)
+        pts_plain = plain.log[args.warmup:]
+        errs = [abs(c["I"] - p["I"]) / max(abs(p["I"]), 1e-300)
+                for c, p in zip(pts_chosen, pts_plain)]
+        ok_pts = sum(1 for c, e in zip(pts_chosen, errs) if c["converged"] and e <= 1e-6)
+        del plain
+    else:
+        errs = [0.0] * len(pts_chosen)
+        ok_pts = conv
+        plain_conv = conv
+
     if world > 1:
         tt = torch.tensor([t_dev, t_e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_dev, t_e2e = float(tt[0]), float(tt[1])
-        cc = torch.tensor([conv], device="cuda", dtype=torch.float64)
+        cc = torch.tensor([ok_pts], device="cuda", dtype=torch.float64)
         dist.all_reduce(cc, op=dist.ReduceOp.SUM)
-        conv_all = int(cc.item())
+        ok_all = int(cc.item())
     else:
-        conv_all = conv
+        ok_all = ok_pts
 
     # ---- live roofline of the dominant kernel (block SpMV on the last J) and
     # of the assembly, CUDA events on the launching stream
@@ -265,9 +305,8 @@ def run_ours(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / reps
 
-    # the scaled operator needs D^-1 blocks: re-assemble and set up once
     pk.assemble(_lib.MODE_ELIMINATE)
-    st = torch.zeros(1, dtype=torch.int32, device=pk.device)
+    st = torch.zeros(max(1, len(pk.setups)), dtype=torch.int32, device=pk.device)
     lib.tcad_block_jacobi_setup(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(st), sp)
     t_spmv = time_kernel(lambda: lib.tcad_block_spmv(pk.pref, _lib.ptr(pk.J), _lib.ptr(x),
                                                      _lib.ptr(y), sp), 50)
@@ -279,30 +318,34 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     ach_spmv = BYTES_SPMV[dim] * N / t_spmv / 1e9
     ach_asm = BYTES_ASM[dim] * N / t_asm / 1e9
-    tr = load_traffic(f"spmv{dim}d_{args.workload}")
 
     res = {}
     if rank == 0:
-        pts = [r for r in newton_log]
-        nn = [r["iters"] for r in pts]
-        kk = [r["krylov_iters"] for r in pts]
-        value = conv_all / t_dev
+        nn = [r["iters"] for r in pts_chosen]
+        kk = [r["krylov_iters"] for r in pts_chosen]
+        value = ok_all / t_dev
+        method_desc = {"mixed": "mixed precision: FP64 fused SG assembly, residual, Newton and "
+                                "convergence test; FP32 node-block-scaled BiCGStab inside FP64 "
+                                "iterative refinement; inexact-Newton forcing",
+                       "fp64": "plain FP64: fused SG assembly, node-block-scaled BiCGStab, "
+                               "damped Newton"}[args.method]
         res = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (FP32 inner Krylov)" if args.method == "mixed" else "f64",
             "data": "synthetic device (analytic doping profiles, explicit mesh)",
-            "config": {"workload": desc, "method": "plain FP64 GPU path: fused SG assembly, "
-                       "node-block-scaled BiCGStab, damped Newton (+1 polishing step)",
+            "config": {"workload": chosen.desc, "method": method_desc + " (+1 polishing Newton step)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (J alone is "
                              f"{8 * _lib.NE[dim] * N / 1e6:.0f} MB)"},
-            "p50_ms": statistics.median(lat_dev),
-            "p99_ms": float(np.percentile(lat_dev, 99)),
-            "converged_points": conv_all, "points": args.steps * world,
+            "p50_ms": statistics.median(lat), "p99_ms": float(np.percentile(lat, 99)),
+            "converged_points": conv, "points_within_1e-6_of_plain_fp64": ok_pts,
+            "points": args.steps * world,
+            "max_rel_current_err_vs_plain_fp64": float(max(errs)) if errs else None,
             "newton_iters_mean": float(np.mean(nn)), "krylov_iters_mean": float(np.mean(kk)),
-            "e2e": {"value": conv_all / t_e2e, "unit": UNIT,
+            "e2e": {"value": ok_all / t_e2e, "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d_tot / args.steps),
                     "d2h_bytes_per_step": int(d2h_tot / args.steps),
                     "p50_ms": statistics.median(lat_e2e),
@@ -312,7 +355,8 @@ def run_ours(args):
                          "unit": "GB/s", "frac": ach_spmv / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "bytes_per_launch": BYTES_SPMV[dim] * N,
-                         "launch_ms": t_spmv * 1e3, "traffic": tr},
+                         "launch_ms": t_spmv * 1e3,
+                         "traffic": load_traffic(f"spmv{dim}d_{args.workload}")},
             "roofline_assembly": {"kernel": "k_sg_assemble", "bound": "hbm",
                                   "achieved": ach_asm, "peak": peak, "unit": "GB/s",
                                   "frac": ach_asm / peak,
@@ -323,6 +367,13 @@ def run_ours(args):
             "clocks": clk.summary(),
             "wall_s": wall,
         }
+        if plain_lat is not None:
+            res["plain_fp64_gpu"] = {
+                "value": plain_conv / (sum(plain_lat) / 1e3), "unit": UNIT,
+                "p50_ms": statistics.median(plain_lat),
+                "p99_ms": float(np.percentile(plain_lat, 99)),
+                "converged_points": plain_conv}
+            res["chosen_over_plain"] = value / res["plain_fp64_gpu"]["value"]
         if world == 1 and not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(dev, args, nn, kk)
     if world > 1:

@@ -248,7 +248,9 @@ typedef struct tcad_newton_opts {
   int32_t polish;        /* extra Newton steps after the update test passes */
   double eta_max;        /* forcing: loosest Krylov tolerance of an early step */
   int32_t forcing;       /* 0: every step at rtol; 1: eta_k = clamp(0.1 err_{k-1}, rtol, eta_max) */
-  int32_t pad;
+  int32_t precision;     /* 64: FP64 Krylov; 32: FP32 Krylov on an FP32 copy of the scaled
+                            operator inside FP64 iterative refinement (residual, Newton,
+                            convergence test stay FP64) */
 } tcad_newton_opts_t;
 
 /* Per-instance result of a Newton solve (host memory). */

@@ -55,7 +55,7 @@ class NewtonOpts(ctypes.Structure):
                 ("rtol", ctypes.c_double), ("dens_floor", ctypes.c_double),
                 ("verbose", ctypes.c_int32), ("polish", ctypes.c_int32),
                 ("eta_max", ctypes.c_double), ("forcing", ctypes.c_int32),
-                ("pad", ctypes.c_int32)]
+                ("precision", ctypes.c_int32)]
 
 
 class NewtonResult(ctypes.Structure):

@@ -24,7 +24,7 @@ struct NodeVals {
 __device__ __forceinline__ int nb(int d, int m) { return 9 + 5 * d + m; }
 
 template <int DIM>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, 3)
 k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
               const double* __restrict__ nn, const double* __restrict__ pp,
               double* __restrict__ F, double* __restrict__ J, int mode) {
@@ -139,19 +139,20 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
     }
     __syncthreads();
 
-    // ---- assemble the own node's row block
+    // ---- assemble the own node's row block.  Each neighbour block is
+    // streamed to HBM as soon as it is known (no per-node entry array in
+    // registers, so several tiles stay resident per SM).
     if (own) {
       const int64_t k = plane + (int64_t)j * g.nx + i;
       const uint8_t flag = s_flag[ty + 1][tx + 1];
-      double Fv[3];
-      double Jv[NE];
-#pragma unroll
-      for (int e = 0; e < NE; ++e) Jv[e] = 0.0;
+      double* __restrict__ Jk = J + k;
+      auto st = [&](int e, double v) { Jk[(int64_t)e * NN] = v; };
       if (flag & TCAD_BC_CONTACT) {
-        Fv[0] = cur.psi - pk.bc_psi0[k];
-        Fv[1] = cur.n - pk.bc_n0[k];
-        Fv[2] = cur.p - pk.bc_p0[k];
-        Jv[0] = 1.0; Jv[4] = 1.0; Jv[8] = 1.0;
+        F[k] = cur.psi - pk.bc_psi0[k];
+        F[NN + k] = cur.n - pk.bc_n0[k];
+        F[2 * NN + k] = cur.p - pk.bc_p0[k];
+#pragma unroll
+        for (int e = 0; e < NE; ++e) st(e, (e == 0 || e == 4 || e == 8) ? 1.0 : 0.0);
       } else {
         const double dvx = pk.dv[0][ax0 + i], dvy = pk.dv[1][ay0 + j];
         const double dvz = DIM == 3 ? pk.dv[2][az0 + kz] : 1.0;
@@ -165,24 +166,32 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
         const Edge& E = s_ex[ty][tx + 1];
         const Edge& S = s_ey[ty][tx];
         const Edge& N = s_ey[ty + 1][tx];
+        const double hW = vW ? pk.h[0][ax0 + i - 1] : 1.0, hE = vE ? pk.h[0][ax0 + i] : 1.0;
+        const double hS = vS ? pk.h[1][ay0 + j - 1] : 1.0, hN = vN ? pk.h[1][ay0 + j] : 1.0;
+        const double hD = vD ? pk.h[2][az0 + kz - 1] : 1.0, hU = vU ? pk.h[2][az0 + kz] : 1.0;
         // divergences: div[lo] += f; div[hi] -= f  (device2d.py:1512-1525)
-        double dx0 = 0.0, dx1 = 0.0, dx2 = 0.0, dy0 = 0.0, dy1 = 0.0, dy2 = 0.0;
-        double dz0 = 0.0, dz1 = 0.0, dz2 = 0.0;
-        if (vE) { dx0 = dx0 + E.f; dx1 = dx1 + E.Jn; dx2 = dx2 + E.Jp; }
-        if (vW) { dx0 = dx0 - W.f; dx1 = dx1 - W.Jn; dx2 = dx2 - W.Jp; }
-        if (vN) { dy0 = dy0 + N.f; dy1 = dy1 + N.Jn; dy2 = dy2 + N.Jp; }
-        if (vS) { dy0 = dy0 - S.f; dy1 = dy1 - S.Jn; dy2 = dy2 - S.Jp; }
-        if (vU) { dz0 = dz0 + eU.f; dz1 = dz1 + eU.Jn; dz2 = dz2 + eU.Jp; }
-        if (vD) { dz0 = dz0 - eD.f; dz1 = dz1 - eD.Jn; dz2 = dz2 - eD.Jp; }
+        double f0, f1, f2;
+        {
+          double dx0 = 0.0, dx1 = 0.0, dx2 = 0.0, dy0 = 0.0, dy1 = 0.0, dy2 = 0.0;
+          if (vE) { dx0 = dx0 + E.f; dx1 = dx1 + E.Jn; dx2 = dx2 + E.Jp; }
+          if (vW) { dx0 = dx0 - W.f; dx1 = dx1 - W.Jn; dx2 = dx2 - W.Jp; }
+          if (vN) { dy0 = dy0 + N.f; dy1 = dy1 + N.Jn; dy2 = dy2 + N.Jp; }
+          if (vS) { dy0 = dy0 - S.f; dy1 = dy1 - S.Jn; dy2 = dy2 - S.Jp; }
+          f0 = fx * dx0 + fy * dy0;
+          f1 = fx * dx1 + fy * dy1;
+          f2 = fx * dx2 + fy * dy2;
+          if (DIM == 3) {
+            double dz0 = 0.0, dz1 = 0.0, dz2 = 0.0;
+            if (vU) { dz0 = dz0 + eU.f; dz1 = dz1 + eU.Jn; dz2 = dz2 + eU.Jp; }
+            if (vD) { dz0 = dz0 - eD.f; dz1 = dz1 - eD.Jn; dz2 = dz2 - eD.Jp; }
+            f0 = f0 + fz * dz0; f1 = f1 + fz * dz1; f2 = f2 + fz * dz2;
+          }
+        }
         double Rs, dRsn, dRsp;
         recomb(cur.n, cur.p, pk.nie[k], pk.tau_n[k], pk.tau_p[k], par, Rs, dRsn, dRsp);
-        double f0 = fx * dx0 + fy * dy0;
-        double f1 = fx * dx1 + fy * dy1;
-        double f2 = fx * dx2 + fy * dy2;
-        if (DIM == 3) { f0 = f0 + fz * dz0; f1 = f1 + fz * dz1; f2 = f2 + fz * dz2; }
-        Fv[0] = f0 - dV * (cur.n - cur.p - pk.C[k]);
-        Fv[1] = f1 - Rs * dV;
-        Fv[2] = f2 + Rs * dV;
+        double F0 = f0 - dV * (cur.n - cur.p - pk.C[k]);
+        double F1 = f1 - Rs * dV;
+        double F2 = f2 + Rs * dV;
         // diagonal block, summed in the reference's stamp order per axis
         // (low-role edge first, then high-role edge)
         double d00 = 0.0, d10 = 0.0, d11 = 0.0, d20 = 0.0, d22 = 0.0;
@@ -200,76 +209,61 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
           d20 = d20 + (-(face * e.ppsi));
           d22 = d22 + (-face) * e.phi;
         };
-        // Poisson row entries come first in the COO (x then y then z), the
-        // continuity rows interleave psi/n stamps per axis; each diagonal
-        // entry only collects one kind, so per-entry order is axis by axis.
-        if (vE) lo_role(E, fx, pk.h[0][ax0 + i]);
-        if (vW) hi_role(W, fx, pk.h[0][ax0 + i - 1]);
-        if (vN) lo_role(N, fy, pk.h[1][ay0 + j]);
-        if (vS) hi_role(S, fy, pk.h[1][ay0 + j - 1]);
-        if (vU) lo_role(eU, fz, pk.h[2][az0 + kz]);
-        if (vD) hi_role(eD, fz, pk.h[2][az0 + kz - 1]);
+        if (vE) lo_role(E, fx, hE);
+        if (vW) hi_role(W, fx, hW);
+        if (vN) lo_role(N, fy, hN);
+        if (vS) hi_role(S, fy, hS);
+        if (DIM == 3) {
+          if (vU) lo_role(eU, fz, hU);
+          if (vD) hi_role(eD, fz, hD);
+        }
         d11 = d11 + (-dRsn) * dV;
         d22 = d22 + dRsp * dV;
-        Jv[0] = d00; Jv[1] = -dV; Jv[2] = dV;
-        Jv[3] = d10; Jv[4] = d11; Jv[5] = (-dRsp) * dV;
-        Jv[6] = d20; Jv[7] = dRsn * dV; Jv[8] = d22;
-        // off-diagonal blocks
-        auto put_lo = [&](int d, const Edge& e, double face, double h) {  // nbr = high end
-          Jv[nb(d, 0)] = face / h;
-          Jv[nb(d, 1)] = face * e.npsi;
-          Jv[nb(d, 2)] = face * e.nhi;
-          Jv[nb(d, 3)] = face * e.ppsi;
-          Jv[nb(d, 4)] = face * e.phi;
-        };
-        auto put_hi = [&](int d, const Edge& e, double face, double h) {  // nbr = low end
-          Jv[nb(d, 0)] = face / h;
-          Jv[nb(d, 1)] = face * e.npsi;
-          Jv[nb(d, 2)] = (-face) * e.nlo;
-          Jv[nb(d, 3)] = face * e.ppsi;
-          Jv[nb(d, 4)] = (-face) * e.plo;
-        };
-        if (vW) put_hi(0, W, fx, pk.h[0][ax0 + i - 1]);
-        if (vE) put_lo(1, E, fx, pk.h[0][ax0 + i]);
-        if (vS) put_hi(2, S, fy, pk.h[1][ay0 + j - 1]);
-        if (vN) put_lo(3, N, fy, pk.h[1][ay0 + j]);
-        if (DIM == 3) {
-          if (vD) put_hi(4, eD, fz, pk.h[2][az0 + kz - 1]);
-          if (vU) put_lo(5, eU, fz, pk.h[2][az0 + kz]);
-        }
         if (flag & TCAD_BC_GATE) {  // oxide Robin term (device2d.py:1624-1637)
           const double gk = pk.gate_k[k];
-          Fv[0] = Fv[0] + gk * (pk.gate_v[k] - (cur.psi - pk.gate_b[k]));
-          Jv[0] = Jv[0] + (-gk);
+          F0 = F0 + gk * (pk.gate_v[k] - (cur.psi - pk.gate_b[k]));
+          d00 = d00 + (-gk);
         }
-        if (mode == TCAD_MODE_ELIMINATE) {
-          // fold contact neighbours' known updates into F, empty the column
-          auto fold = [&](int d, bool valid, uint8_t nflag, int64_t m) {
-            if (!valid || !(nflag & TCAD_BC_CONTACT)) return;
-            const double g0 = psi[m] - pk.bc_psi0[m];
-            const double g1 = nn[m] - pk.bc_n0[m];
-            const double g2 = pp[m] - pk.bc_p0[m];
-            Fv[0] = Fv[0] - Jv[nb(d, 0)] * g0;
-            Fv[1] = Fv[1] - (Jv[nb(d, 1)] * g0 + Jv[nb(d, 2)] * g1);
-            Fv[2] = Fv[2] - (Jv[nb(d, 3)] * g0 + Jv[nb(d, 4)] * g2);
-#pragma unroll
-            for (int q = 0; q < 5; ++q) Jv[nb(d, q)] = 0.0;
-          };
-          fold(0, vW, s_flag[ty + 1][tx], k - 1);
-          fold(1, vE, s_flag[ty + 1][tx + 2], k + 1);
-          fold(2, vS, s_flag[ty][tx + 1], k - g.nx);
-          fold(3, vN, s_flag[ty + 2][tx + 1], k + g.nx);
-          if (DIM == 3) {
-            fold(4, vD, vD ? pk.bcflag[k - sxy] : 0, k - sxy);
-            fold(5, vU, vU ? pk.bcflag[k + sxy] : 0, k + sxy);
+        st(0, d00); st(1, -dV); st(2, dV);
+        st(3, d10); st(4, d11); st(5, (-dRsp) * dV);
+        st(6, d20); st(7, dRsn * dV); st(8, d22);
+        // off-diagonal blocks, W,E,S,N,D,U; in ELIMINATE mode a contact
+        // neighbour's known update is folded into F and its block emptied
+        const bool elim = mode == TCAD_MODE_ELIMINATE;
+        auto emit = [&](int d, bool valid, bool lo_end, const Edge& e, double face, double h,
+                        uint8_t nflag, int64_t m) {
+          double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+          if (valid) {
+            a0 = face / h;
+            a1 = face * e.npsi;
+            a3 = face * e.ppsi;
+            if (lo_end) { a2 = face * e.nhi; a4 = face * e.phi; }          // nbr = high end
+            else { a2 = (-face) * e.nlo; a4 = (-face) * e.plo; }           // nbr = low end
+            if (elim && (nflag & TCAD_BC_CONTACT)) {
+              const double g0 = psi[m] - pk.bc_psi0[m];
+              const double g1 = nn[m] - pk.bc_n0[m];
+              const double g2 = pp[m] - pk.bc_p0[m];
+              F0 = F0 - a0 * g0;
+              F1 = F1 - (a1 * g0 + a2 * g1);
+              F2 = F2 - (a3 * g0 + a4 * g2);
+              a0 = a1 = a2 = a3 = a4 = 0.0;
+            }
           }
+          st(nb(d, 0), a0); st(nb(d, 1), a1); st(nb(d, 2), a2); st(nb(d, 3), a3);
+          st(nb(d, 4), a4);
+        };
+        emit(0, vW, false, W, fx, hW, s_flag[ty + 1][tx], k - 1);
+        emit(1, vE, true, E, fx, hE, s_flag[ty + 1][tx + 2], k + 1);
+        emit(2, vS, false, S, fy, hS, s_flag[ty][tx + 1], k - g.nx);
+        emit(3, vN, true, N, fy, hN, s_flag[ty + 2][tx + 1], k + g.nx);
+        if (DIM == 3) {
+          emit(4, vD, false, eD, fz, hD, vD ? pk.bcflag[k - sxy] : 0, k - sxy);
+          emit(5, vU, true, eU, fz, hU, vU ? pk.bcflag[k + sxy] : 0, k + sxy);
         }
+        F[k] = F0;
+        F[NN + k] = F1;
+        F[2 * NN + k] = F2;
       }
-      F[k] = Fv[0];
-      F[NN + k] = Fv[1];
-      F[2 * NN + k] = Fv[2];
-#pragma unroll
-      for (int e = 0; e < NE; ++e) J[(int64_t)e * NN + k] = Jv[e];
     }
     __syncthreads();
     if (DIM == 3) {

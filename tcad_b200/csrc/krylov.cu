@@ -130,23 +130,24 @@ k_bj_setup(const tcad_pack_t pk, double* __restrict__ J, double* __restrict__ F,
 
 // y = x + Dinv * (sum_d A_d x_nbr(d))      (SCALED)
 // y = D x + sum_d A_d x_nbr(d)             (raw J, !SCALED)
-template <int DIM, bool SCALED>
-__device__ __forceinline__ void spmv_node(const double* __restrict__ J,
-                                          const double* __restrict__ x, int64_t k,
-                                          int64_t NN, const int64_t* off, int64_t lo,
-                                          int64_t hi, double& y0, double& y1, double& y2) {
-  double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+// T is the storage and arithmetic type (double: plain path; float: the
+// mixed-precision inner solves).
+template <int DIM, bool SCALED, class T>
+__device__ __forceinline__ void spmv_node(const T* __restrict__ J, const T* __restrict__ x,
+                                          int64_t k, int64_t NN, const int64_t* off,
+                                          int64_t lo, int64_t hi, T& y0, T& y1, T& y2) {
+  T t0 = T(0), t1 = T(0), t2 = T(0);
 #pragma unroll
   for (int d = 0; d < 2 * DIM; ++d) {
     const int64_t m = clampi(k + off[d], lo, hi);
     const int e = 9 + 5 * d;
-    const double xs = x[m], xn = x[NN + m], xp = x[2 * NN + m];
+    const T xs = x[m], xn = x[NN + m], xp = x[2 * NN + m];
     t0 += J[(int64_t)e * NN + k] * xs;
     t1 += J[(int64_t)(e + 1) * NN + k] * xs + J[(int64_t)(e + 2) * NN + k] * xn;
     t2 += J[(int64_t)(e + 3) * NN + k] * xs + J[(int64_t)(e + 4) * NN + k] * xp;
   }
-  const double x0 = x[k], x1 = x[NN + k], x2 = x[2 * NN + k];
-  double d[9];
+  const T x0 = x[k], x1 = x[NN + k], x2 = x[2 * NN + k];
+  T d[9];
 #pragma unroll
   for (int e = 0; e < 9; ++e) d[e] = J[(int64_t)e * NN + k];
   if (SCALED) {
@@ -171,20 +172,24 @@ k_spmv(const tcad_pack_t pk, const double* __restrict__ J, const double* __restr
   const int64_t NN = pk.n_nodes;
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
     double y0, y1, y2;
-    spmv_node<DIM, SCALED>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    spmv_node<DIM, SCALED, double>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
     y[k] = y0; y[NN + k] = y1; y[2 * NN + k] = y2;
   }
 }
 
 // --------------------------------------------------------------------------
 // BiCGStab on A^ (per instance).  Vectors: r, rh (shadow), p, v, s, t; x.
-struct BiVec {
-  double *r, *rh, *p, *v, *s, *t;
+// Scalars and dot products are always FP64.
+template <class T>
+struct BiVecT {
+  T *r, *rh, *p, *v, *s, *t;
 };
+using BiVec = BiVecT<double>;
 
+template <class T>
 __global__ void __launch_bounds__(NT)
-k_bi_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict__ x,
-          BiVec w, KState* ks, double* partial, unsigned* ticket, double rtol, int maxit,
+k_bi_init(const tcad_pack_t pk, const T* __restrict__ b, T* __restrict__ x, BiVecT<T> w,
+          KState* ks, double* partial, unsigned* ticket, double rtol, int maxit,
           const int32_t* __restrict__ pre_status, const double* __restrict__ rtol_inst) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const int64_t NN = pk.n_nodes;
@@ -193,9 +198,9 @@ k_bi_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t q = c * NN + k;
-      const double bv = b[q];
-      x[q] = 0.0; w.r[q] = bv; w.rh[q] = bv; w.p[q] = 0.0; w.v[q] = 0.0;
-      v[0] += bv * bv;
+      const T bv = b[q];
+      x[q] = T(0); w.r[q] = bv; w.rh[q] = bv; w.p[q] = T(0); w.v[q] = T(0);
+      v[0] += (double)bv * (double)bv;
     }
   }
   double tot[1];
@@ -214,31 +219,33 @@ k_bi_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict
 }
 
 // p = r + beta (p - omega v)   (restart: rh = r, p = r)
+template <class T>
 __global__ void __launch_bounds__(NT)
-k_bi_p(const tcad_pack_t pk, BiVec w, const KState* ks) {
+k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const KState s = ks[fb.inst];
   if (!s.active) return;
   const int64_t NN = pk.n_nodes;
+  const T beta = (T)s.beta, omega = (T)s.omega;
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t q = c * NN + k;
-      const double r = w.r[q];
+      const T r = w.r[q];
       if (s.restart) {
         w.rh[q] = r;
         w.p[q] = r;
       } else {
-        w.p[q] = r + s.beta * (w.p[q] - s.omega * w.v[q]);
+        w.p[q] = r + beta * (w.p[q] - omega * w.v[q]);
       }
     }
   }
 }
 
 // v = A^ p, alpha = rho / (rh, v)
-template <int DIM>
+template <int DIM, class T>
 __global__ void __launch_bounds__(NT)
-k_bi_v(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
+k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
        double* partial, unsigned* ticket) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   if (!ks[fb.inst].active) return;
@@ -248,10 +255,10 @@ k_bi_v(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
   const int64_t NN = pk.n_nodes;
   double v[1] = {0.0};
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
-    double y0, y1, y2;
-    spmv_node<DIM, true>(J, w.p, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    T y0, y1, y2;
+    spmv_node<DIM, true, T>(J, w.p, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
     w.v[k] = y0; w.v[NN + k] = y1; w.v[2 * NN + k] = y2;
-    v[0] += w.rh[k] * y0 + w.rh[NN + k] * y1 + w.rh[2 * NN + k] * y2;
+    v[0] += (double)w.rh[k] * y0 + (double)w.rh[NN + k] * y1 + (double)w.rh[2 * NN + k] * y2;
   }
   double tot[1];
   if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
@@ -268,20 +275,22 @@ k_bi_v(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
 }
 
 // s = r - alpha v, (s, s)
+template <class T>
 __global__ void __launch_bounds__(NT)
-k_bi_s(const tcad_pack_t pk, BiVec w, KState* ks, double* partial, unsigned* ticket) {
+k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned* ticket) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const KState s0 = ks[fb.inst];
   if (!s0.active) return;
   const int64_t NN = pk.n_nodes;
+  const T alpha = (T)s0.alpha;
   double v[1] = {0.0};
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t q = c * NN + k;
-      const double sv = w.r[q] - s0.alpha * w.v[q];
+      const T sv = w.r[q] - alpha * w.v[q];
       w.s[q] = sv;
-      v[0] += sv * sv;
+      v[0] += (double)sv * (double)sv;
     }
   }
   double tot[1];
@@ -293,9 +302,9 @@ k_bi_s(const tcad_pack_t pk, BiVec w, KState* ks, double* partial, unsigned* tic
 }
 
 // t = A^ s, omega = (t, s) / (t, t)
-template <int DIM>
+template <int DIM, class T>
 __global__ void __launch_bounds__(NT)
-k_bi_t(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
+k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
        double* partial, unsigned* ticket) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   if (!ks[fb.inst].active) return;
@@ -305,11 +314,11 @@ k_bi_t(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
   const int64_t NN = pk.n_nodes;
   double v[2] = {0.0, 0.0};
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
-    double y0, y1, y2;
-    spmv_node<DIM, true>(J, w.s, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    T y0, y1, y2;
+    spmv_node<DIM, true, T>(J, w.s, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
     w.t[k] = y0; w.t[NN + k] = y1; w.t[2 * NN + k] = y2;
-    v[0] += y0 * w.s[k] + y1 * w.s[NN + k] + y2 * w.s[2 * NN + k];
-    v[1] += y0 * y0 + y1 * y1 + y2 * y2;
+    v[0] += (double)y0 * w.s[k] + (double)y1 * w.s[NN + k] + (double)y2 * w.s[2 * NN + k];
+    v[1] += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
   }
   double tot[2];
   if (Reduce<2>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
@@ -319,24 +328,26 @@ k_bi_t(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
 }
 
 // x += alpha p + omega s; r = s - omega t; rho = (rh, r); (r, r)
+template <class T>
 __global__ void __launch_bounds__(NT)
-k_bi_x(const tcad_pack_t pk, double* __restrict__ x, BiVec w, KState* ks, double* partial,
+k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double* partial,
        unsigned* ticket) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const KState s0 = ks[fb.inst];
   if (!s0.active) return;
   const int64_t NN = pk.n_nodes;
+  const T alpha = (T)s0.alpha, omega = (T)s0.omega;
   double v[3] = {0.0, 0.0, 0.0};
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t q = c * NN + k;
-      x[q] = x[q] + s0.alpha * w.p[q] + s0.omega * w.s[q];
-      const double r = w.s[q] - s0.omega * w.t[q];
+      x[q] = x[q] + alpha * w.p[q] + omega * w.s[q];
+      const T r = w.s[q] - omega * w.t[q];
       w.r[q] = r;
       const double rh = w.rh[q];
       v[0] += rh * r;
-      v[1] += r * r;
+      v[1] += (double)r * r;
       v[2] += rh * rh;
     }
   }
@@ -368,11 +379,11 @@ k_bi_x(const tcad_pack_t pk, double* __restrict__ x, BiVec w, KState* ks, double
 
 // true scaled residual r = b - A^ x, its norm into the state; re-arm a restart
 // when it is not within the tolerance the recursive residual claimed
-template <int DIM>
+template <int DIM, class T>
 __global__ void __launch_bounds__(NT)
-k_true_resid(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ b,
-             const double* __restrict__ x, double* __restrict__ r, KState* ks,
-             double* partial, unsigned* ticket, int rearm) {
+k_true_resid(const tcad_pack_t pk, const T* __restrict__ J, const T* __restrict__ b,
+             const T* __restrict__ x, T* __restrict__ r, KState* ks, double* partial,
+             unsigned* ticket, int rearm) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
@@ -380,11 +391,11 @@ k_true_resid(const tcad_pack_t pk, const double* __restrict__ J, const double* _
   const int64_t NN = pk.n_nodes;
   double v[1] = {0.0};
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
-    double y0, y1, y2;
-    spmv_node<DIM, true>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
-    const double a0 = b[k] - y0, a1 = b[NN + k] - y1, a2 = b[2 * NN + k] - y2;
+    T y0, y1, y2;
+    spmv_node<DIM, true, T>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    const T a0 = b[k] - y0, a1 = b[NN + k] - y1, a2 = b[2 * NN + k] - y2;
     r[k] = a0; r[NN + k] = a1; r[2 * NN + k] = a2;
-    v[0] += a0 * a0 + a1 * a1 + a2 * a2;
+    v[0] += (double)a0 * a0 + (double)a1 * a1 + (double)a2 * a2;
   }
   double tot[1];
   if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
@@ -587,6 +598,79 @@ k_slaved(const tcad_pack_t pk, const double* __restrict__ psi, double* __restric
 }
 
 // --------------------------------------------------------------------------
+// mixed precision: FP32 copy of the block-scaled operator, FP64 iterative
+// refinement around FP32 BiCGStab (the residual always uses the FP64 A^)
+__global__ void __launch_bounds__(NT)
+k_to_f32(const tcad_pack_t pk, int ne, const double* __restrict__ J, float* __restrict__ J32) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const int64_t NN = pk.n_nodes;
+  for (int e = 0; e < ne; ++e)
+    for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT)
+      J32[(int64_t)e * NN + k] = (float)J[(int64_t)e * NN + k];
+}
+
+// x = 0, r32 = (float) b, ||b||^2
+__global__ void __launch_bounds__(NT)
+k_ir_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict__ x,
+          float* __restrict__ r32, KState* irs, double* partial, unsigned* ticket) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const int64_t NN = pk.n_nodes;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t q = c * NN + k;
+      const double bv = b[q];
+      x[q] = 0.0;
+      r32[q] = (float)bv;
+      v[0] += bv * bv;
+    }
+  }
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    irs[fb.inst].bb = tot[0];
+    irs[fb.inst].rr = tot[0];
+  }
+}
+
+// x += d32 for the instances still refining
+__global__ void __launch_bounds__(NT)
+k_ir_axpy(const tcad_pack_t pk, double* __restrict__ x, const float* __restrict__ d,
+          const int32_t* __restrict__ pre_status) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  if (pre_status[fb.inst] != TCAD_OK) return;
+  const int64_t NN = pk.n_nodes;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[c * NN + k] += (double)d[c * NN + k];
+}
+
+// r = b - A^ x in FP64 (FP64 operator), r32 = (float) r, ||r||^2
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_ir_resid(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ b,
+           const double* __restrict__ x, float* __restrict__ r32, KState* irs,
+           const int32_t* __restrict__ pre_status, double* partial, unsigned* ticket) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  if (pre_status[fb.inst] != TCAD_OK) return;
+  const Inst g = load_inst(pk, fb.inst);
+  int64_t off[6];
+  nbr_offsets(g, off);
+  const int64_t NN = pk.n_nodes;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    double y0, y1, y2;
+    spmv_node<DIM, true, double>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    const double a0 = b[k] - y0, a1 = b[NN + k] - y1, a2 = b[2 * NN + k] - y2;
+    r32[k] = (float)a0; r32[NN + k] = (float)a1; r32[2 * NN + k] = (float)a2;
+    v[0] += a0 * a0 + a1 * a1 + a2 * a2;
+  }
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
+    irs[fb.inst].rr = tot[0];
+}
+
+// --------------------------------------------------------------------------
 // workspace carving
 struct Carve {
   char* base;
@@ -613,6 +697,38 @@ struct Work {
   size_t bytes;
 };
 
+// FP32 extension of the workspace (mixed-precision Newton), carved after Work
+struct Work32 {
+  BiVecT<float> bi;
+  float* J32;
+  float* r32;
+  float* d32;
+  KState* irs;
+  double* eta_in;
+  int32_t* pre;
+  size_t bytes;
+};
+
+static Work32 carve32(const tcad_pack_t* pk, void* base) {
+  Carve c{reinterpret_cast<char*>(base), 0, 0};
+  Work32 w;
+  const size_t v3 = 3 * (size_t)pk->n_nodes;
+  w.bi.r = c.take<float>(v3);
+  w.bi.rh = c.take<float>(v3);
+  w.bi.p = c.take<float>(v3);
+  w.bi.v = c.take<float>(v3);
+  w.bi.s = c.take<float>(v3);
+  w.bi.t = c.take<float>(v3);
+  w.J32 = c.take<float>((size_t)(pk->dim == 2 ? TCAD_NE2 : TCAD_NE3) * pk->n_nodes);
+  w.r32 = c.take<float>(v3);
+  w.d32 = c.take<float>(v3);
+  w.irs = c.take<KState>(pk->n_inst);
+  w.eta_in = c.take<double>(pk->n_inst);
+  w.pre = c.take<int32_t>(pk->n_inst);
+  w.bytes = c.used;
+  return w;
+}
+
 static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   Carve c{reinterpret_cast<char*>(base), 0, cap};
   Work w;
@@ -638,14 +754,15 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   return w;
 }
 
-static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double* b,
-                           double* x, double rtol, int maxiter, const Work& w,
-                           const int32_t* pre_status, std::vector<KState>& hks,
-                           cudaStream_t s, const double* rtol_inst = nullptr) {
+template <class T>
+static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x, double rtol,
+                             int maxiter, const BiVecT<T>& bi, const Work& w,
+                             const int32_t* pre_status, std::vector<KState>& hks,
+                             cudaStream_t s, const double* rtol_inst) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
-  k_bi_init<<<nb, NT, 0, s>>>(*pk, b, x, w.bi, w.ks, w.partial, w.ticket, rtol, maxiter,
+  k_bi_init<<<nb, NT, 0, s>>>(*pk, b, x, bi, w.ks, w.partial, w.ticket, rtol, maxiter,
                               pre_status, rtol_inst);
   note_launch();
   TCAD_LAUNCH_CHECK();
@@ -655,21 +772,21 @@ static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double*
   int rechecks = 0;
   for (;;) {
     for (int q = 0; q < check; ++q) {
-      k_bi_p<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks);
+      k_bi_p<<<nb, NT, 0, s>>>(*pk, bi, w.ks);
       note_launch();
       if (pk->dim == 2)
-        k_bi_v<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+        k_bi_v<2><<<nb, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket);
       else
-        k_bi_v<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+        k_bi_v<3><<<nb, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket);
       note_launch();
-      k_bi_s<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks, w.partial, w.ticket);
+      k_bi_s<<<nb, NT, 0, s>>>(*pk, bi, w.ks, w.partial, w.ticket);
       note_launch();
       if (pk->dim == 2)
-        k_bi_t<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+        k_bi_t<2><<<nb, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket);
       else
-        k_bi_t<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+        k_bi_t<3><<<nb, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket);
       note_launch();
-      k_bi_x<<<nb, NT, 0, s>>>(*pk, x, w.bi, w.ks, w.partial, w.ticket);
+      k_bi_x<<<nb, NT, 0, s>>>(*pk, x, bi, w.ks, w.partial, w.ticket);
       note_launch();
     }
     TCAD_LAUNCH_CHECK();
@@ -684,9 +801,9 @@ static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double*
       // re-armed from the true residual (bounded number of re-checks)
       const int rearm = rechecks < 8 ? 1 : 0;
       if (pk->dim == 2)
-        k_true_resid<2><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w.ks, w.partial, w.ticket, rearm);
+        k_true_resid<2><<<nb, NT, 0, s>>>(*pk, J, b, x, bi.r, w.ks, w.partial, w.ticket, rearm);
       else
-        k_true_resid<3><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w.ks, w.partial, w.ticket, rearm);
+        k_true_resid<3><<<nb, NT, 0, s>>>(*pk, J, b, x, bi.r, w.ks, w.partial, w.ticket, rearm);
       note_launch();
       TCAD_LAUNCH_CHECK();
       TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState) * ni,
@@ -698,6 +815,86 @@ static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double*
     }
     if (done_iters > 64) check = 16;
     if (done_iters > 1024) check = 32;
+  }
+  return TCAD_OK;
+}
+
+static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double* b,
+                           double* x, double rtol, int maxiter, const Work& w,
+                           const int32_t* pre_status, std::vector<KState>& hks,
+                           cudaStream_t s, const double* rtol_inst = nullptr) {
+  return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, w.bi, w, pre_status, hks, s,
+                                   rtol_inst);
+}
+
+// FP64 iterative refinement of A^ x = b (both FP64) with FP32 BiCGStab inner
+// solves on the FP32 copy of A^: per instance, stop when the FP64 residual is
+// within eta[i] ||b|| (instances whose pre_status is not OK stay idle).  Inner
+// tolerance max(1e-4, min(0.5, eta / current relative residual)).  Returns the
+// summed inner iterations, final relative residuals and statuses in res_*.
+static int solve_mixed(const tcad_pack_t* pk, const double* J, const double* b, double* x,
+                       const double* eta, int inner_maxiter, int max_ir, const Work& w,
+                       const Work32& w32, const int32_t* pre_status_host,
+                       std::vector<KState>& hks, int32_t* res_iters, int32_t* res_status,
+                       double* res_relres, cudaStream_t s) {
+  const unsigned nb = (unsigned)pk->n_flat;
+  const int ni = pk->n_inst;
+  const int ne = pk->dim == 2 ? TCAD_NE2 : TCAD_NE3;
+  k_to_f32<<<nb, NT, 0, s>>>(*pk, ne, J, w32.J32);
+  note_launch();
+  TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
+  k_ir_init<<<nb, NT, 0, s>>>(*pk, b, x, w32.r32, w32.irs, w.partial, w.ticket);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  std::vector<KState> irs(ni);
+  std::vector<int32_t> pre(ni);
+  std::vector<double> eta_in(ni);
+  for (int i = 0; i < ni; ++i) {
+    res_iters[i] = 0;
+    res_status[i] = pre_status_host[i];
+    res_relres[i] = 1.0;
+  }
+  for (int ir = 0;; ++ir) {
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(irs.data(), w32.irs, sizeof(KState) * ni,
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int i = 0; i < ni; ++i) {
+      if (pre_status_host[i] != TCAD_OK) { pre[i] = -1; continue; }
+      const double rel = irs[i].bb > 0.0 ? std::sqrt(irs[i].rr / irs[i].bb) : 0.0;
+      res_relres[i] = rel;
+      const bool done = !(rel > eta[i]) || res_status[i] == TCAD_ERR_NONFINITE ||
+                        res_status[i] == TCAD_ERR_BREAKDOWN || !std::isfinite(rel);
+      if (!done && ir >= max_ir) { res_status[i] = TCAD_ERR_NOCONV; pre[i] = -1; continue; }
+      if (!done) res_status[i] = TCAD_OK;
+      pre[i] = done ? -1 : TCAD_OK;
+      eta_in[i] = std::max(1e-4, std::min(0.5, eta[i] / std::max(rel, 1e-300)));
+      any = any || !done;
+    }
+    if (!any) break;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(w32.pre, pre.data(), sizeof(int32_t) * ni,
+                                    cudaMemcpyHostToDevice, s));
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(w32.eta_in, eta_in.data(), sizeof(double) * ni,
+                                    cudaMemcpyHostToDevice, s));
+    int rc = launch_bicgstab_t<float>(pk, w32.J32, w32.r32, w32.d32, 1e-4, inner_maxiter,
+                                      w32.bi, w, w32.pre, hks, s, w32.eta_in);
+    if (rc != TCAD_OK) return rc;
+    for (int i = 0; i < ni; ++i) {
+      if (pre[i] != TCAD_OK) continue;
+      res_iters[i] += hks[i].it;
+      if (hks[i].status == TCAD_ERR_NONFINITE || hks[i].status == TCAD_ERR_BREAKDOWN)
+        res_status[i] = hks[i].status;
+    }
+    k_ir_axpy<<<nb, NT, 0, s>>>(*pk, x, w32.d32, w32.pre);
+    note_launch();
+    if (pk->dim == 2)
+      k_ir_resid<2><<<nb, NT, 0, s>>>(*pk, J, b, x, w32.r32, w32.irs, w32.pre, w.partial,
+                                      w.ticket);
+    else
+      k_ir_resid<3><<<nb, NT, 0, s>>>(*pk, J, b, x, w32.r32, w32.irs, w32.pre, w.partial,
+                                      w.ticket);
+    note_launch();
+    TCAD_LAUNCH_CHECK();
   }
   return TCAD_OK;
 }
@@ -748,7 +945,8 @@ extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, 
   if (!pk) return 0;
   (void)method; (void)restart;
   Work w = carve(pk, nullptr, 0);
-  return w.bytes + 256;
+  Work32 w32 = carve32(pk, nullptr);
+  return w.bytes + w32.bytes + 512;  // FP64 work, then the FP32 extension
 }
 
 extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
@@ -833,6 +1031,12 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   std::vector<unsigned long long> herr(ni);
   std::vector<int32_t> hstat(ni);
   std::vector<int> polish_left(ni, -1);  // -1: not yet converged
+  if (opts->precision != 64 && opts->precision != 32) return TCAD_ERR_ARG;
+  if (opts->precision == 32 && work_bytes < tcad_block_workspace_bytes(pk, 0, 0))
+    return TCAD_ERR_ARG;
+  const Work32 w32 = carve32(pk, reinterpret_cast<char*>(work) + ((w.bytes + 255) & ~(size_t)255));
+  std::vector<int32_t> mix_it(ni), mix_st(ni);
+  std::vector<double> mix_rr(ni);
   std::vector<double> heta(ni, opts->forcing ? std::max(opts->eta_max, opts->rtol) : opts->rtol);
   for (int it = 0; it < opts->max_iter; ++it) {
     int rc = tcad_sg_assemble(pk, psi, n, p, F, J, TCAD_MODE_ELIMINATE, stream);
@@ -851,15 +1055,29 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
                                     cudaMemcpyHostToDevice, s));
     TCAD_CUDA_CHECK(cudaMemcpyAsync(w.eta, heta.data(), sizeof(double) * ni,
                                     cudaMemcpyHostToDevice, s));
-    rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
-                         w.eta);
-    if (rc != TCAD_OK) return rc;
-    // instances whose linear solve broke down / diverged keep their state
-    for (int i = 0; i < ni; ++i) {
-      if (!hact[i]) continue;
-      result[i].krylov_iters += hks[i].it;
-      result[i].status = hks[i].status;
-      result[i].relres = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
+    if (opts->precision == 32) {
+      // FP32 inner Krylov inside FP64 iterative refinement
+      rc = solve_mixed(pk, J, F, du, heta.data(), opts->krylov_maxiter, 30, w, w32,
+                       hstat.data(), hks, mix_it.data(), mix_st.data(), mix_rr.data(), s);
+      if (rc != TCAD_OK) return rc;
+      for (int i = 0; i < ni; ++i) {
+        if (!hact[i]) continue;
+        result[i].krylov_iters += mix_it[i];
+        result[i].status = mix_st[i];
+        result[i].relres = mix_rr[i];
+        hks[i].it = mix_it[i];
+      }
+    } else {
+      rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
+                           w.eta);
+      if (rc != TCAD_OK) return rc;
+      // instances whose linear solve broke down / diverged keep their state
+      for (int i = 0; i < ni; ++i) {
+        if (!hact[i]) continue;
+        result[i].krylov_iters += hks[i].it;
+        result[i].status = hks[i].status;
+        result[i].relres = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
+      }
     }
     TCAD_CUDA_CHECK(cudaMemcpyAsync(active, hact.data(), ni, cudaMemcpyHostToDevice, s));
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));

@@ -87,6 +87,11 @@ class NewtonOptions:
     # every step to linsolve_rtol like the reference's iterative branch.
     forcing: str = "adaptive"
     eta_max: float = 1e-3
+    # GPU-only: "fp64" solves the Newton systems in FP64; "mixed" runs the
+    # Krylov iterations in FP32 on an FP32 copy of the block-scaled Jacobian
+    # inside FP64 iterative refinement -- residual, Newton update and the
+    # convergence test stay FP64, so the converged state is the FP64 one.
+    precision: str = "fp64"
 
     def __post_init__(self):
         if self.precond not in ("auto", "block_jacobi", "schur"):
@@ -99,3 +104,5 @@ class NewtonOptions:
         if self.linsolve not in ("auto", "direct", "gmres", "bicgstab", "gpu_direct",
                                  "petsc", "mumps"):
             raise ValueError(f"unknown linsolve {self.linsolve!r}")
+        if self.precision not in ("fp64", "mixed"):
+            raise ValueError(f"NewtonOptions.precision={self.precision!r}: 'fp64' or 'mixed'")

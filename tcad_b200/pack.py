@@ -467,6 +467,7 @@ class Pack:
         o.polish = 0 if equilibrium else int(getattr(opts, "polish", 0))
         o.forcing = 1 if getattr(opts, "forcing", "fixed") == "adaptive" else 0
         o.eta_max = float(getattr(opts, "eta_max", 1e-3))
+        o.precision = 32 if getattr(opts, "precision", "fp64") == "mixed" and not equilibrium else 64
         return o
 
     def newton(self, opts, active=None):

@@ -127,3 +127,37 @@ def test_diode_c1_sweep():
                 assert np.abs(phi - phr).max() * VT < 1e-8, c
     I = np.array(I)
     assert fx.vec_err(I, g["I"], 1e-9 * np.abs(g["I"]).max()) < TOL_I
+
+
+@pytest.mark.parametrize("name", ["mosfet_small", "trigate_small"])
+def test_mixed_precision_sweep(name):
+    """The mixed-precision Newton (FP32 Krylov on an FP32 copy of the
+    block-scaled Jacobian inside FP64 iterative refinement) converges to the
+    same FP64 discrete solution: psi within 1e-9 V, currents within 1e-6."""
+    import tcad_b200 as tb
+    g = fx.load(name)
+    dev = fx.gpu_device(g)
+    dev.solve_equilibrium()
+    opts = tb.NewtonOptions(precision="mixed")
+    gates = [b for b in dev.bcs if b.startswith("gate")]
+    for v, Iref in zip(g["Vg"], g["I"]):
+        volts = {"drain": float(g["Vd"]), **{gt: float(v) for gt in gates}}
+        dev.solve_bias(volts, opts)
+        assert dev.last_converged
+        tag = "%02d" % int(round(v * 10))
+        assert np.abs(dev.psi.ravel() - g["psi_" + tag]).max() * dev.VT < TOL_PSI_V
+        assert abs(dev.terminal_current("drain") - Iref) <= TOL_I * abs(Iref)
+
+
+def test_mixed_precision_diode_c1():
+    import tcad_b200 as tb
+    g = fx.load("diode_c1")
+    dev = fx.gpu_device(g, material=dict(tau_n0=1e-7, tau_p0=1e-7, tau_Nref=1e300))
+    dev.solve_equilibrium()
+    opts = tb.NewtonOptions(precision="mixed")
+    I = []
+    for V in g["V"]:
+        dev.solve_bias({"anode": float(V)}, opts)
+        assert dev.last_converged, V
+        I.append(dev.terminal_current("anode"))
+    assert fx.vec_err(np.array(I), g["I"], 1e-9 * np.abs(g["I"]).max()) < TOL_I
