@@ -49,6 +49,27 @@ BYTES_ASM = {2: (13 + 32) * 8 + 1, 3: (16 + 42) * 8 + 1}
 TRIGATE_ITERS = {"newton_per_point": 4.0, "krylov_per_newton": 250.0}
 
 
+# The Newton/Krylov methods the bench can time.  "plain" is the reference's
+# iterative semantics on the GPU kernels: every Newton step's BiCGStab solved
+# to the fixed rtol 1e-10 on (dpsi, dn, dp) with node-block Jacobi.
+METHODS = {
+    "plain": dict(precision="fp64", forcing="fixed", krylov_unknowns="absolute"),
+    "fp64": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative"),
+    "mixed": dict(precision="mixed", forcing="adaptive", krylov_unknowns="relative"),
+}
+METHOD_DESC = {
+    "plain": "plain FP64: fused SG assembly, node-block-Jacobi BiCGStab to rtol 1e-10 on "
+             "(dpsi, dn, dp) every Newton step, damped Newton",
+    "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the block-scaled system in "
+            "relative unknowns (dpsi, dn/n, dp/p) with forcing eta_k = clamp(0.1 "
+            "update_{k-1}, 1e-10, 1e-3)",
+    "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
+             "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
+             "relative unknowns, adaptive forcing; per-instance FP64 fallback when an "
+             "FP32-solved step is rejected",
+}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -58,11 +79,9 @@ def parse():
     ap.add_argument("--workload", default="trigate3d", choices=["trigate3d", "diode2d"])
     ap.add_argument("--small", action="store_true", help="down-scaled mesh (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"],
+    ap.add_argument("--method", default="mixed", choices=list(METHODS),
                     help="the timed (chosen) path; the plain FP64 path is always run "
                          "beside it on the same points for the current check")
-    ap.add_argument("--plain-steps", type=int, default=None,
-                    help="points of the plain FP64 comparison run (default: warmup+steps)")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--kernels", action="store_true",
                     help="profiling mode: assembly, block-Jacobi set-up and 20 BiCGStab "
@@ -175,8 +194,7 @@ class PointRunner:
         self.args = args
         self.dev, self.sched, self.desc, self.contact = build_workload(
             args.workload, args.small, *dev_classes)
-        self.opts = tb.NewtonOptions(verbose=bool(args.verbose),
-                                     precision="mixed" if method == "mixed" else "fp64")
+        self.opts = tb.NewtonOptions(verbose=bool(args.verbose), **METHODS[method])
         self.method = method
         self.q = 0
         self.log = []
@@ -200,6 +218,9 @@ class PointRunner:
                              f"{r['krylov_iters']} relres={r['relres']:.1e} I={I:.9e}\n")
             sys.stderr.flush()
         return I, dev.last_converged, h2d, 8
+
+    def release(self):
+        self.dev = None
 
 
 def timed_points(torch, runner, steps, e2e):
@@ -261,20 +282,22 @@ def run_ours(args):
     # the plain FP64 path on the same points: its throughput, and the
     # reference currents for the chosen path's 1e-6 check
     plain_lat = None
-    if args.method != "fp64":
-        plain = PointRunner(args, "fp64", classes)
+    if args.method != "plain":
+        plain = PointRunner(args, "plain", classes)
         for _ in range(args.warmup):
             plain.point()
         plain_lat, _, plain_conv, _, _ = timed_points(torch, plain, args.steps, False)
         pts_plain = plain.log[args.warmup:]
         errs = [abs(c["I"] - p["I"]) / max(abs(p["I"]), 1e-300)
                 for c, p in zip(pts_chosen, pts_plain)]
+        plain_counts = ([r["iters"] for r in pts_plain], [r["krylov_iters"] for r in pts_plain])
         ok_pts = sum(1 for c, e in zip(pts_chosen, errs) if c["converged"] and e <= 1e-6)
         del plain
     else:
         errs = [0.0] * len(pts_chosen)
         ok_pts = conv
         plain_conv = conv
+        plain_counts = ([r["iters"] for r in pts_chosen], [r["krylov_iters"] for r in pts_chosen])
 
     if world > 1:
         tt = torch.tensor([t_dev, t_e2e], device="cuda", dtype=torch.float64)
@@ -324,11 +347,7 @@ def run_ours(args):
         nn = [r["iters"] for r in pts_chosen]
         kk = [r["krylov_iters"] for r in pts_chosen]
         value = ok_all / t_dev
-        method_desc = {"mixed": "mixed precision: FP64 fused SG assembly, residual, Newton and "
-                                "convergence test; FP32 node-block-scaled BiCGStab inside FP64 "
-                                "iterative refinement; inexact-Newton forcing",
-                       "fp64": "plain FP64: fused SG assembly, node-block-scaled BiCGStab, "
-                               "damped Newton"}[args.method]
+        method_desc = METHOD_DESC[args.method]
         res = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -344,6 +363,7 @@ def run_ours(args):
             "converged_points": conv, "points_within_1e-6_of_plain_fp64": ok_pts,
             "points": args.steps * world,
             "max_rel_current_err_vs_plain_fp64": float(max(errs)) if errs else None,
+            "fp64_fallback_points": sum(1 for r in pts_chosen if r.get("fp64_from", -1) >= 0),
             "newton_iters_mean": float(np.mean(nn)), "krylov_iters_mean": float(np.mean(kk)),
             "e2e": {"value": ok_all / t_e2e, "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d_tot / args.steps),
@@ -375,7 +395,7 @@ def run_ours(args):
                 "converged_points": plain_conv}
             res["chosen_over_plain"] = value / res["plain_fp64_gpu"]["value"]
         if world == 1 and not args.no_cpu_baseline:
-            res["cpu_baseline"] = cpu_baseline(dev, args, nn, kk)
+            res["cpu_baseline"] = cpu_baseline(dev, args, *plain_counts)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -251,6 +251,9 @@ typedef struct tcad_newton_opts {
   int32_t precision;     /* 64: FP64 Krylov; 32: FP32 Krylov on an FP32 copy of the scaled
                             operator inside FP64 iterative refinement (residual, Newton,
                             convergence test stay FP64) */
+  int32_t density_scaling; /* 1: Krylov unknowns are (dpsi, dn/s_n, dp/s_p), s = max(n|p,
+                              dens_floor) -- the quantities of the Newton update test */
+  int32_t pad;
 } tcad_newton_opts_t;
 
 /* Per-instance result of a Newton solve (host memory). */
@@ -261,6 +264,10 @@ typedef struct tcad_newton_result {
   int32_t status;        /* last linear-solve status */
   double err;            /* last update norm */
   double relres;         /* last scaled linear residual */
+  int32_t fp64_from;     /* precision 32: Newton iteration from which this instance
+                            solved in FP64 after an FP32-solved step was rejected
+                            (-1: never; always -1 for precision 64) */
+  int32_t pad;
 } tcad_newton_result_t;
 
 /* Full coupled Newton solve at the contact targets stored in the pack

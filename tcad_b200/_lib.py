@@ -55,13 +55,15 @@ class NewtonOpts(ctypes.Structure):
                 ("rtol", ctypes.c_double), ("dens_floor", ctypes.c_double),
                 ("verbose", ctypes.c_int32), ("polish", ctypes.c_int32),
                 ("eta_max", ctypes.c_double), ("forcing", ctypes.c_int32),
-                ("precision", ctypes.c_int32)]
+                ("precision", ctypes.c_int32),
+                ("density_scaling", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 class NewtonResult(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int32), ("converged", ctypes.c_int32),
                 ("krylov_iters", ctypes.c_int32), ("status", ctypes.c_int32),
-                ("err", ctypes.c_double), ("relres", ctypes.c_double)]
+                ("err", ctypes.c_double), ("relres", ctypes.c_double),
+                ("fp64_from", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 # name -> (restype, argtypes)

@@ -84,11 +84,24 @@ struct Reduce {
 
 // --------------------------------------------------------------------------
 // block-Jacobi set-up: invert the 3x3 diagonal blocks, scale the rhs
+//
+// With densities (nn, pp non-null) the unknowns become relative updates
+// (dpsi, dn/s_n, dp/s_p), s = max(density, floor): the operator is
+// S^-1 D^-1 A S -- a similarity transform of the block-scaled operator, so
+// the same SpMV applies -- with the n/p rows of D^-1 divided by the node's s
+// and every neighbour block's n<-n / p<-p entry multiplied by that neighbour's
+// s.  Every component of the Krylov vectors is then on the scale of the
+// Newton update test, which is what an FP32 inner solve needs.
+template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_bj_setup(const tcad_pack_t pk, double* __restrict__ J, double* __restrict__ F,
-           int32_t* __restrict__ status) {
+           int32_t* __restrict__ status, const double* __restrict__ nn,
+           const double* __restrict__ pp, double floor_) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const int64_t NN = pk.n_nodes;
+  const bool rel = nn != nullptr;
+  int64_t off[6];
+  if (rel) nbr_offsets(load_inst(pk, fb.inst), off);
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
     double a[9];
 #pragma unroll
@@ -116,6 +129,22 @@ k_bj_setup(const tcad_pack_t pk, double* __restrict__ J, double* __restrict__ F,
       atomicExch(&status[fb.inst], TCAD_ERR_SINGULAR);
 #pragma unroll
       for (int e = 0; e < 9; ++e) inv[e] = (e % 4 == 0) ? 1.0 : 0.0;
+    }
+    double sn = 1.0, sp = 1.0;
+    if (rel) {
+      sn = fmax(nn[k], floor_);
+      sp = fmax(pp[k], floor_);
+      const double isn = 1.0 / sn, isp = 1.0 / sp;
+      inv[3] *= isn; inv[4] *= isn; inv[5] *= isn;
+      inv[6] *= isp; inv[7] *= isp; inv[8] *= isp;
+#pragma unroll
+      for (int d = 0; d < 2 * DIM; ++d) {
+        const int64_t m = clampi(k + off[d], fb.ioff, fb.iend);
+        const int64_t en = (int64_t)(9 + 5 * d + 2) * NN + k;   // n <- n
+        const int64_t ep = (int64_t)(9 + 5 * d + 4) * NN + k;   // p <- p
+        J[en] = J[en] * fmax(nn[m], floor_);
+        J[ep] = J[ep] * fmax(pp[m], floor_);
+      }
     }
 #pragma unroll
     for (int e = 0; e < 9; ++e) J[(int64_t)e * NN + k] = inv[e];
@@ -417,17 +446,20 @@ __global__ void __launch_bounds__(NT)
 k_newton_update(const tcad_pack_t pk, double* __restrict__ psi, double* __restrict__ nn,
                 double* __restrict__ pp, const double* __restrict__ du, double max_dpsi,
                 double floor_, const uint8_t* __restrict__ active,
-                unsigned long long* __restrict__ err) {
+                unsigned long long* __restrict__ err, int relative, int dry) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   if (active && !active[fb.inst]) return;
   __shared__ double sm[32];
   const int64_t NN = pk.n_nodes;
   double e = 0.0;
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
-    const double u0 = du[k], u1 = du[NN + k], u2 = du[2 * NN + k];
+    const double n0 = nn[k], p0 = pp[k];
+    const double u0 = du[k];
+    // relative-update unknowns come back scaled by max(density, floor)
+    const double u1 = relative ? du[NN + k] * fmax(n0, floor_) : du[NN + k];
+    const double u2 = relative ? du[2 * NN + k] * fmax(p0, floor_) : du[2 * NN + k];
     const bool finite = isfinite(u0) && isfinite(u1) && isfinite(u2);
     double dpsi = u0 < -max_dpsi ? -max_dpsi : (u0 > max_dpsi ? max_dpsi : u0);
-    const double n0 = nn[k], p0 = pp[k];
     double n1 = n0 + u1, p1 = p0 + u2;
     // numpy.clip(a, lo, hi) = minimum(maximum(a, lo), hi)
     n1 = fmin(fmax(n1, 0.1 * n0), 10.0 * n0);
@@ -437,9 +469,11 @@ k_newton_update(const tcad_pack_t pk, double* __restrict__ psi, double* __restri
     double ek = fmax(fabs(dpsi), fmax(rn, rp));
     if (!finite || !(ek == ek)) ek = INFINITY;  // NaN update: never "converged"
     e = fmax(e, ek);
-    psi[k] = psi[k] + dpsi;
-    nn[k] = n1;
-    pp[k] = p1;
+    if (!dry) {
+      psi[k] = psi[k] + dpsi;
+      nn[k] = n1;
+      pp[k] = p1;
+    }
   }
   const double m = block_max<NT>(e, sm);
   if (threadIdx.x == 0) atomicMax(&err[fb.inst], (unsigned long long)__double_as_longlong(m));
@@ -849,6 +883,7 @@ static int solve_mixed(const tcad_pack_t* pk, const double* J, const double* b, 
   std::vector<KState> irs(ni);
   std::vector<int32_t> pre(ni);
   std::vector<double> eta_in(ni);
+  if ((int)hks.size() < ni) hks.resize(ni);
   for (int i = 0; i < ni; ++i) {
     res_iters[i] = 0;
     res_status[i] = pre_status_host[i];
@@ -952,7 +987,12 @@ extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, 
 extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
                                        int32_t* status, void* stream) {
   if (!pk || !J || !F || !status) return TCAD_ERR_ARG;
-  k_bj_setup<<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status);
+  if (pk->dim == 2)
+    k_bj_setup<2><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status,
+                                                                         nullptr, nullptr, 0.0);
+  else
+    k_bj_setup<3><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status,
+                                                                         nullptr, nullptr, 0.0);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1002,7 +1042,7 @@ extern "C" int tcad_newton_update(const tcad_pack_t* pk, double* psi, double* n,
   TCAD_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(double) * pk->n_inst, s));
   k_newton_update<<<(unsigned)pk->n_flat, NT, 0, s>>>(
       *pk, psi, n, p, du, max_dpsi, dens_floor, active,
-      reinterpret_cast<unsigned long long*>(err));
+      reinterpret_cast<unsigned long long*>(err), 0, 0);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1026,8 +1066,9 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   for (int i = 0; i < ni; ++i) {
     result[i].iters = 0; result[i].converged = 0; result[i].krylov_iters = 0;
     result[i].status = TCAD_OK; result[i].err = INFINITY; result[i].relres = 0.0;
+    result[i].fp64_from = -1; result[i].pad = 0;
   }
-  std::vector<KState> hks;
+  std::vector<KState> hks(ni);  // sized up front: a solve may end before any inner launch
   std::vector<unsigned long long> herr(ni);
   std::vector<int32_t> hstat(ni);
   std::vector<int> polish_left(ni, -1);  // -1: not yet converged
@@ -1035,14 +1076,24 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   if (opts->precision == 32 && work_bytes < tcad_block_workspace_bytes(pk, 0, 0))
     return TCAD_ERR_ARG;
   const Work32 w32 = carve32(pk, reinterpret_cast<char*>(work) + ((w.bytes + 255) & ~(size_t)255));
-  std::vector<int32_t> mix_it(ni), mix_st(ni);
-  std::vector<double> mix_rr(ni);
+  std::vector<int32_t> mix_it(ni), mix_st(ni), mix_grew(ni, 0), mix_steps(ni, 0);
+  std::vector<double> mix_rr(ni), mix_prev(ni, -1.0);
+  std::vector<uint8_t> use64(ni, 0);  // precision 32: instances switched to FP64
+  std::vector<int32_t> last_kit(ni, 0);
   std::vector<double> heta(ni, opts->forcing ? std::max(opts->eta_max, opts->rtol) : opts->rtol);
   for (int it = 0; it < opts->max_iter; ++it) {
     int rc = tcad_sg_assemble(pk, psi, n, p, F, J, TCAD_MODE_ELIMINATE, stream);
     if (rc != TCAD_OK) return rc;
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int32_t) * ni, s));
-    k_bj_setup<<<nb, NT, 0, s>>>(*pk, J, F, w.status);
+    {
+      const bool rel = opts->density_scaling != 0;
+      const double* sn_ = rel ? n : nullptr;
+      const double* sp_ = rel ? p : nullptr;
+      if (pk->dim == 2)
+        k_bj_setup<2><<<nb, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, opts->dens_floor);
+      else
+        k_bj_setup<3><<<nb, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, opts->dens_floor);
+    }
     note_launch();
     TCAD_LAUNCH_CHECK();
     // inactive instances: pre-mark so their Krylov stays idle
@@ -1055,36 +1106,101 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
                                     cudaMemcpyHostToDevice, s));
     TCAD_CUDA_CHECK(cudaMemcpyAsync(w.eta, heta.data(), sizeof(double) * ni,
                                     cudaMemcpyHostToDevice, s));
-    if (opts->precision == 32) {
+    // instances whose step is solved in FP64 this iteration, and those whose
+    // (FP32-solved) step is applied before the FP64 solve starts
+    std::vector<uint8_t> grp64(ni, 0), grp32(ni, 0);
+    for (int i = 0; i < ni; ++i) {
+      if (!hact[i]) continue;
+      if (opts->precision == 32 && !use64[i] && hstat[i] == TCAD_OK) grp32[i] = 1;
+      else grp64[i] = 1;  // includes failed block set-ups: their update is zero
+    }
+    bool any32 = false, any64 = false;
+    for (int i = 0; i < ni; ++i) { any32 = any32 || grp32[i]; }
+    TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
+    if (any32) {
       // FP32 inner Krylov inside FP64 iterative refinement
+      std::vector<int32_t> st32(ni);
+      for (int i = 0; i < ni; ++i) st32[i] = grp32[i] ? TCAD_OK : -1;
       rc = solve_mixed(pk, J, F, du, heta.data(), opts->krylov_maxiter, 30, w, w32,
-                       hstat.data(), hks, mix_it.data(), mix_st.data(), mix_rr.data(), s);
+                       st32.data(), hks, mix_it.data(), mix_st.data(), mix_rr.data(), s);
       if (rc != TCAD_OK) return rc;
+      // Acceptance test before the step is applied (a dry-run update): an
+      // FP32-solved step is rejected when its refinement failed (breakdown,
+      // no convergence), when the update is non-finite, when it hits the
+      // 10x density clip, when the update norm grew on two mixed steps in a
+      // row, or when the instance has taken max_iter/3 mixed steps without
+      // converging.  A rejected instance re-solves this step in FP64 and
+      // stays in FP64 for the rest of the call.
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp32.data(), ni, cudaMemcpyHostToDevice, s));
+      k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
+                                        active, w.err, opts->density_scaling, 1);
+      note_launch();
+      TCAD_LAUNCH_CHECK();
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
+                                      cudaMemcpyDeviceToHost, s));
+      TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+      TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
+      bool acc_any = false;
       for (int i = 0; i < ni; ++i) {
-        if (!hact[i]) continue;
+        if (!grp32[i]) continue;
+        double e;
+        std::memcpy(&e, &herr[i], sizeof(double));
+        const bool grew = mix_prev[i] >= 0.0 && e >= mix_prev[i];
+        mix_grew[i] = grew ? mix_grew[i] + 1 : 0;
+        ++mix_steps[i];
+        const bool reject = mix_st[i] != TCAD_OK || !std::isfinite(e) || e >= 8.999 ||
+                            mix_grew[i] >= 2 ||
+                            mix_steps[i] > std::max(4, opts->max_iter / 3);
+        mix_prev[i] = e;
+        if (opts->verbose && reject)
+          std::fprintf(stderr, "    [gpu] inst %d it %2d  fp32 step rejected (err=%.3e st=%d)"
+                               " -> fp64\n", i, it, e, mix_st[i]);
         result[i].krylov_iters += mix_it[i];
-        result[i].status = mix_st[i];
-        result[i].relres = mix_rr[i];
-        hks[i].it = mix_it[i];
+        if (reject) {
+          grp32[i] = 0;
+          grp64[i] = 1;
+          use64[i] = 1;
+          result[i].fp64_from = it;
+        } else {
+          result[i].status = mix_st[i];
+          result[i].relres = mix_rr[i];
+          last_kit[i] = mix_it[i];
+          acc_any = true;
+        }
       }
-    } else {
+      if (acc_any) {
+        TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp32.data(), ni, cudaMemcpyHostToDevice, s));
+        k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi,
+                                          opts->dens_floor, active, w.err,
+                                          opts->density_scaling, 0);
+        note_launch();
+        TCAD_LAUNCH_CHECK();
+      }
+    }
+    for (int i = 0; i < ni; ++i) { any64 = any64 || grp64[i]; }
+    if (any64) {
+      // FP64 BiCGStab for the FP64 group; the other instances stay idle
+      std::vector<int32_t> st64(ni);
+      for (int i = 0; i < ni; ++i) st64[i] = grp64[i] ? hstat[i] : -1;
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(w.status, st64.data(), sizeof(int32_t) * ni,
+                                      cudaMemcpyHostToDevice, s));
       rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
                            w.eta);
       if (rc != TCAD_OK) return rc;
       // instances whose linear solve broke down / diverged keep their state
       for (int i = 0; i < ni; ++i) {
-        if (!hact[i]) continue;
+        if (!grp64[i]) continue;
+        last_kit[i] = hks[i].it;
         result[i].krylov_iters += hks[i].it;
         result[i].status = hks[i].status;
         result[i].relres = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
       }
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp64.data(), ni, cudaMemcpyHostToDevice, s));
+      k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
+                                        active, w.err, opts->density_scaling, 0);
+      note_launch();
+      TCAD_LAUNCH_CHECK();
     }
-    TCAD_CUDA_CHECK(cudaMemcpyAsync(active, hact.data(), ni, cudaMemcpyHostToDevice, s));
-    TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
-    k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
-                                      active, w.err);
-    note_launch();
-    TCAD_LAUNCH_CHECK();
     TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
                                     cudaMemcpyDeviceToHost, s));
     TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1100,7 +1216,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
                         result[i].status == TCAD_ERR_NONFINITE;
       if (opts->verbose)
         std::fprintf(stderr, "    [gpu] inst %d it %2d  err=%.3e  krylov=%d relres=%.2e eta=%.1e st=%d\n",
-                    i, it, e, hks[i].it, result[i].relres, heta[i], result[i].status);
+                    i, it, e, last_kit[i], result[i].relres, heta[i], result[i].status);
       // forcing term of the next step (inexact Newton): quadratic convergence
       // is kept while the linear tolerance tracks the update size
       if (opts->forcing)
@@ -1141,6 +1257,7 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
   for (int i = 0; i < ni; ++i) {
     result[i].iters = 0; result[i].converged = 0; result[i].krylov_iters = 0;
     result[i].status = TCAD_OK; result[i].err = INFINITY; result[i].relres = 0.0;
+    result[i].fp64_from = -1; result[i].pad = 0;
   }
   std::vector<KState> hks;
   std::vector<unsigned long long> herr(ni);

@@ -92,6 +92,11 @@ class NewtonOptions:
     # inside FP64 iterative refinement -- residual, Newton update and the
     # convergence test stay FP64, so the converged state is the FP64 one.
     precision: str = "fp64"
+    # GPU-only: Krylov unknowns.  "relative" solves for (dpsi, dn/max(n,1e-10),
+    # dp/max(p,1e-10)) -- the quantities the Newton update test measures --
+    # through a similarity transform of the block-scaled Jacobian; "absolute"
+    # for (dpsi, dn, dp).
+    krylov_unknowns: str = "relative"
 
     def __post_init__(self):
         if self.precond not in ("auto", "block_jacobi", "schur"):

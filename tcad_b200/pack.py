@@ -323,6 +323,7 @@ class Pack:
         psi0eq = np.zeros(N)
         gk = np.zeros(N); gv = np.zeros(N); gveq = np.zeros(N); gb = np.zeros(N)
         c_nodes, c_cid, c_L, c_n0, c_p0 = [], [], [], [], []
+        self.c_off = [0]
         self.contact_names = []
         self.cid_base = []
         base = 0
@@ -338,6 +339,7 @@ class Pack:
             flag[off + nodes] |= _lib.BC_CONTACT
             psi0eq[off + nodes] = 0.0 / s.VT + L
             c_nodes.append(off + nodes); c_cid.append(base + cid)
+            self.c_off.append(self.c_off[-1] + nodes.size)
             c_L.append(L); c_n0.append(n0); c_p0.append(p0)
             base += len(names)
         self.n_contacts_total = base
@@ -396,11 +398,20 @@ class Pack:
             self.t["gate_v"].copy_(torch.from_numpy(gv).to(self.device))
         self._vvt = vvt  # keep alive until the kernel ran
 
-    def stamp_contacts(self):
-        rc = self.lib.tcad_stamp_contacts(self.pref, _lib.ptr(self.c_nodes),
-                                          self.c_nodes.numel(), _lib.ptr(self.psi),
-                                          _lib.ptr(self.n), _lib.ptr(self.p), self.sp())
-        _lib.check(rc, "tcad_stamp_contacts")
+    def stamp_contacts(self, active=None):
+        """Contact nodes take their targets (all instances, or the instances
+        with active[i] set: their contact nodes are contiguous in c_nodes)."""
+        if active is None:
+            ranges = [(0, self.c_nodes.numel())]
+        else:
+            ranges = [(self.c_off[i], self.c_off[i + 1]) for i, a in enumerate(active) if a]
+        for a, b in ranges:
+            if b <= a:
+                continue
+            rc = self.lib.tcad_stamp_contacts(
+                self.pref, ctypes.c_void_p(self.c_nodes.data_ptr() + 8 * a), b - a,
+                _lib.ptr(self.psi), _lib.ptr(self.n), _lib.ptr(self.p), self.sp())
+            _lib.check(rc, "tcad_stamp_contacts")
 
     # ---- kernels -----------------------------------------------------------
     def assemble(self, mode, psi=None, n=None, p=None):
@@ -468,6 +479,7 @@ class Pack:
         o.forcing = 1 if getattr(opts, "forcing", "fixed") == "adaptive" else 0
         o.eta_max = float(getattr(opts, "eta_max", 1e-3))
         o.precision = 32 if getattr(opts, "precision", "fp64") == "mixed" and not equilibrium else 64
+        o.density_scaling = 1 if getattr(opts, "krylov_unknowns", "relative") == "relative" else 0
         return o
 
     def newton(self, opts, active=None):
@@ -485,7 +497,7 @@ class Pack:
         _lib.check(rc, "tcad_newton_solve")
         return [dict(iters=r.iters, converged=bool(r.converged),
                      krylov_iters=r.krylov_iters, status=r.status, err=r.err,
-                     relres=r.relres) for r in res]
+                     relres=r.relres, fp64_from=r.fp64_from) for r in res]
 
     def equilibrium(self, opts):
         ni = len(self.setups)
@@ -500,4 +512,4 @@ class Pack:
         _lib.check(rc, "tcad_equilibrium_solve")
         return [dict(iters=r.iters, converged=bool(r.converged),
                      krylov_iters=r.krylov_iters, status=r.status, err=r.err,
-                     relres=r.relres) for r in res]
+                     relres=r.relres, fp64_from=r.fp64_from) for r in res]

@@ -116,3 +116,53 @@ def trigate_schedule():
         for q, vg in enumerate(TRIGATE_VG):
             pts.append((vd, vg, q == 0))
     return pts
+
+
+def mosfet2d(dev_cls, nx=120, ny=60, Lg=100e-7, Lsd=None, depth=None, Na=1e17,
+             Nsd_peak=1e20, tox=2e-7, sigma=None, ratio_x=1.08, ratio_y=1.06,
+             models=None):
+    """n-channel MOSFET on an exact nx x ny mesh, the structure of
+    pytcad/mosfet.py:57-87 (build_mosfet): source/drain ohmic contacts on the
+    surface over x <= Lsd / x >= Lsd+Lg, body contact on the bottom row, an
+    oxide gate over the channel (n+poly flat-band), Gaussian-erfc S/D."""
+    Lsd = Lg if Lsd is None else Lsd
+    depth = 2.0 * Lg + 50e-7 if depth is None else depth
+    sigma = Lg / 4.0 if sigma is None else sigma
+    L = 2 * Lsd + Lg
+    x = graded_nodes(nx, L, [Lsd, Lsd + Lg], ratio_x)
+    y = graded_nodes(ny, depth, [0.0], ratio_y)
+    dop, ntot = mosfet_doping(x, y, Lsd, Lg, Na, Nsd_peak, sigma, sigma)
+    dev = dev_cls(Mesh2D(x, y), dop, Ntotal=ntot, models=models or Models())
+    i_src = np.where(x <= Lsd)[0]
+    i_drn = np.where(x >= Lsd + Lg)[0]
+    i_gate = np.where((x > Lsd) & (x < Lsd + Lg))[0]
+    dev.add_contact("source", i_src, np.zeros_like(i_src))
+    dev.add_contact("drain", i_drn, np.zeros_like(i_drn))
+    dev.add_contact("body", np.arange(nx), np.full(nx, ny - 1))
+    Vfb = flatband_voltage(-Na, tox, "n+poly")
+    dev.add_gate("gate", i_gate, np.zeros_like(i_gate), tox_cm=tox, Vfb=Vfb)
+    return dev
+
+
+def mosfet_batch_params(count=512, seed=2026, nx=(80, 400), ny=(40, 200), Lg=(30e-7, 200e-7),
+                        Na=(1e16, 1e18), Npk=(1e19, 1e20), V=(0.0, 1.2)):
+    """Seeded draws of the batched 2D MOSFET workload: per instance nx, ny
+    uniform integers, Lg uniform, body doping and S/D peak log-uniform, and its
+    own (Vg, Vd) uniform."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        out.append(dict(
+            nx=int(rng.integers(nx[0], nx[1] + 1)), ny=int(rng.integers(ny[0], ny[1] + 1)),
+            Lg=float(rng.uniform(*Lg)),
+            Na=float(10.0 ** rng.uniform(np.log10(Na[0]), np.log10(Na[1]))),
+            Nsd_peak=float(10.0 ** rng.uniform(np.log10(Npk[0]), np.log10(Npk[1]))),
+            Vg=float(rng.uniform(*V)), Vd=float(rng.uniform(*V))))
+    return out
+
+
+def ramp(target, steps):
+    """The explicit bias ramp both sides use: equal steps from 0 to the
+    target, `steps` of them (the reference has no ramp of its own; every
+    instance jumps from equilibrium through the same schedule)."""
+    return [{k: v * (s + 1) / steps for k, v in target.items()} for s in range(steps)]

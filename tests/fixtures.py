@@ -121,3 +121,17 @@ def gpu_device(g, material=None):
             dev.bcs[name] = Gate(k, v[0], v[1], v[2], s.gate_weight(idx, axis), axis)
     dev._bcs_changed()
     return dev
+
+
+def current_err(I, g, floor_frac=1e-9):
+    """Relative distance of currents I to the reference's: the smaller of the
+    distances to its converged state and to the other state of its Newton
+    limit cycle (fixture key I_alt; equal to I where there is no cycle).
+    Points with a current below floor_frac x the sweep's largest compare on
+    that scale (the V = 0 point carries a round-off-level current)."""
+    I = np.asarray(I, dtype=float)
+    ref = np.asarray(g["I"], dtype=float)
+    alt = np.asarray(g["I_alt"], dtype=float) if "I_alt" in g else ref
+    scale = np.maximum(np.abs(ref), floor_frac * np.abs(ref).max())
+    scale = np.where(scale == 0, 1.0, scale)
+    return float((np.minimum(np.abs(I - ref), np.abs(I - alt)) / scale).max())

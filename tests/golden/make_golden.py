@@ -81,6 +81,20 @@ def _geom(n, L, focus, ratio):
     return nodes
 
 
+def _next_state_current(dev, volts, opts, contact):
+    """Current after one more reference Newton step from the converged state
+    (a second solve_bias call takes exactly one step).  At some low-bias
+    points the reference's Newton settles into a period-2 round-off limit
+    cycle between two states whose currents differ by up to ~1e-5 relative
+    (sub-floor minority densities); this records the cycle's other state.
+    The device state is restored afterwards."""
+    keep = (dev.psi.copy(), dev.n.copy(), dev.p.copy())
+    dev.solve_bias(volts, opts)
+    I = dev.terminal_current(contact)
+    dev.psi, dev.n, dev.p = keep
+    return I
+
+
 def _csr(J):
     J = J.tocsr()
     J.sort_indices()
@@ -271,11 +285,13 @@ def diode_c1(pt, out, nx=201, ny=101, vmax=0.70):
     Vs = np.round(np.arange(0.0, vmax + 1e-9, 0.05), 10)
     I, keep = [], {}
     t_pts = []
+    I_alt = []
     for V in Vs:
         t1 = time.time()
         dev.solve_bias({"anode": float(V)}, opts)
         t_pts.append(time.time() - t1)
         I.append(dev.terminal_current("anode"))
+        I_alt.append(_next_state_current(dev, {"anode": float(V)}, opts, "anode"))
         if abs(V - 0.35) < 1e-9 or abs(V - Vs[-1]) < 1e-9:
             tag = "%03d" % int(round(V * 100))
             keep["psi_" + tag] = dev.psi.ravel().copy()
@@ -283,7 +299,8 @@ def diode_c1(pt, out, nx=201, ny=101, vmax=0.70):
             keep["p_" + tag] = dev.p.ravel().copy()
     print(f"  diode {nx}x{ny}: {time.time() - t0:.1f} s, per point "
           f"{np.mean(t_pts):.2f} s")
-    extra = dict(V=Vs, I=np.array(I), psi_eq=psi_eq.ravel(), tol_update=SWEEP_TOL,
+    extra = dict(V=Vs, I=np.array(I), I_alt=np.array(I_alt), psi_eq=psi_eq.ravel(),
+                 tol_update=SWEEP_TOL,
                  sec_per_point=np.array(t_pts), mat_tau=1e-7, **keep)
     np.savez_compressed(out, **_dump_dev(dev, 2, extra))
 
@@ -340,17 +357,19 @@ def trigate_small(pt, out):
     dev.solve_equilibrium(opts)
     keep = dict(psi_eq=dev.psi.ravel().copy())
     Vg = [0.0, 0.4, 0.8]
-    I = []
+    I, I_alt = [], []
     for v in Vg:
-        dev.solve_bias({"drain": 0.05, "gate_top": v, "gate_left": v,
-                        "gate_right": v}, opts)
+        volts = {"drain": 0.05, "gate_top": v, "gate_left": v, "gate_right": v}
+        dev.solve_bias(volts, opts)
         I.append(dev.terminal_current("drain"))
         tag = "%02d" % int(round(v * 10))
         keep["psi_" + tag] = dev.psi.ravel().copy()
         keep["n_" + tag] = dev.n.ravel().copy()
         keep["p_" + tag] = dev.p.ravel().copy()
+        I_alt.append(_next_state_current(dev, volts, opts, "drain"))
     print(f"  trigate small {mesh.N} nodes: {time.time() - t0:.1f} s")
-    extra = dict(Vg=np.array(Vg), Vd=0.05, I=np.array(I), tol_update=SWEEP_TOL, **keep)
+    extra = dict(Vg=np.array(Vg), Vd=0.05, I=np.array(I), I_alt=np.array(I_alt),
+                 tol_update=SWEEP_TOL, **keep)
     np.savez_compressed(out, **_dump_dev(dev, 3, extra))
 
 
@@ -363,7 +382,7 @@ def mosfet_small(pt, out):
     opts = NewtonOptions(linsolve="direct", tol_update=SWEEP_TOL)
     dev.solve_equilibrium(opts)
     keep = dict(psi_eq=dev.psi.ravel().copy())
-    I = []
+    I, I_alt = [], []
     Vg = [0.0, 0.6, 1.2]
     for v in Vg:
         dev.solve_bias({"drain": 0.5, "gate": v}, opts)
@@ -372,7 +391,9 @@ def mosfet_small(pt, out):
         keep["psi_" + tag] = dev.psi.ravel().copy()
         keep["n_" + tag] = dev.n.ravel().copy()
         keep["p_" + tag] = dev.p.ravel().copy()
-    extra = dict(Vg=np.array(Vg), Vd=0.5, I=np.array(I), tol_update=SWEEP_TOL, **keep)
+        I_alt.append(_next_state_current(dev, {"drain": 0.5, "gate": v}, opts, "drain"))
+    extra = dict(Vg=np.array(Vg), Vd=0.5, I=np.array(I), I_alt=np.array(I_alt),
+                 tol_update=SWEEP_TOL, **keep)
     np.savez_compressed(out, **_dump_dev(dev, 2, extra))
 
 

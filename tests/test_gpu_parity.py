@@ -69,35 +69,36 @@ def test_diode_small_sweep():
         dev.solve_bias({"anode": float(V)})
         assert dev.last_converged, V
         I.append(dev.terminal_current("anode"))
-    I = np.array(I)
-    # the V = 0 point carries a round-off-level current: compare on the scale
-    # of the sweep
-    assert fx.vec_err(I, g["I"], 1e-9 * np.abs(g["I"]).max()) < TOL_I
+    assert fx.current_err(I, g) < TOL_I
 
 
 def test_mosfet_small_sweep():
     g = fx.load("mosfet_small")
     dev = fx.gpu_device(g)
     dev.solve_equilibrium()
+    I = []
     for v, Iref in zip(g["Vg"], g["I"]):
         dev.solve_bias({"drain": float(g["Vd"]), "gate": float(v)})
         assert dev.last_converged
         tag = "%02d" % int(round(v * 10))
         assert np.abs(dev.psi.ravel() - g["psi_" + tag]).max() * dev.VT < TOL_PSI_V
-        assert abs(dev.terminal_current("drain") - Iref) <= TOL_I * abs(Iref)
+        I.append(dev.terminal_current("drain"))
+    assert fx.current_err(I, g) < TOL_I
 
 
 def test_trigate_small_sweep():
     g = fx.load("trigate_small")
     dev = fx.gpu_device(g)
     dev.solve_equilibrium()
+    I = []
     for v, Iref in zip(g["Vg"], g["I"]):
         dev.solve_bias({"drain": float(g["Vd"]), "gate_top": float(v),
                         "gate_left": float(v), "gate_right": float(v)})
         assert dev.last_converged
         tag = "%02d" % int(round(v * 10))
         assert np.abs(dev.psi.ravel() - g["psi_" + tag]).max() * dev.VT < TOL_PSI_V
-        assert abs(dev.terminal_current("drain") - Iref) <= TOL_I * abs(Iref)
+        I.append(dev.terminal_current("drain"))
+    assert fx.current_err(I, g) < TOL_I
 
 
 def test_smoke_entry():
@@ -125,8 +126,7 @@ def test_diode_c1_sweep():
                 phi = dev.psi.ravel() + sgn * np.log(getattr(dev, c).ravel() / dev.nie_s.ravel())
                 phr = g["psi_" + tag] + sgn * np.log(g[c + "_" + tag] / dev.nie_s.ravel())
                 assert np.abs(phi - phr).max() * VT < 1e-8, c
-    I = np.array(I)
-    assert fx.vec_err(I, g["I"], 1e-9 * np.abs(g["I"]).max()) < TOL_I
+    assert fx.current_err(I, g) < TOL_I
 
 
 @pytest.mark.parametrize("name", ["mosfet_small", "trigate_small"])
@@ -140,16 +140,21 @@ def test_mixed_precision_sweep(name):
     dev.solve_equilibrium()
     opts = tb.NewtonOptions(precision="mixed")
     gates = [b for b in dev.bcs if b.startswith("gate")]
-    for v, Iref in zip(g["Vg"], g["I"]):
+    I = []
+    for v in g["Vg"]:
         volts = {"drain": float(g["Vd"]), **{gt: float(v) for gt in gates}}
         dev.solve_bias(volts, opts)
         assert dev.last_converged
         tag = "%02d" % int(round(v * 10))
         assert np.abs(dev.psi.ravel() - g["psi_" + tag]).max() * dev.VT < TOL_PSI_V
-        assert abs(dev.terminal_current("drain") - Iref) <= TOL_I * abs(Iref)
+        I.append(dev.terminal_current("drain"))
+    assert fx.current_err(I, g) < TOL_I
 
 
 def test_mixed_precision_diode_c1():
+    """Mixed precision on the 201x101 diode: where an FP32-solved step would
+    be rejected (density clip hit, breakdown) the instance falls back to FP64
+    on the GPU; the sweep still converges to the reference's currents."""
     import tcad_b200 as tb
     g = fx.load("diode_c1")
     dev = fx.gpu_device(g, material=dict(tau_n0=1e-7, tau_p0=1e-7, tau_Nref=1e300))
@@ -160,4 +165,4 @@ def test_mixed_precision_diode_c1():
         dev.solve_bias({"anode": float(V)}, opts)
         assert dev.last_converged, V
         I.append(dev.terminal_current("anode"))
-    assert fx.vec_err(np.array(I), g["I"], 1e-9 * np.abs(g["I"]).max()) < TOL_I
+    assert fx.current_err(I, g) < TOL_I
