@@ -76,7 +76,21 @@ def parse():
     ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="trigate3d", choices=["trigate3d", "diode2d"])
+    ap.add_argument("--workload", default="trigate3d",
+                    choices=["trigate3d", "diode2d", "mosfet2d_batch", "serve"])
+    ap.add_argument("--duration", type=float, default=60.0,
+                    help="serve: seconds of Poisson arrivals")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: mean requests/s")
+    ap.add_argument("--budget-gb", type=float, default=160.0,
+                    help="serve: HBM budget of the arenas (GB)")
+    ap.add_argument("--drain", type=float, default=30.0,
+                    help="serve: seconds to finish in-flight work after the arrivals end")
+    ap.add_argument("--plain-seconds", type=float, default=45.0,
+                    help="serve: time cap of the sequential plain FP64 run")
+    ap.add_argument("--batch", type=int, default=512,
+                    help="mosfet2d_batch: instances in the batch")
+    ap.add_argument("--plain-sample", type=int, default=16,
+                    help="mosfet2d_batch: instances of the sequential plain run")
     ap.add_argument("--small", action="store_true", help="down-scaled mesh (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--method", default="mixed", choices=list(METHODS),
@@ -208,8 +222,7 @@ class PointRunner:
             dev.solve_equilibrium(self.opts)
         dev.solve_bias(volts, self.opts)
         I = dev.terminal_current(self.contact)
-        N = dev.N
-        h2d = 8 * (len(volts) + 3) + (8 * N if any(k.startswith("gate") for k in volts) else 0)
+        h2d = dev.pack.last_h2d_bytes   # contact targets + gate-node bias values
         self.log.append(dict(dev.last_newton, first=first, I=I))
         if self.args.verbose:
             r = dev.last_newton
@@ -402,6 +415,315 @@ def run_ours(args):
     return res
 
 
+# ---------------------------------------------------------------------------
+# Batched 2D MOSFETs: one packed batch against sequential plain solves.
+BATCH_RAMP = 4     # equal bias steps from equilibrium to each instance's (Vg, Vd)
+
+
+def batch_devices(args, dev_cls, idx=None):
+    from tcad_b200 import workloads as W
+    params = W.mosfet_batch_params(args.batch)
+    if args.small:
+        params = [dict(q, nx=max(20, q["nx"] // 4), ny=max(12, q["ny"] // 4)) for q in params]
+    idx = range(len(params)) if idx is None else idx
+    out = []
+    for i in idx:
+        q = params[i]
+        out.append((q, W.mosfet2d(dev_cls, nx=q["nx"], ny=q["ny"], Lg=q["Lg"], Na=q["Na"],
+                                  Nsd_peak=q["Nsd_peak"])))
+    return out
+
+
+def run_batch(args):
+    """512 seeded MOSFETs of uneven size, each at its own (Vg, Vd): a step is
+    one packed solve of all of them (equilibrium, then BATCH_RAMP bias steps
+    to the target) and the drain currents read back to the host.  The plain
+    FP64 path solves an evenly spaced sample of the same instances one after
+    another, the same way; its rate is points per second of that sample."""
+    import torch
+    import tcad_b200 as tb
+    from tcad_b200 import _lib
+    from tcad_b200 import workloads as W
+    from tcad_b200.batch import DeviceBatch
+    lib = _lib.load()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    t_build = time.perf_counter()
+    built = batch_devices(args, tb.Device2D)
+    params = [q for q, _ in built]
+    batch = DeviceBatch([d for _, d in built])
+    t_build = time.perf_counter() - t_build
+    N = batch.pack.N
+    opts = tb.NewtonOptions(verbose=bool(args.verbose), **METHODS[args.method])
+    ramps = [W.ramp({"gate": q["Vg"], "drain": q["Vd"]}, BATCH_RAMP) for q in params]
+
+    def step():
+        h2d = 0
+        batch.solve_equilibrium(opts)
+        conv = np.zeros(batch.n, dtype=bool)
+        iters = np.zeros(batch.n)
+        kits = np.zeros(batch.n)
+        for s in range(BATCH_RAMP):
+            res = batch.solve_bias([r[s] for r in ramps], opts)
+            h2d += batch.pack.last_h2d_bytes
+            conv = np.array([r["converged"] for r in res])
+            iters += [r["iters"] for r in res]
+            kits += [r["krylov_iters"] for r in res]
+        I = batch.terminal_currents("drain")   # device -> host
+        return I, conv, h2d, 8 * batch.n, iters, kits
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    L0 = lib.tcad_launch_count()
+    lat = []
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            I, conv, h2d, d2h, iters, kits = step()
+            b.record()
+            torch.cuda.synchronize()
+            lat.append(a.elapsed_time(b))
+    launches = lib.tcad_launch_count() - L0
+    t_dev = sum(lat) / 1e3
+    n_conv = int(conv.sum())
+
+    # sequential plain solves of an evenly spaced sample
+    sample = np.unique(np.linspace(0, batch.n - 1, min(args.plain_sample, batch.n)).astype(int))
+    popts = tb.NewtonOptions(**METHODS["plain"])
+    plain_lat, plain_I, plain_conv = [], [], 0
+    for j, (q, dev) in zip(sample, batch_devices(args, tb.Device2D, sample)):
+        for rep in range(2):         # first solve warms this instance's buffers
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            dev.solve_equilibrium(popts)
+            for volts in ramps[j]:
+                dev.solve_bias(volts, popts)
+            Ij = dev.terminal_current("drain")
+            b.record()
+            torch.cuda.synchronize()
+        plain_lat.append(a.elapsed_time(b))
+        plain_I.append(Ij)
+        plain_conv += int(dev.last_converged)
+        dev._pack = None
+    errs = [abs(I[j] - Ij) / max(abs(Ij), 1e-300) for j, Ij in zip(sample, plain_I)]
+    plain_rate = plain_conv / (sum(plain_lat) / 1e3)
+    value = args.steps * n_conv / t_dev
+    res = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (FP32 inner Krylov)" if args.method == "mixed" else "f64",
+        "data": "synthetic devices (seeded MOSFET draws, analytic doping)",
+        "config": {"workload": f"mosfet2d_batch: {batch.n} Device2D MOSFETs, nx~U[80,400], "
+                               f"ny~U[40,200], seed 2026 ({N:,} nodes packed); each at its "
+                               f"own (Vg, Vd) via {BATCH_RAMP} equal steps from equilibrium",
+                   "method": METHOD_DESC[args.method] + "; one packed ragged batch, "
+                             "per-instance convergence masks",
+                   "parallelism": "single GPU",
+                   "l2": f"inputs larger than L2 (J alone is {8 * 29 * N / 1e6:.0f} MB)"},
+        "p50_ms": statistics.median(lat), "p99_ms": float(np.percentile(lat, 99)),
+        "converged_points": n_conv, "points_per_step": batch.n,
+        "newton_iters_mean_per_instance": float(iters.mean()),
+        "krylov_iters_mean_per_instance": float(kits.mean()),
+        "plain_fp64_gpu": {"value": plain_rate, "unit": UNIT,
+                           "sample_instances": [int(j) for j in sample],
+                           "p50_ms_per_instance": statistics.median(plain_lat),
+                           "p99_ms_per_instance": float(np.percentile(plain_lat, 99)),
+                           "converged": plain_conv},
+        "chosen_over_plain": value / plain_rate if plain_rate > 0 else None,
+        "max_rel_current_err_vs_plain_fp64": float(max(errs)),
+        "e2e": {"value": args.steps * n_conv / t_dev, "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "note": "the timed step already includes the bias uploads and the "
+                        "current read-back"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "build_s": t_build,
+    }
+    return res
+
+
+# ---------------------------------------------------------------------------
+# Serving: an open-loop Poisson request stream through tcad_b200.serve.
+def serve_stream(args, dev2d, dev3d):
+    """The seeded request mix: 70% single-bias 2D MOSFET solves on meshes
+    64x32..512x256, 25% warm-started 2D Id-Vg sweeps of 11..41 points, 5%
+    3D tri-gate solves on meshes 64^3..128^3.  Devices are drawn from seeded
+    design pools (built before the clock starts); every request is its own
+    device (its own key).  Returns [(t_arrival, kind, design, points,
+    report, contact)] and the pools."""
+    from tcad_b200 import workloads as W
+    rng = np.random.default_rng(7)
+    n2, n3 = (24, 3) if args.small else (96, 6)
+    pool2, pool3 = [], []
+    for _ in range(n2):
+        nx, ny = (int(rng.integers(64, 513)), int(rng.integers(32, 257)))
+        if args.small:
+            nx, ny = nx // 4, max(12, ny // 4)
+        pool2.append(dict(nx=nx, ny=ny, Lg=float(rng.uniform(30e-7, 200e-7)),
+                          Na=float(10 ** rng.uniform(16, 18)),
+                          Nsd_peak=float(10 ** rng.uniform(19, 20))))
+    for _ in range(n3):
+        m = int(rng.integers(64, 129))
+        dims = (m, int(rng.integers(64, 129)), int(rng.integers(64, 129)))
+        if args.small:
+            dims = tuple(max(12, d // 4) for d in dims)
+        pool3.append(dims)
+    t, out = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / args.rate))
+        if t >= args.duration:
+            break
+        u = float(rng.uniform())
+        if u < 0.70:
+            d = int(rng.integers(len(pool2)))
+            vg, vd = (float(x) for x in rng.uniform(0.0, 1.2, 2))
+            pts = W.ramp({"gate": vg, "drain": vd}, BATCH_RAMP)
+            out.append((t, "single2d", d, pts, [False] * (BATCH_RAMP - 1) + [True], "drain"))
+        elif u < 0.95:
+            d = int(rng.integers(len(pool2)))
+            vd = float(rng.uniform(0.05, 1.0))
+            npt = int(rng.integers(11, 42))
+            pts = W.ramp({"drain": vd}, 2) + [{"gate": float(vg), "drain": vd}
+                                              for vg in np.linspace(0.0, 1.0, npt)]
+            out.append((t, "sweep2d", d, pts, [False, False] + [True] * npt, "drain"))
+        else:
+            d = int(rng.integers(len(pool3)))
+            vg, vd = (float(x) for x in rng.uniform(0.0, 1.0, 2))
+            pts = [W.trigate_bias(vd * (s + 1) / 3, vg * (s + 1) / 3) for s in range(3)]
+            out.append((t, "single3d", d, pts, [False, False, True], "drain"))
+    return out, pool2, pool3
+
+
+def run_serve(args):
+    import torch
+    import tcad_b200 as tb
+    from tcad_b200 import _lib
+    from tcad_b200 import workloads as W
+    from tcad_b200.serve import Request, Server
+    lib = _lib.load()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream, pool2, pool3 = serve_stream(args, tb.Device2D, tb.Device3D)
+    t_build = time.perf_counter()
+    setups2 = [W.mosfet2d(tb.Device2D, **q).setup for q in pool2]
+    setups3 = [W.trigate3d(tb.Device3D, *d).setup for d in pool3]
+    t_build = time.perf_counter() - t_build
+    opts = tb.NewtonOptions(**METHODS[args.method])
+    budget = args.budget_gb * 1e9
+    srv = Server(budget={2: int(0.75 * budget), 3: int(0.25 * budget)}, opts=opts)
+    # warm-up: one request of each kind, untimed
+    srv.start()
+    for kind, setups in (("2d", setups2), ("3d", setups3)):
+        pts = (W.ramp({"gate": 0.5, "drain": 0.5}, 2) if kind == "2d"
+               else [W.trigate_bias(0.3, 0.3)])
+        srv.submit(Request(f"warm{kind}", setups[0], pts, "drain"))
+    srv.wait_idle()
+    for w in srv.workers.values():
+        w.rounds, w.round_log, w.h2d_bytes, w.d2h_bytes = 0, [], 0, 0
+    torch.cuda.synchronize()
+    L0 = lib.tcad_launch_count()
+    reqs = []
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        t0 = time.perf_counter()
+        for q, (ta, kind, d, pts, rep, contact) in enumerate(stream):
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
+            setup = setups2[d] if kind != "single3d" else setups3[d]
+            reqs.append(srv.submit(Request(f"{kind}-{q}", setup, pts, contact, rep,
+                                           arrival=t0 + ta)))
+        left = max(0.0, t0 + args.duration + args.drain - time.perf_counter())
+        ok = srv.wait_idle(timeout=left)
+        t_end = time.perf_counter()
+    srv.stop(abort=not ok)
+    torch.cuda.synchronize()
+    launches = lib.tcad_launch_count() - L0
+    done = [r for r in reqs
+            if r.finished is not None and r.error is None and r.finished <= t_end]
+    pts_conv = sum(sum(r.converged) for r in done)
+    pts_all = sum(r.reported_points for r in reqs)
+    lat = np.array([r.latency for r in done]) * 1e3
+    elapsed = t_end - t0
+    by_kind = {}
+    for kind in ("single2d", "sweep2d", "single3d"):
+        lk = np.array([r.latency for r in done if r.key.startswith(kind)]) * 1e3
+        if lk.size:
+            by_kind[kind] = {"requests": int(lk.size), "p50_ms": float(np.median(lk)),
+                             "p99_ms": float(np.percentile(lk, 99))}
+    h2d = sum(w.h2d_bytes for w in srv.workers.values())
+    d2h = sum(w.d2h_bytes for w in srv.workers.values())
+    rounds = {d: {"rounds": w.rounds,
+                  "mean_instances": float(np.mean([n for _, _, n, _ in w.round_log]))
+                  if w.round_log else 0.0,
+                  "max_instances": max([n for _, _, n, _ in w.round_log], default=0)}
+              for d, w in srv.workers.items()}
+    value = pts_conv / elapsed
+
+    # the plain FP64 path: the same requests in arrival order, one after another
+    # through the drop-in device API, until the time cap
+    popts = tb.NewtonOptions(**METHODS["plain"])
+    p_pts, p_time, p_req, p_err = 0, 0.0, 0, []
+    served = {r.key: r for r in reqs}
+    for q, (ta, kind, d, pts, rep, contact) in enumerate(stream):
+        if p_time > args.plain_seconds:
+            break
+        dev = (W.mosfet2d(tb.Device2D, **pool2[d]) if kind != "single3d"
+               else W.trigate3d(tb.Device3D, *pool3[d]))
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        dev.solve_equilibrium(popts)
+        I = []
+        for v, r_ in zip(pts, rep):
+            dev.solve_bias(v, popts)
+            if r_:
+                I.append(dev.terminal_current(contact))
+                p_pts += int(dev.last_converged)
+        torch.cuda.synchronize()
+        p_time += time.perf_counter() - a
+        p_req += 1
+        r = served[f"{kind}-{q}"]
+        if r.error is None and r.currents:
+            p_err.extend(abs(x - y) / max(abs(y), 1e-300) for x, y in zip(r.currents, I))
+        dev._pack = None
+    plain_rate = p_pts / p_time if p_time > 0 else None
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": len(reqs), "warmup": 2, "ms_per_step": 1e3 * elapsed / max(len(reqs), 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (FP32 inner Krylov)" if args.method == "mixed" else "f64",
+        "data": "synthetic request stream (seeded Poisson arrivals, seeded device designs)",
+        "config": {"workload": f"serve: Poisson {args.rate:g} req/s for {args.duration:g} s; "
+                               "70% single-bias 2D MOSFET 64x32..512x256 (4-step ramp), "
+                               "25% warm-started 2D Id-Vg sweeps of 11..41 points, 5% 3D "
+                               "tri-gate 64^3..128^3 (3-step ramp)",
+                   "method": METHOD_DESC[args.method] + "; continuous batching at bias-point "
+                             "rounds over HBM arenas (2D and 3D on separate streams)",
+                   "budget_gb": args.budget_gb, "parallelism": "single GPU"},
+        "requests": len(reqs), "completed": len(done), "drained": bool(ok),
+        "unfinished": len(reqs) - len(done),
+        "converged_points": int(pts_conv), "reported_points": int(pts_all),
+        "elapsed_s": elapsed, "offered_points_per_s": pts_all / args.duration,
+        "p50_ms": float(np.median(lat)) if lat.size else None,
+        "p99_ms": float(np.percentile(lat, 99)) if lat.size else None,
+        "latency_by_kind": by_kind, "rounds": rounds,
+        "plain_fp64_gpu": {"value": plain_rate, "unit": UNIT, "requests": p_req,
+                           "points": p_pts, "seconds": p_time,
+                           "note": "the first requests of the same stream, solved one "
+                                   "after another through Device2D/Device3D"},
+        "chosen_over_plain": value / plain_rate if plain_rate else None,
+        "max_rel_current_err_vs_plain_fp64": float(max(p_err)) if p_err else None,
+        "e2e": {"value": value, "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d / max(len(reqs), 1)),
+                "d2h_bytes_per_step": int(d2h / max(len(reqs), 1)),
+                "note": "a step is one request; arrival to completion, uploads of each "
+                        "new device's arrays and bias values and the current read-back "
+                        "included"},
+        "gpu_launches": int(launches), "clocks": clk.summary(), "build_s": t_build,
+    }
+
+
 def oracle_from(dev):
     """The same device, state and BCs for the CPU oracle."""
     from oracle import OracleDevice, OracleModels
@@ -584,6 +906,10 @@ def main():
         return
     if args.impl == "reference":
         res = run_reference(args)
+    elif args.workload == "mosfet2d_batch":
+        res = run_batch(args)
+    elif args.workload == "serve":
+        res = run_serve(args)
     else:
         res = run_ours(args)
     if res:

@@ -9,9 +9,11 @@
  * TCAD_ERR_SINGULAR / _NONFINITE / _NOCONV / _BREAKDOWN -> LinearSolveError
  * (pytcad/linsolve.py:344), TCAD_ERR_CUDA -> RuntimeError.
  *
- * Data model ("pack"): one or more devices (instances) of one dimension are
- * packed back to back.  Node arrays are structure-of-arrays of length
- * n_nodes, node k of instance i sitting at node_off[i] + k with
+ * Data model ("pack"): one or more devices (instances) of one dimension share
+ * the node arrays.  Node arrays are structure-of-arrays of length n_nodes,
+ * node k of instance i sitting at node_off[i] + k (instance i spans
+ * Nx*Ny*Nz nodes; instances are listed in increasing node_off and may leave
+ * gaps, as in a serving arena whose resident devices keep their places) with
  * k = (kz*Ny + j)*Nx + i_x (x fastest), the reference's flat order
  * (pytcad/mesh2d.py:1-7, pytcad/mesh3d.py:1-10).  Edge coefficients live at
  * the edge's low ("owner") node.  Vectors of the coupled system are
@@ -72,12 +74,13 @@ extern "C" {
 typedef struct tcad_pack {
   int32_t dim;           /* 2 or 3 */
   int32_t n_inst;        /* packed instances */
-  int64_t n_nodes;       /* total nodes */
+  int64_t n_nodes;       /* length of every node array (>= the last instance's end) */
   int64_t n_flat;        /* flat blocks (TCAD_FLAT_NODES nodes, never straddling instances) */
   int64_t n_tiles;       /* stencil tiles */
   /* per-instance tables (device memory) */
   const int32_t* shape;    /* [3*n_inst] Nx, Ny, Nz (Nz = 1 in 2D) */
-  const int64_t* node_off; /* [n_inst+1] */
+  const int64_t* node_off; /* [n_inst+1] first node of each instance, increasing;
+                              node_off[n_inst] = n_nodes */
   const int64_t* flat_off; /* [n_inst+1] first flat block of each instance */
   const int32_t* flat_inst;/* [n_flat] instance of each flat block */
   const int64_t* axis_off; /* [3*n_inst] start of the instance's x/y/z entries in h[]/dv[] */

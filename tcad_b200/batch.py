@@ -32,6 +32,7 @@ class DeviceBatch:
         self.n = len(self.devices)
         self.have_state = np.zeros(self.n, dtype=bool)
         self.last = None
+        self._guess = None   # bulk-guess potential, resident after first use
 
     def _ctypes_voltages(self, voltages):
         if voltages is None:
@@ -45,8 +46,10 @@ class DeviceBatch:
         """Equilibrium Poisson for every instance (one packed solve)."""
         opts = opts or NewtonOptions()
         pk = self.pack
-        guess = np.concatenate([d.setup.bulk_guess().ravel() for d in self.devices])
-        pk.psi.copy_(pk.torch.from_numpy(guess).to(pk.device))
+        if self._guess is None:
+            guess = np.concatenate([d.setup.bulk_guess().ravel() for d in self.devices])
+            self._guess = pk.torch.from_numpy(guess).to(pk.device)
+        pk.psi.copy_(self._guess)
         res = pk.equilibrium(opts)
         self.have_state[:] = True
         self.last = res

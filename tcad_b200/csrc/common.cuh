@@ -36,7 +36,7 @@ __device__ __forceinline__ Inst load_inst(const tcad_pack_t& pk, int inst) {
   g.ny = pk.shape[3 * inst + 1];
   g.nz = pk.shape[3 * inst + 2];
   g.off = pk.node_off[inst];
-  g.n = pk.node_off[inst + 1] - g.off;
+  g.n = (int64_t)g.nx * g.ny * g.nz;  // instances may sit apart (node_off need not be dense)
   return g;
 }
 
@@ -88,7 +88,8 @@ __device__ __forceinline__ FlatBlock flat_block(const tcad_pack_t& pk, int64_t b
   FlatBlock fb;
   fb.inst = pk.flat_inst[b];
   fb.ioff = pk.node_off[fb.inst];
-  fb.iend = pk.node_off[fb.inst + 1];
+  fb.iend = fb.ioff + (int64_t)pk.shape[3 * fb.inst] * pk.shape[3 * fb.inst + 1] *
+                          pk.shape[3 * fb.inst + 2];
   const int64_t local = b - pk.flat_off[fb.inst];
   fb.begin = fb.ioff + local * TCAD_FLAT_NODES;
   fb.end = fb.begin + TCAD_FLAT_NODES < fb.iend ? fb.begin + TCAD_FLAT_NODES : fb.iend;

@@ -199,10 +199,164 @@ class Setup:
         return cnt > 0, gk, gv, gveq, gb
 
 
+NODE_ARRAYS = ("C", "nie", "nie_s", "tau_n", "tau_p")
+BC_ARRAYS = ("bc_psi0", "bc_n0", "bc_p0", "bc_psi0_eq", "gate_k", "gate_v", "gate_veq",
+             "gate_b")
+
+
+def node_arrays(s):
+    """Per-node coefficient arrays of a set-up, flattened, by pack name."""
+    out = {name: getattr(s, name).ravel() for name in NODE_ARRAYS}
+    for a in range(s.dim):
+        for name in ("an", "ap", "dl"):
+            out[f"{name}{a}"] = getattr(s, name)[a].ravel()
+    return out
+
+
+def axis_arrays(s, dim):
+    """Per-axis (h, dv) of a set-up as packed: h padded with one 0 so that both
+    have the node count; axes beyond dim get a single (0, 1) entry."""
+    out = []
+    for a in range(3):
+        if a < dim:
+            out.append((np.concatenate([s.h[a], [0.0]]), s.dv[a]))
+        else:
+            out.append((np.zeros(1), np.ones(1)))
+    return out
+
+
+def instance_par(s):
+    par = np.zeros(_lib.NPAR)
+    par[0] = s.Ns
+    par[1] = s.R0
+    par[2] = s.mat.Cn_auger
+    par[3] = s.mat.Cp_auger
+    par[4] = 1.0 if s.models.srh else 0.0
+    par[5] = 1.0 if s.models.auger else 0.0
+    return par
+
+
+def instance_tiles(s, dim):
+    """Stencil tiles (i0, j0, k0) of one instance, x fastest."""
+    nz = s.nax[2] if dim == 3 else 1
+    kstep = _lib.TILE_Z if dim == 3 else 1
+    k0, j0, i0 = np.meshgrid(np.arange(0, nz, kstep), np.arange(0, s.nax[1], _lib.TILE_Y),
+                             np.arange(0, s.nax[0], _lib.TILE_X), indexing="ij")
+    return np.stack([i0.ravel(), j0.ravel(), k0.ravel()], axis=1).astype(np.int32)
+
+
+def instance_tables(setups, dim, node_off, axis_off, tiles=None):
+    """The per-instance tables of include/tcad_b200.h for instances placed at
+    node_off[i] (increasing) with axis entries at axis_off[i, a]."""
+    ni = len(setups)
+    sizes = [s.N for s in setups]
+    nflat = [-(-n // _lib.FLAT_NODES) for n in sizes]
+    flat_off = np.concatenate(([0], np.cumsum(nflat))).astype(np.int64)
+    flat_inst = np.repeat(np.arange(ni, dtype=np.int32), nflat)
+    shape = np.ones((ni, 3), dtype=np.int32)
+    for i, s in enumerate(setups):
+        shape[i, :dim] = s.nax[:dim]
+    tiles = tiles if tiles is not None else [instance_tiles(s, dim) for s in setups]
+    tl = (np.concatenate([np.concatenate([np.full((t.shape[0], 1), i, np.int32), t], axis=1)
+                          for i, t in enumerate(tiles)]).ravel()
+          if ni else np.zeros(0, np.int32))
+    par = np.stack([instance_par(s) for s in setups]) if ni else np.zeros((0, _lib.NPAR))
+    return dict(shape=shape.ravel(), node_off=np.asarray(node_off, np.int64),
+                flat_off=flat_off, flat_inst=flat_inst,
+                axis_off=np.asarray(axis_off, np.int64).ravel(), tile=tl.astype(np.int32),
+                par=par.ravel())
+
+
+def bc_node_arrays(s):
+    """Boundary-condition node arrays of one instance (local node index):
+    flag, psi0 at equilibrium on contacts, and the gate arrays; plus its
+    contact table."""
+    flag = np.zeros(s.N, dtype=np.uint8)
+    psi0eq = np.zeros(s.N)
+    names, nodes, cid, L, n0, p0 = s.contact_table()
+    g_on, g_k, g_v, g_veq, g_b = s.gate_arrays()
+    flag[g_on] |= _lib.BC_GATE
+    flag[nodes] |= _lib.BC_CONTACT
+    psi0eq[nodes] = 0.0 / s.VT + L
+    arrs = dict(bcflag=flag, bc_psi0_eq=psi0eq, gate_k=g_k, gate_v=g_v, gate_veq=g_veq,
+                gate_b=g_b)
+    return arrs, (names, nodes, cid, L, n0, p0)
+
+
+def gate_map(s):
+    """What the bias update needs to recompute V/VT - Vfb/VT on an
+    instance's gate nodes alone: the gates, each gate's slots among the gate
+    nodes, its kappa*w, the nodes' summed kappa*w, VT; and the local gate
+    nodes.  (None, None) when the instance has no gate."""
+    gates = [b for b in s.bcs.values() if b.kind == "gate"]
+    if not gates:
+        return None, None
+    on, gk, _, _, _ = s.gate_arrays()
+    nodes = np.nonzero(on)[0]
+    slot = np.full(s.N, -1, dtype=np.int64)
+    slot[nodes] = np.arange(nodes.size)
+    return (gates, [slot[b.nodes] for b in gates], [b.kappa * b.w for b in gates],
+            gk[nodes], s.VT), nodes
+
+
+def gate_values(gm):
+    """V/VT - Vfb/VT on the gate nodes, Setup.gate_arrays' arithmetic in the
+    same order (a node under several gates takes the kappa*w-weighted mean)."""
+    gates, slots, kws, gk, VT = gm
+    m = gk.size
+    gv = np.zeros(m); acc = np.zeros(m); cnt = np.zeros(m, dtype=np.int64)
+    for b, j, kw in zip(gates, slots, kws):
+        v = b.Vg / VT - b.Vfb / VT
+        first = cnt[j] == 0
+        gv[j] = np.where(first, v, gv[j])
+        acc[j] += kw * v
+        cnt[j] += 1
+    multi = cnt > 1
+    gv[multi] = acc[multi] / gk[multi]
+    return gv
+
+
 class Pack:
-    """Device-memory image of a list of Setups of one dimension."""
+    """Device-memory image of a list of Setups of one dimension, packed back
+    to back."""
 
     def __init__(self, setups, device="cuda"):
+        import torch
+        self._init_common(setups, device)
+        dim = self.dim
+        sizes = [s.N for s in self.setups]
+        node_off = np.concatenate(([0], np.cumsum(sizes))).astype(np.int64)
+        self.N = int(node_off[-1])
+        axes = [axis_arrays(s, dim) for s in self.setups]
+        axis_off = np.zeros((len(self.setups), 3), dtype=np.int64)
+        for a in range(3):
+            lens = [ax[a][1].size for ax in axes]
+            axis_off[:, a] = np.concatenate(([0], np.cumsum(lens)[:-1]))
+        up = self._up
+        t = {}
+        for a in range(3):
+            t[f"h{a}"] = up(np.concatenate([ax[a][0] for ax in axes]))
+            t[f"dv{a}"] = up(np.concatenate([ax[a][1] for ax in axes]))
+        per = [node_arrays(s) for s in self.setups]
+        for name in per[0]:
+            t[name] = up(np.concatenate([q[name] for q in per]))
+        for name in BC_ARRAYS:
+            t[name] = torch.zeros(self.N, dtype=torch.float64, device=self.device)
+        t["bcflag"] = torch.zeros(self.N, dtype=torch.uint8, device=self.device)
+        self.t = t
+        self._set_tables(instance_tables(self.setups, dim, node_off[:-1], axis_off))
+        # state and solver buffers
+        z = lambda n: torch.zeros(n, dtype=torch.float64, device=self.device)  # noqa: E731
+        self.psi, self.n, self.p = z(self.N), z(self.N), z(self.N)
+        self.F = z(3 * self.N)
+        self.J = z(_lib.NE[dim] * self.N)
+        self.du = z(3 * self.N)
+        wb = int(self.lib.tcad_block_workspace_bytes(self.pref, 0, 0))
+        self.work = torch.empty(wb, dtype=torch.uint8, device=self.device)
+        self.active = torch.ones(len(self.setups), dtype=torch.uint8, device=self.device)
+        self.refresh_bcs()
+
+    def _init_common(self, setups, device):
         import torch
         self.torch = torch
         self.setups = list(setups)
@@ -212,83 +366,36 @@ class Pack:
         self.dim = dims.pop()
         self.lib = _lib.load()
         self.device = torch.device(device)
-        dim = self.dim
+        self.last_h2d_bytes = 0
+
+    def _up(self, a, dtype=None):
+        torch = self.torch
+        return torch.from_numpy(np.ascontiguousarray(a)).to(self.device,
+                                                            dtype or torch.float64)
+
+    def _set_tables(self, tb):
+        """Upload the per-instance tables (instances at tb["node_off"], node
+        arrays of length self.N) and fill the C struct."""
+        torch = self.torch
+        t = self.t
         ni = len(self.setups)
-        sizes = [s.N for s in self.setups]
-        self.node_off = np.concatenate(([0], np.cumsum(sizes))).astype(np.int64)
-        self.N = int(self.node_off[-1])
-        nflat = [-(-n // _lib.FLAT_NODES) for n in sizes]
-        self.flat_off = np.concatenate(([0], np.cumsum(nflat))).astype(np.int64)
-        flat_inst = np.repeat(np.arange(ni, dtype=np.int32), nflat)
-        shape = np.ones((ni, 3), dtype=np.int32)
-        axis_off = np.zeros((ni, 3), dtype=np.int64)
-        hs = [[], [], []]; dvs = [[], [], []]
-        cur = [0, 0, 0]
-        for i, s in enumerate(self.setups):
-            for a in range(3):
-                if a < dim:
-                    shape[i, a] = s.nax[a]
-                    hh = np.concatenate([s.h[a], [0.0]])
-                    dd = s.dv[a]
-                else:
-                    hh, dd = np.zeros(1), np.ones(1)
-                axis_off[i, a] = cur[a]
-                cur[a] += hh.size
-                hs[a].append(hh); dvs[a].append(dd)
-        tiles = []
-        for i, s in enumerate(self.setups):
-            nz = s.nax[2] if dim == 3 else 1
-            kstep = _lib.TILE_Z if dim == 3 else 1
-            for k0 in range(0, nz, kstep):
-                for j0 in range(0, s.nax[1], _lib.TILE_Y):
-                    for i0 in range(0, s.nax[0], _lib.TILE_X):
-                        tiles.append((i, i0, j0, k0))
-        tiles = np.asarray(tiles, dtype=np.int32).ravel()
-        par = np.zeros((ni, _lib.NPAR))
-        for i, s in enumerate(self.setups):
-            par[i, 0] = s.Ns
-            par[i, 1] = s.R0
-            par[i, 2] = s.mat.Cn_auger
-            par[i, 3] = s.mat.Cp_auger
-            par[i, 4] = 1.0 if s.models.srh else 0.0
-            par[i, 5] = 1.0 if s.models.auger else 0.0
-        self.n_tiles = tiles.size // 4
+        self.node_off = np.concatenate([tb["node_off"][:ni], [self.N]]).astype(np.int64)
+        self.flat_off = tb["flat_off"]
         self.n_flat = int(self.flat_off[-1])
-
-        def cat(attr):
-            return np.concatenate([getattr(s, attr).ravel() for s in self.setups])
-
-        def up(a, dtype=torch.float64):
-            return torch.from_numpy(np.ascontiguousarray(a)).to(self.device, dtype)
-
-        t = {}
-        t["shape"] = up(shape.ravel(), torch.int32)
-        t["node_off"] = up(self.node_off, torch.int64)
-        t["flat_off"] = up(self.flat_off, torch.int64)
-        t["flat_inst"] = up(flat_inst, torch.int32)
-        t["axis_off"] = up(axis_off.ravel(), torch.int64)
-        t["tile"] = up(tiles, torch.int32)
-        t["par"] = up(par.ravel())
-        for a in range(3):
-            t[f"h{a}"] = up(np.concatenate(hs[a]))
-            t[f"dv{a}"] = up(np.concatenate(dvs[a]))
-        for name in ("C", "nie", "nie_s", "tau_n", "tau_p"):
-            t[name] = up(cat(name))
-        for a in range(dim):
-            for name in ("an", "ap", "dl"):
-                t[f"{name}{a}"] = up(np.concatenate([getattr(s, name)[a].ravel()
-                                                     for s in self.setups]))
-        for name in ("bc_psi0", "bc_n0", "bc_p0", "bc_psi0_eq", "gate_k", "gate_v",
-                     "gate_veq", "gate_b"):
-            t[name] = torch.zeros(self.N, dtype=torch.float64, device=self.device)
-        t["bcflag"] = torch.zeros(self.N, dtype=torch.uint8, device=self.device)
-        self.t = t
+        self.n_tiles = tb["tile"].size // 4
+        t["shape"] = self._up(tb["shape"], torch.int32)
+        t["node_off"] = self._up(self.node_off, torch.int64)
+        t["flat_off"] = self._up(tb["flat_off"], torch.int64)
+        t["flat_inst"] = self._up(tb["flat_inst"], torch.int32)
+        t["axis_off"] = self._up(tb["axis_off"], torch.int64)
+        t["tile"] = self._up(tb["tile"], torch.int32)
+        t["par"] = self._up(tb["par"])
+        dim = self.dim
         P = _lib.TcadPack()
         P.dim = dim; P.n_inst = ni; P.n_nodes = self.N
         P.n_flat = self.n_flat; P.n_tiles = self.n_tiles
         for f in ("shape", "node_off", "flat_off", "flat_inst", "axis_off", "tile", "par",
-                  "C", "nie", "nie_s", "tau_n", "tau_p", "bcflag", "bc_psi0", "bc_n0",
-                  "bc_p0", "bc_psi0_eq", "gate_k", "gate_v", "gate_veq", "gate_b"):
+                  "C", "nie", "nie_s", "tau_n", "tau_p", "bcflag") + BC_ARRAYS:
             setattr(P, f, t[f].data_ptr())
         for a in range(3):
             P.h[a] = t[f"h{a}"].data_ptr()
@@ -299,17 +406,6 @@ class Pack:
             P.dl[a] = t[f"dl{src}"].data_ptr()
         self.P = P
         self.pref = ctypes.byref(P)
-        # state and solver buffers
-        z = lambda n: torch.zeros(n, dtype=torch.float64, device=self.device)  # noqa: E731
-        self.psi, self.n, self.p = z(self.N), z(self.N), z(self.N)
-        self.F = z(3 * self.N)
-        self.J = z(_lib.NE[dim] * self.N)
-        self.du = z(3 * self.N)
-        wb = int(self.lib.tcad_block_workspace_bytes(self.pref, 0, 0))
-        self.work = torch.empty(wb, dtype=torch.uint8, device=self.device)
-        self.active = torch.ones(ni, dtype=torch.uint8, device=self.device)
-        self.contact_nodes = [None] * ni
-        self.refresh_bcs()
 
     # ---------------------------------------------------------------------
     def sp(self):
@@ -319,54 +415,74 @@ class Pack:
         """(Re)build the boundary-condition arrays from every instance's BCs."""
         torch = self.torch
         N = self.N
-        flag = np.zeros(N, dtype=np.uint8)
-        psi0eq = np.zeros(N)
-        gk = np.zeros(N); gv = np.zeros(N); gveq = np.zeros(N); gb = np.zeros(N)
+        full = {"bcflag": np.zeros(N, dtype=np.uint8)}
+        for name in ("bc_psi0_eq", "gate_k", "gate_v", "gate_veq", "gate_b"):
+            full[name] = np.zeros(N)
+        tables = []
+        for i, s in enumerate(self.setups):
+            off = int(self.node_off[i])
+            arrs, ctab = bc_node_arrays(s)
+            for name, a in arrs.items():
+                full[name][off:off + s.N] = a
+            tables.append(ctab)
+        for name, a in full.items():
+            self.t[name].copy_(self._up(a, torch.uint8 if name == "bcflag" else None))
+        self._contact_tables(tables)
+        self._build_gate_map()
+        self.set_bias()
+
+    def _contact_tables(self, tables):
+        """Device contact lists from each instance's contact table (local node
+        indices) placed at node_off[i]."""
+        torch = self.torch
         c_nodes, c_cid, c_L, c_n0, c_p0 = [], [], [], [], []
         self.c_off = [0]
         self.contact_names = []
         self.cid_base = []
         base = 0
-        for i, s in enumerate(self.setups):
+        for i, (names, nodes, cid, L, n0, p0) in enumerate(tables):
             off = int(self.node_off[i])
-            names, nodes, cid, L, n0, p0 = s.contact_table()
             self.contact_names.append(names)
             self.cid_base.append(base)
-            g_on, g_k, g_v, g_veq, g_b = s.gate_arrays()
-            sl = slice(off, off + s.N)
-            flag[sl][g_on] |= _lib.BC_GATE
-            gk[sl] = g_k; gv[sl] = g_v; gveq[sl] = g_veq; gb[sl] = g_b
-            flag[off + nodes] |= _lib.BC_CONTACT
-            psi0eq[off + nodes] = 0.0 / s.VT + L
             c_nodes.append(off + nodes); c_cid.append(base + cid)
             self.c_off.append(self.c_off[-1] + nodes.size)
             c_L.append(L); c_n0.append(n0); c_p0.append(p0)
             base += len(names)
         self.n_contacts_total = base
-        up = lambda a, dt=torch.float64: torch.from_numpy(  # noqa: E731
-            np.ascontiguousarray(a)).to(self.device, dt)
-        self.t["bcflag"].copy_(up(flag, torch.uint8))
-        self.t["bc_psi0_eq"].copy_(up(psi0eq))
-        self.t["gate_k"].copy_(up(gk)); self.t["gate_v"].copy_(up(gv))
-        self.t["gate_veq"].copy_(up(gveq)); self.t["gate_b"].copy_(up(gb))
-        self.c_nodes = up(np.concatenate(c_nodes) if c_nodes else np.zeros(0), torch.int64)
-        self.c_cid = up(np.concatenate(c_cid) if c_cid else np.zeros(0), torch.int32)
-        self.c_L = up(np.concatenate(c_L) if c_L else np.zeros(0))
-        self.c_n0 = up(np.concatenate(c_n0) if c_n0 else np.zeros(0))
-        self.c_p0 = up(np.concatenate(c_p0) if c_p0 else np.zeros(0))
-        self._gate_host = gv
+        cat = lambda xs: np.concatenate(xs) if xs else np.zeros(0)  # noqa: E731
+        self.c_nodes = self._up(cat(c_nodes), torch.int64)
+        self.c_cid = self._up(cat(c_cid), torch.int32)
+        self.c_L = self._up(cat(c_L))
+        self.c_n0 = self._up(cat(c_n0))
+        self.c_p0 = self._up(cat(c_p0))
         # per contact: device node list (for terminal currents)
         self.contact_lists = {}
         for i, s in enumerate(self.setups):
             off = int(self.node_off[i])
             for name, b in s.bcs.items():
                 if b.kind == "contact":
-                    self.contact_lists[(i, name)] = up(off + np.unique(b.nodes), torch.int64)
+                    self.contact_lists[(i, name)] = self._up(off + np.unique(b.nodes),
+                                                             torch.int64)
         maxc = max([v.numel() for v in self.contact_lists.values()] + [1])
         self.cur_partial = torch.zeros(2 * maxc, dtype=torch.float64, device=self.device)
         self.cur_out = torch.zeros(max(len(self.contact_lists), 1), dtype=torch.float64,
                                    device=self.device)
-        self.set_bias()
+
+    def _build_gate_map(self, cached=None):
+        """Per instance with gates: gate map and global gate nodes (increasing)
+        for set_bias; cached: optional per-instance (map, local nodes)."""
+        self._gate_maps, self._gate_inst, idx = {}, [], []
+        for i, s in enumerate(self.setups):
+            gm, nodes = cached[i] if cached is not None else gate_map(s)
+            if gm is None:
+                continue
+            self._gate_maps[i] = gm
+            self._gate_inst.append(i)
+            idx.append(int(self.node_off[i]) + nodes)
+        self._gate_idx = self._up(np.concatenate(idx), self.torch.int64) if idx else None
+
+    def _gate_values(self, i):
+        return gate_values(self._gate_maps[i])
 
     def set_bias(self, voltages=None):
         """Contact targets at each contact's voltage and the gates' Vg terms.
@@ -385,17 +501,16 @@ class Pack:
             _lib.ptr(self.t["bc_psi0"]), _lib.ptr(self.t["bc_n0"]), _lib.ptr(self.t["bc_p0"]),
             self.sp())
         _lib.check(rc, "tcad_set_contacts")
-        # gate V/VT - Vfb/VT at the current Vg (host recompute: gate sets are small
-        # relative to the mesh, the upload is one node array)
-        gv = np.zeros(self.N)
-        changed = False
-        for i, s in enumerate(self.setups):
-            if any(b.kind == "gate" for b in s.bcs.values()):
-                off = int(self.node_off[i])
-                gv[off:off + s.N] = s.gate_arrays()[2]
-                changed = True
-        if changed:
-            self.t["gate_v"].copy_(torch.from_numpy(gv).to(self.device))
+        # gate V/VT - Vfb/VT at the current Vg, recomputed on the gate nodes
+        # only (the arithmetic of Setup.gate_arrays, in the same order) and
+        # scattered into the node array on the device
+        self.last_h2d_bytes = vv.nbytes
+        if self._gate_idx is not None:
+            vals = np.concatenate([self._gate_values(i) for i in self._gate_inst])
+            vt = torch.from_numpy(vals).to(self.device)
+            self.t["gate_v"].index_copy_(0, self._gate_idx, vt)
+            self.last_h2d_bytes += vals.nbytes
+            self._gvt = vt
         self._vvt = vvt  # keep alive until the kernel ran
 
     def stamp_contacts(self, active=None):

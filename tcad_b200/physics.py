@@ -201,29 +201,49 @@ def graded_nodes(n, L, focus, ratio):
     size of pytcad/mesh.py:30-116 (graded_mesh), i.e. a geometric series of
     cell sizes with the given ratio -- with h0 chosen so that the node count
     is exactly n.  Used by the workload builders, which need explicit node
-    counts."""
-    focus = np.sort(np.clip(np.atleast_1d(np.asarray(focus, dtype=float)), 0.0, L))
+    counts.
+
+    The node density 1/s(d) is integrated in closed form: between the
+    breakpoints (ends, focus points, midpoints between focus points) d is
+    linear with slope +-1, so the cell count over a piece is
+    |ln(s(d_b) / s(d_a))| / g, and the count-to-position map inverts with an
+    exponential."""
+    focus = np.unique(np.clip(np.atleast_1d(np.asarray(focus, dtype=float)), 0.0, L))
     if n < 2:
         raise ValueError("need at least 2 nodes")
     g = ratio - 1.0
-    xs = np.linspace(0.0, L, 400001)
-    d = np.min(np.abs(xs[:, None] - focus[None, :]), axis=1)
+    bp = np.unique(np.concatenate(([0.0, L], focus, 0.5 * (focus[1:] + focus[:-1]))))
+    a, b = bp[:-1], bp[1:]
+    dist = lambda x: np.min(np.abs(np.asarray(x)[:, None] - focus[None, :]), axis=1)  # noqa: E731
+    da, db = dist(a), dist(b)
+    up = db >= da                      # d grows along the piece
 
-    def cells(h0):
-        w = 1.0 / (h0 + g * d)
-        return np.concatenate(([0.0], np.cumsum(0.5 * (w[1:] + w[:-1]) * np.diff(xs))))
+    def counts(h0):
+        if g == 0.0:
+            return (b - a) / h0
+        return np.abs(np.log((h0 + g * db) / (h0 + g * da))) / g
 
-    lo, hi = L * 1e-9, L
-    for _ in range(200):            # bisection on h0 (log scale)
+    lo, hi = L * 1e-12, 2.0 * L
+    for _ in range(300):               # bisection on h0 (log scale)
         h0 = np.sqrt(lo * hi)
-        if cells(h0)[-1] > n - 1:
+        if counts(h0).sum() > n - 1:
             lo = h0
         else:
             hi = h0
-        if hi / lo < 1.0 + 1e-13:
+        if hi / lo < 1.0 + 1e-15:
             break
-    cum = cells(np.sqrt(lo * hi))
-    cum /= cum[-1]
-    x = np.interp(np.linspace(0.0, 1.0, n), cum, xs)
+    h0 = np.sqrt(lo * hi)
+    c = counts(h0)
+    c *= (n - 1) / c.sum()             # exact total, the bisection's residue spread
+    C = np.concatenate(([0.0], np.cumsum(c)))
+    t = np.arange(n, dtype=float)
+    seg = np.clip(np.searchsorted(C, t, side="right") - 1, 0, a.size - 1)
+    u = np.minimum(t - C[seg], c[seg])
+    sa = h0 + g * da[seg]
+    if g == 0.0:
+        dd = u * h0
+    else:
+        dd = np.where(up[seg], (sa * np.expm1(g * u)) / g, (sa * -np.expm1(-g * u)) / g)
+    x = np.minimum(a[seg] + dd, b[seg])
     x[0], x[-1] = 0.0, L
     return x

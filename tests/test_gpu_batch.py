@@ -62,3 +62,21 @@ def test_batch_mask_keeps_inactive_state():
     after = batch.state(1)
     for a, b in zip(before, after):
         assert np.array_equal(a, b)
+
+
+def test_gate_bias_upload_matches_setup():
+    """set_bias recomputes V/VT - Vfb/VT on the gate nodes alone and
+    scatters it: the device array equals the full-mesh host recomputation
+    bit for bit, including nodes under two gates (the tri-gate corners)."""
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    from tcad_b200.pack import Pack
+    devs = [_build(PARAMS[0]), W.trigate3d(tb.Device3D, 24, 16, 12)]
+    for d, volts in ((devs[0], {"gate": 0.7}),
+                     (devs[1], {"gate_top": 0.3, "gate_left": 0.8, "gate_right": 0.55})):
+        pk = Pack([d.setup])
+        d._apply_voltages(volts)
+        pk.set_bias()
+        want = d.setup.gate_arrays()[2]
+        assert np.array_equal(pk.t["gate_v"].cpu().numpy(), want)
+        assert pk.last_h2d_bytes < 8 * d.N / 4

@@ -90,3 +90,28 @@ def test_product_does_not_import_oracle():
             if f.endswith((".py", ".cu", ".cuh")):
                 txt = open(os.path.join(dirpath, f)).read()
                 assert "import oracle" not in txt and "from oracle" not in txt, f
+
+
+def test_range_allocator_first_fit_and_coalescing():
+    from tcad_b200.serve import RangeAllocator
+    a = RangeAllocator(1000, align=10)
+    x = a.alloc(95)          # rounds to 100
+    y = a.alloc(200)
+    z = a.alloc(300)
+    assert (x, y, z) == (0, 100, 300)
+    assert a.alloc(500) is None and a.largest() == 400
+    a.release(y, 200)
+    assert a.alloc(150) == 100           # first fit into the hole
+    a.release(100, 150)
+    a.release(x, 95)
+    assert a.free[0] == (0, 300)         # coalesced with the hole
+    a.release(z, 300)
+    assert a.free == [(0, 1000)] and a.free_total() == 1000
+
+
+def test_arena_bytes_per_node():
+    from tcad_b200.serve import bytes_per_node
+    # coefficients + BC + state + F + J + du (doubles), bcflag, FP64 and FP32
+    # Krylov workspace
+    assert 780 <= bytes_per_node(2) <= 840
+    assert 920 <= bytes_per_node(3) <= 1000
