@@ -49,10 +49,10 @@ extern "C" {
 
 #define TCAD_NE2 29
 #define TCAD_NE3 39
-#define TCAD_FLAT_NODES 1024 /* nodes per flat (vector-kernel) block */
+#define TCAD_FLAT_NODES 1024 /* default nodes per flat (vector-kernel) block */
 #define TCAD_TILE_X 32       /* stencil tile: 32 x 8 nodes (x, y) */
 #define TCAD_TILE_Y 8
-#define TCAD_TILE_Z 16       /* z planes marched by one 3D stencil tile */
+#define TCAD_TILE_Z 16       /* largest z depth of a 3D stencil tile (tile_z <= this) */
 
 /* per-instance scalar parameters: par[i*TCAD_NPAR + TCAD_P_*] */
 #define TCAD_NPAR 8
@@ -75,8 +75,11 @@ typedef struct tcad_pack {
   int32_t dim;           /* 2 or 3 */
   int32_t n_inst;        /* packed instances */
   int64_t n_nodes;       /* length of every node array (>= the last instance's end) */
-  int64_t n_flat;        /* flat blocks (TCAD_FLAT_NODES nodes, never straddling instances) */
+  int64_t n_flat;        /* flat blocks (flat_nodes nodes, never straddling instances) */
   int64_t n_tiles;       /* stencil tiles */
+  int32_t tile_z;        /* z planes one 3D tile marches (1..TCAD_TILE_Z; the tiles'
+                            k0 are multiples of it); 1 in 2D */
+  int32_t flat_nodes;    /* nodes per flat block (>= 1; each instance starts a block) */
   /* per-instance tables (device memory) */
   const int32_t* shape;    /* [3*n_inst] Nx, Ny, Nz (Nz = 1 in 2D) */
   const int64_t* node_off; /* [n_inst+1] first node of each instance, increasing;
@@ -175,6 +178,16 @@ size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart
  * block with |det| < 1e-300 or a non-finite entry. */
 int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
                             int32_t* status, void* stream);
+
+/* The same set-up in relative unknowns (u_psi, u_n, u_p) = (dpsi, dn/s_n,
+ * dp/s_p) with s_n = max(n, dens_floor), s_p = max(p, dens_floor) at the
+ * node: J and F are prepared for A^ = S^-1 D^-1 A S, S = diag(1, s_n, s_p),
+ * and b^ = S^-1 D^-1 (-F).  The Krylov solve of tcad_newton_solve with
+ * density_scaling = 1 runs on this operator; the update the reference's
+ * Newton measures (pytcad/device2d.py:2079-2100) is relative in n and p. */
+int tcad_block_jacobi_setup_rel(const tcad_pack_t* pk, double* J, double* F,
+                                int32_t* status, const double* n, const double* p,
+                                double dens_floor, void* stream);
 
 /* y = A^ x with A^ = I + D^-1 (off-diagonal blocks), J prepared by
  * tcad_block_jacobi_setup; x, y are [3][n_nodes]. */

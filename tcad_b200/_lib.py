@@ -23,7 +23,7 @@ STATUS_NAMES = {0: "ok", 1: "bad argument", 2: "singular node block",
 
 NE = {2: 29, 3: 39}
 FLAT_NODES = 1024
-TILE_X, TILE_Y, TILE_Z = 32, 8, 16
+TILE_X, TILE_Y, TILE_Z_MAX = 32, 8, 16
 NPAR = 8
 MODE_RAW, MODE_ELIMINATE = 0, 1
 BC_CONTACT, BC_GATE = 1, 2
@@ -36,7 +36,8 @@ class TcadPack(ctypes.Structure):
     _fields_ = [
         ("dim", ctypes.c_int32), ("n_inst", ctypes.c_int32),
         ("n_nodes", ctypes.c_int64), ("n_flat", ctypes.c_int64),
-        ("n_tiles", ctypes.c_int64),
+        ("n_tiles", ctypes.c_int64), ("tile_z", ctypes.c_int32),
+        ("flat_nodes", ctypes.c_int32),
         ("shape", _p), ("node_off", _p), ("flat_off", _p), ("flat_inst", _p),
         ("axis_off", _p), ("tile", _p), ("par", _p),
         ("h", _p * 3), ("dv", _p * 3),
@@ -78,6 +79,8 @@ _SIGS = {
     "tcad_poisson_assemble": (ctypes.c_int, [_p, _p, _p, _p, ctypes.c_int, _p]),
     "tcad_block_workspace_bytes": (ctypes.c_size_t, [_p, ctypes.c_int, ctypes.c_int]),
     "tcad_block_jacobi_setup": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "tcad_block_jacobi_setup_rel": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, ctypes.c_double,
+                                                   _p]),
     "tcad_block_spmv": (ctypes.c_int, [_p, _p, _p, _p, _p]),
     "tcad_block_krylov": (ctypes.c_int, [_p, _p, _p, _p, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_int, ctypes.c_int, _p, ctypes.c_size_t,

@@ -7,7 +7,7 @@
 // line).  The tile's plane values plus a one-node halo are staged in shared
 // memory; every x- and y-edge touching the tile is evaluated ONCE (Bernoulli
 // functions included) into shared memory and read by both endpoint nodes.
-// In 3D the CTA marches up to TCAD_TILE_Z planes in z, carrying the z-edge
+// In 3D the CTA marches up to pk.tile_z planes in z, carrying the z-edge
 // between consecutive planes in registers (the up-edge of plane k is the
 // down-edge of plane k+1), so z-edges are also evaluated once.
 #include "sg_edge.cuh"
@@ -46,7 +46,7 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
   const int64_t sxy = (int64_t)g.nx * g.ny;
   const int64_t NN = pk.n_nodes;
   const double* par = pk.par + TCAD_NPAR * inst;
-  const int kend = DIM == 3 ? min(k0 + TCAD_TILE_Z, g.nz) : 1;
+  const int kend = DIM == 3 ? min(k0 + pk.tile_z, g.nz) : 1;
 
   // z-march registers (3D): own node values of the current / next plane
   NodeVals cur{0.0, 0.0, 0.0}, nxt{0.0, 0.0, 0.0};
@@ -473,7 +473,7 @@ using namespace tcad;
 extern "C" int tcad_sg_assemble(const tcad_pack_t* pk, const double* psi, const double* n,
                                 const double* p, double* F, double* J, int mode,
                                 void* stream) {
-  if (!pk || (pk->dim != 2 && pk->dim != 3) || pk->n_tiles <= 0) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || pk->n_tiles <= 0) return TCAD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const unsigned nt = (unsigned)pk->n_tiles;
   if (pk->dim == 2)
@@ -489,7 +489,7 @@ extern "C" int tcad_contact_current(const tcad_pack_t* pk, const double* psi,
                                     const double* n, const double* p,
                                     const int64_t* nodes, int64_t count, double* partial,
                                     int64_t partial_len, double* out_sum, void* stream) {
-  if (!pk || count < 0 || partial_len < 2 * count) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || count < 0 || partial_len < 2 * count) return TCAD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   if (count > 0) {
     const unsigned nb_ = (unsigned)((count + 255) / 256);
@@ -509,7 +509,7 @@ extern "C" int tcad_contact_current(const tcad_pack_t* pk, const double* psi,
 extern "C" int tcad_edge_currents(const tcad_pack_t* pk, int axis, const double* psi,
                                   const double* n, const double* p, double* Jn,
                                   double* Jp, void* stream) {
-  if (!pk || axis < 0 || axis >= pk->dim) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || axis < 0 || axis >= pk->dim) return TCAD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const unsigned nb_ = (unsigned)pk->n_flat;
   if (pk->dim == 2)
@@ -523,7 +523,7 @@ extern "C" int tcad_edge_currents(const tcad_pack_t* pk, int axis, const double*
 
 extern "C" int tcad_poisson_assemble(const tcad_pack_t* pk, const double* psi, double* F,
                                      double* J, int mode, void* stream) {
-  if (!pk || (pk->dim != 2 && pk->dim != 3)) return TCAD_ERR_ARG;
+  if (!pack_ok(pk)) return TCAD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const unsigned nb_ = (unsigned)pk->n_flat;
   if (pk->dim == 2)

@@ -35,7 +35,7 @@ extern "C" int tcad_set_contacts(const tcad_pack_t* pk, const int64_t* nodes, in
                                  const int32_t* cid, const double* vv, const double* L,
                                  const double* n0, const double* p0, double* bc_psi0,
                                  double* bc_n0, double* bc_p0, void* stream) {
-  if (!pk || count < 0) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || count < 0) return TCAD_ERR_ARG;
   if (count == 0) return TCAD_OK;
   k_set_contacts<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       nodes, count, cid, vv, L, n0, p0, bc_psi0, bc_n0, bc_p0);
@@ -46,7 +46,7 @@ extern "C" int tcad_set_contacts(const tcad_pack_t* pk, const int64_t* nodes, in
 
 extern "C" int tcad_stamp_contacts(const tcad_pack_t* pk, const int64_t* nodes, int64_t count,
                                    double* psi, double* n, double* p, void* stream) {
-  if (!pk || count < 0) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || count < 0) return TCAD_ERR_ARG;
   if (count == 0) return TCAD_OK;
   k_stamp_contacts<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       *pk, nodes, count, psi, n, p);

@@ -20,8 +20,14 @@ namespace tcad {
 void note_launch(uint64_t n = 1);
 
 constexpr int kFlatThreads = 256;
-constexpr int kFlatPerThread = TCAD_FLAT_NODES / kFlatThreads;  // 4
 constexpr int kTileThreads = TCAD_TILE_X * TCAD_TILE_Y;           // 256
+
+// Host-side sanity of the pack's launch-shape fields (the tables themselves
+// are the caller's responsibility).
+inline bool pack_ok(const tcad_pack_t* pk) {
+  return pk && (pk->dim == 2 || pk->dim == 3) && pk->n_inst >= 0 && pk->flat_nodes >= 1 &&
+         (pk->dim == 2 || (pk->tile_z >= 1 && pk->tile_z <= TCAD_TILE_Z));
+}
 
 // Geometry of one instance as seen by a kernel.
 struct Inst {
@@ -75,7 +81,7 @@ __device__ __forceinline__ double block_max(double v, double* smem) {
   return r;
 }
 
-// Flat-block addressing: block b of the pack covers TCAD_FLAT_NODES nodes of
+// Flat-block addressing: block b of the pack covers pk.flat_nodes nodes of
 // exactly one instance.  Returns the instance, the first node of the block
 // and the instance's end node.
 struct FlatBlock {
@@ -91,8 +97,8 @@ __device__ __forceinline__ FlatBlock flat_block(const tcad_pack_t& pk, int64_t b
   fb.iend = fb.ioff + (int64_t)pk.shape[3 * fb.inst] * pk.shape[3 * fb.inst + 1] *
                           pk.shape[3 * fb.inst + 2];
   const int64_t local = b - pk.flat_off[fb.inst];
-  fb.begin = fb.ioff + local * TCAD_FLAT_NODES;
-  fb.end = fb.begin + TCAD_FLAT_NODES < fb.iend ? fb.begin + TCAD_FLAT_NODES : fb.iend;
+  fb.begin = fb.ioff + local * pk.flat_nodes;
+  fb.end = fb.begin + pk.flat_nodes < fb.iend ? fb.begin + pk.flat_nodes : fb.iend;
   return fb;
 }
 

@@ -1,6 +1,6 @@
 // Node-block linear algebra, Krylov solvers and the Newton drivers.
 //
-// All kernels are "flat": block b owns TCAD_FLAT_NODES consecutive nodes of
+// All kernels are "flat": block b owns pk.flat_nodes consecutive nodes of
 // one instance (flat_block()).  Reductions are per instance and
 // deterministic: each block writes its partial sums, and the LAST block of
 // the instance to finish (atomic ticket) sums the partials in block order and
@@ -643,10 +643,14 @@ k_to_f32(const tcad_pack_t pk, int ne, const double* __restrict__ J, float* __re
       J32[(int64_t)e * NN + k] = (float)J[(int64_t)e * NN + k];
 }
 
-// x = 0, r32 = (float) b, ||b||^2
+// x = 0, ||b||^2.  The refinement keeps its residual in FP64 and hands the
+// inner FP32 solve r / ||r|| (k_ir_scale): the scaled right-hand side of a
+// Newton step far from the solution can exceed the FP32 range where the
+// relative unknowns divide by a density at the floor; normalised, every
+// entry is at most 1 and the FP32 solve sees a unit-norm system.
 __global__ void __launch_bounds__(NT)
 k_ir_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict__ x,
-          float* __restrict__ r32, KState* irs, double* partial, unsigned* ticket) {
+          KState* irs, double* partial, unsigned* ticket) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const int64_t NN = pk.n_nodes;
   double v[1] = {0.0};
@@ -656,7 +660,6 @@ k_ir_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict
       const int64_t q = c * NN + k;
       const double bv = b[q];
       x[q] = 0.0;
-      r32[q] = (float)bv;
       v[0] += bv * bv;
     }
   }
@@ -667,23 +670,38 @@ k_ir_init(const tcad_pack_t pk, const double* __restrict__ b, double* __restrict
   }
 }
 
-// x += d32 for the instances still refining
+// r32 = (float)(r / ||r||) for the instances still refining (||r||^2 in irs)
 __global__ void __launch_bounds__(NT)
-k_ir_axpy(const tcad_pack_t pk, double* __restrict__ x, const float* __restrict__ d,
-          const int32_t* __restrict__ pre_status) {
+k_ir_scale(const tcad_pack_t pk, const double* __restrict__ r, float* __restrict__ r32,
+           const KState* irs, const int32_t* __restrict__ pre_status) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   if (pre_status[fb.inst] != TCAD_OK) return;
   const int64_t NN = pk.n_nodes;
+  const double nrm = sqrt(irs[fb.inst].rr);
+  const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) x[c * NN + k] += (double)d[c * NN + k];
+    for (int c = 0; c < 3; ++c) r32[c * NN + k] = (float)(r[c * NN + k] * inv);
 }
 
-// r = b - A^ x in FP64 (FP64 operator), r32 = (float) r, ||r||^2
+// x += ||r|| d32 for the instances still refining (d32 solves A^ d = r/||r||)
+__global__ void __launch_bounds__(NT)
+k_ir_axpy(const tcad_pack_t pk, double* __restrict__ x, const float* __restrict__ d,
+          const KState* irs, const int32_t* __restrict__ pre_status) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  if (pre_status[fb.inst] != TCAD_OK) return;
+  const int64_t NN = pk.n_nodes;
+  const double nrm = sqrt(irs[fb.inst].rr);
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[c * NN + k] += nrm * (double)d[c * NN + k];
+}
+
+// r = b - A^ x in FP64 (FP64 operator) into r64, ||r||^2
 template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_ir_resid(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ b,
-           const double* __restrict__ x, float* __restrict__ r32, KState* irs,
+           const double* __restrict__ x, double* __restrict__ r64, KState* irs,
            const int32_t* __restrict__ pre_status, double* partial, unsigned* ticket) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   if (pre_status[fb.inst] != TCAD_OK) return;
@@ -696,7 +714,7 @@ k_ir_resid(const tcad_pack_t pk, const double* __restrict__ J, const double* __r
     double y0, y1, y2;
     spmv_node<DIM, true, double>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
     const double a0 = b[k] - y0, a1 = b[NN + k] - y1, a2 = b[2 * NN + k] - y2;
-    r32[k] = (float)a0; r32[NN + k] = (float)a1; r32[2 * NN + k] = (float)a2;
+    r64[k] = a0; r64[NN + k] = a1; r64[2 * NN + k] = a2;
     v[0] += a0 * a0 + a1 * a1 + a2 * a2;
   }
   double tot[1];
@@ -877,7 +895,7 @@ static int solve_mixed(const tcad_pack_t* pk, const double* J, const double* b, 
   k_to_f32<<<nb, NT, 0, s>>>(*pk, ne, J, w32.J32);
   note_launch();
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
-  k_ir_init<<<nb, NT, 0, s>>>(*pk, b, x, w32.r32, w32.irs, w.partial, w.ticket);
+  k_ir_init<<<nb, NT, 0, s>>>(*pk, b, x, w32.irs, w.partial, w.ticket);
   note_launch();
   TCAD_LAUNCH_CHECK();
   std::vector<KState> irs(ni);
@@ -911,6 +929,9 @@ static int solve_mixed(const tcad_pack_t* pk, const double* J, const double* b, 
                                     cudaMemcpyHostToDevice, s));
     TCAD_CUDA_CHECK(cudaMemcpyAsync(w32.eta_in, eta_in.data(), sizeof(double) * ni,
                                     cudaMemcpyHostToDevice, s));
+    // the FP64 residual lives in the (idle) first FP64 Krylov vector
+    k_ir_scale<<<nb, NT, 0, s>>>(*pk, ir == 0 ? b : w.bi.r, w32.r32, w32.irs, w32.pre);
+    note_launch();
     int rc = launch_bicgstab_t<float>(pk, w32.J32, w32.r32, w32.d32, 1e-4, inner_maxiter,
                                       w32.bi, w, w32.pre, hks, s, w32.eta_in);
     if (rc != TCAD_OK) return rc;
@@ -920,13 +941,13 @@ static int solve_mixed(const tcad_pack_t* pk, const double* J, const double* b, 
       if (hks[i].status == TCAD_ERR_NONFINITE || hks[i].status == TCAD_ERR_BREAKDOWN)
         res_status[i] = hks[i].status;
     }
-    k_ir_axpy<<<nb, NT, 0, s>>>(*pk, x, w32.d32, w32.pre);
+    k_ir_axpy<<<nb, NT, 0, s>>>(*pk, x, w32.d32, w32.irs, w32.pre);
     note_launch();
     if (pk->dim == 2)
-      k_ir_resid<2><<<nb, NT, 0, s>>>(*pk, J, b, x, w32.r32, w32.irs, w32.pre, w.partial,
+      k_ir_resid<2><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w32.irs, w32.pre, w.partial,
                                       w.ticket);
     else
-      k_ir_resid<3><<<nb, NT, 0, s>>>(*pk, J, b, x, w32.r32, w32.irs, w32.pre, w.partial,
+      k_ir_resid<3><<<nb, NT, 0, s>>>(*pk, J, b, x, w.bi.r, w32.irs, w32.pre, w.partial,
                                       w.ticket);
     note_launch();
     TCAD_LAUNCH_CHECK();
@@ -986,7 +1007,7 @@ extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, 
 
 extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
                                        int32_t* status, void* stream) {
-  if (!pk || !J || !F || !status) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || !J || !F || !status) return TCAD_ERR_ARG;
   if (pk->dim == 2)
     k_bj_setup<2><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status,
                                                                          nullptr, nullptr, 0.0);
@@ -998,9 +1019,25 @@ extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double*
   return TCAD_OK;
 }
 
+extern "C" int tcad_block_jacobi_setup_rel(const tcad_pack_t* pk, double* J, double* F,
+                                           int32_t* status, const double* n, const double* p,
+                                           double dens_floor, void* stream) {
+  if (!pack_ok(pk) || !J || !F || !status || !n || !p || !(dens_floor > 0.0))
+    return TCAD_ERR_ARG;
+  if (pk->dim == 2)
+    k_bj_setup<2><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status, n,
+                                                                         p, dens_floor);
+  else
+    k_bj_setup<3><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status, n,
+                                                                         p, dens_floor);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
 extern "C" int tcad_block_spmv(const tcad_pack_t* pk, const double* J, const double* x,
                                double* y, void* stream) {
-  if (!pk) return TCAD_ERR_ARG;
+  if (!pack_ok(pk)) return TCAD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   if (pk->dim == 2)
     k_spmv<2, true><<<(unsigned)pk->n_flat, NT, 0, s>>>(*pk, J, x, y);
@@ -1015,7 +1052,7 @@ extern "C" int tcad_block_krylov(const tcad_pack_t* pk, const double* J, const d
                                  double* x, int method, double rtol, int maxiter,
                                  int restart, void* work, size_t work_bytes, int32_t* iters,
                                  int32_t* status, double* relres, void* stream) {
-  if (!pk || !work) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || !work) return TCAD_ERR_ARG;
   if (method != 0) return TCAD_ERR_ARG;  // GMRES on the block layout: not in this library
   (void)restart;
   Work w = carve(pk, work, work_bytes);
@@ -1036,7 +1073,7 @@ extern "C" int tcad_newton_update(const tcad_pack_t* pk, double* psi, double* n,
                                   const double* du, double max_dpsi, double dens_floor,
                                   const uint8_t* active, double* partial, double* err,
                                   void* stream) {
-  if (!pk) return TCAD_ERR_ARG;
+  if (!pack_ok(pk)) return TCAD_ERR_ARG;
   (void)partial;
   cudaStream_t s = (cudaStream_t)stream;
   TCAD_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(double) * pk->n_inst, s));
@@ -1053,7 +1090,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
                                  const tcad_newton_opts_t* opts, uint8_t* active,
                                  void* work, size_t work_bytes,
                                  tcad_newton_result_t* result, void* stream) {
-  if (!pk || !opts || !active || !result || !work) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || !opts || !active || !result || !work) return TCAD_ERR_ARG;
   if (opts->method != 0) return TCAD_ERR_ARG;
   Work w = carve(pk, work, work_bytes);
   if (w.bytes > work_bytes) return TCAD_ERR_ARG;
@@ -1246,7 +1283,7 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
                                       const tcad_newton_opts_t* opts, void* work,
                                       size_t work_bytes, tcad_newton_result_t* result,
                                       void* stream) {
-  if (!pk || !opts || !result || !work) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || !opts || !result || !work) return TCAD_ERR_ARG;
   Work w = carve(pk, work, work_bytes);
   if (w.bytes > work_bytes) return TCAD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
@@ -1350,7 +1387,7 @@ extern "C" int tcad_block_krylov_noalloc(const tcad_pack_t* pk, const double* J,
                                          const double* b, double* x, double rtol,
                                          int maxiter, int32_t* iters, int32_t* status,
                                          double* relres, void* stream) {
-  if (!pk || !J || !b || !x) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || !J || !b || !x) return TCAD_ERR_ARG;
   if (pk->n_nodes > TCAD_STATIC_MAX_NODES || pk->n_inst > TCAD_STATIC_MAX_INST ||
       pk->n_inst < 1)
     return TCAD_ERR_ARG;  // beyond the static scratch: use tcad_block_krylov

@@ -236,33 +236,53 @@ def instance_par(s):
     return par
 
 
-def instance_tiles(s, dim):
+def choose_tile_z(setups, dim, sm_count=148, ctas_per_sm=3, waves=2.0):
+    """Z depth of the 3D assembly tiles: the deepest of 16, 8, 4, 2 planes
+    whose tile count still fills `waves` waves of the GPU's CTA slots (a
+    deeper tile re-evaluates fewer z-edges at its first plane; a shallower
+    one keeps every SM busy on small meshes)."""
+    if dim != 3:
+        return 1
+    slots = sm_count * ctas_per_sm * waves
+    for tz in (16, 8, 4, 2):
+        n = sum(-(-s.nax[0] // _lib.TILE_X) * -(-s.nax[1] // _lib.TILE_Y) * -(-s.nax[2] // tz)
+                for s in setups)
+        if n >= slots:
+            return tz
+    return 2
+
+
+def instance_tiles(s, dim, tile_z=1):
     """Stencil tiles (i0, j0, k0) of one instance, x fastest."""
     nz = s.nax[2] if dim == 3 else 1
-    kstep = _lib.TILE_Z if dim == 3 else 1
+    kstep = tile_z if dim == 3 else 1
     k0, j0, i0 = np.meshgrid(np.arange(0, nz, kstep), np.arange(0, s.nax[1], _lib.TILE_Y),
                              np.arange(0, s.nax[0], _lib.TILE_X), indexing="ij")
     return np.stack([i0.ravel(), j0.ravel(), k0.ravel()], axis=1).astype(np.int32)
 
 
-def instance_tables(setups, dim, node_off, axis_off, tiles=None):
+def instance_tables(setups, dim, node_off, axis_off, tiles=None, tile_z=1,
+                    flat_nodes=None):
     """The per-instance tables of include/tcad_b200.h for instances placed at
-    node_off[i] (increasing) with axis entries at axis_off[i, a]."""
+    node_off[i] (increasing) with axis entries at axis_off[i, a]; 3D tiles
+    `tile_z` planes deep, flat blocks of `flat_nodes` nodes."""
     ni = len(setups)
+    flat_nodes = int(flat_nodes or _lib.FLAT_NODES)
     sizes = [s.N for s in setups]
-    nflat = [-(-n // _lib.FLAT_NODES) for n in sizes]
+    nflat = [-(-n // flat_nodes) for n in sizes]
     flat_off = np.concatenate(([0], np.cumsum(nflat))).astype(np.int64)
     flat_inst = np.repeat(np.arange(ni, dtype=np.int32), nflat)
     shape = np.ones((ni, 3), dtype=np.int32)
     for i, s in enumerate(setups):
         shape[i, :dim] = s.nax[:dim]
-    tiles = tiles if tiles is not None else [instance_tiles(s, dim) for s in setups]
+    tiles = tiles if tiles is not None else [instance_tiles(s, dim, tile_z) for s in setups]
     tl = (np.concatenate([np.concatenate([np.full((t.shape[0], 1), i, np.int32), t], axis=1)
                           for i, t in enumerate(tiles)]).ravel()
           if ni else np.zeros(0, np.int32))
     par = np.stack([instance_par(s) for s in setups]) if ni else np.zeros((0, _lib.NPAR))
     return dict(shape=shape.ravel(), node_off=np.asarray(node_off, np.int64),
-                flat_off=flat_off, flat_inst=flat_inst,
+                flat_off=flat_off, flat_inst=flat_inst, tile_z=int(tile_z),
+                flat_nodes=flat_nodes,
                 axis_off=np.asarray(axis_off, np.int64).ravel(), tile=tl.astype(np.int32),
                 par=par.ravel())
 
@@ -344,7 +364,8 @@ class Pack:
             t[name] = torch.zeros(self.N, dtype=torch.float64, device=self.device)
         t["bcflag"] = torch.zeros(self.N, dtype=torch.uint8, device=self.device)
         self.t = t
-        self._set_tables(instance_tables(self.setups, dim, node_off[:-1], axis_off))
+        self._set_tables(instance_tables(self.setups, dim, node_off[:-1], axis_off,
+                                         tile_z=choose_tile_z(self.setups, dim)))
         # state and solver buffers
         z = lambda n: torch.zeros(n, dtype=torch.float64, device=self.device)  # noqa: E731
         self.psi, self.n, self.p = z(self.N), z(self.N), z(self.N)
@@ -394,6 +415,8 @@ class Pack:
         P = _lib.TcadPack()
         P.dim = dim; P.n_inst = ni; P.n_nodes = self.N
         P.n_flat = self.n_flat; P.n_tiles = self.n_tiles
+        P.tile_z = self.tile_z = tb["tile_z"]
+        P.flat_nodes = self.flat_nodes = tb["flat_nodes"]
         for f in ("shape", "node_off", "flat_off", "flat_inst", "axis_off", "tile", "par",
                   "C", "nie", "nie_s", "tau_n", "tau_p", "bcflag") + BC_ARRAYS:
             setattr(P, f, t[f].data_ptr())

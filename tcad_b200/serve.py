@@ -35,6 +35,8 @@ from .options import NewtonOptions
 from .pack import (BC_ARRAYS, NODE_ARRAYS, Pack, axis_arrays, bc_node_arrays, gate_map,
                    instance_tables, instance_tiles, node_arrays)
 
+TILE_Z = 4          # 3D tile depth of resident devices (rounds mix device sizes)
+
 ALIGN = 32          # region starts on 32-node (256-byte) boundaries
 
 
@@ -45,7 +47,7 @@ def bytes_per_node(dim):
     path)."""
     ne = _lib.NE[dim]
     doubles = len(NODE_ARRAYS) + 3 * dim + len(BC_ARRAYS) + 3 + 3 + ne + 3
-    work64 = 6 * 3 * 8 + 4 * 8 / _lib.FLAT_NODES
+    work64 = 6 * 3 * 8 + 4 * 8 / 256
     work32 = 6 * 3 * 4 + ne * 4 + 2 * 3 * 4
     return int(np.ceil(doubles * 8 + 1 + work64 + work32))
 
@@ -140,7 +142,9 @@ class Arena:
         P.dim = dim
         P.n_inst = self.max_inst
         P.n_nodes = cap
-        P.n_flat = cap // _lib.FLAT_NODES + self.max_inst
+        P.n_flat = cap // 256 + self.max_inst    # any flat_nodes >= 256
+        P.flat_nodes = _lib.FLAT_NODES
+        P.tile_z = TILE_Z
         wb = int(self.lib.tcad_block_workspace_bytes(ctypes_ref(P), 0, 0))
         self.work = torch.empty(wb, dtype=torch.uint8, device=self.device)
         self.nodes = RangeAllocator(cap, ALIGN)
@@ -202,7 +206,7 @@ class Arena:
         h2d += guess.nbytes
         gm, gnodes = gate_map(setup)
         return Placement(off, setup.N, axis_off, [axes[a][1].size for a in range(3)],
-                         instance_tiles(setup, dim), ctab, gm, gnodes, h2d)
+                         instance_tiles(setup, dim, TILE_Z), ctab, gm, gnodes, h2d)
 
     def release(self, pl):
         with self.lock:
@@ -233,7 +237,8 @@ class RoundPack(Pack):
         dim = self.dim
         self._set_tables(instance_tables(
             self.setups, dim, [s.pl.off for s in sessions],
-            np.stack([s.pl.axis_off for s in sessions]), [s.pl.tiles for s in sessions]))
+            np.stack([s.pl.axis_off for s in sessions]), [s.pl.tiles for s in sessions],
+            tile_z=TILE_Z if dim == 3 else 1))
         self.psi, self.n, self.p = arena.psi, arena.n, arena.p
         self.F, self.J, self.du, self.work = arena.F, arena.J, arena.du, arena.work
         self.active = self.torch.ones(len(sessions), dtype=self.torch.uint8,
