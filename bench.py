@@ -53,20 +53,23 @@ TRIGATE_ITERS = {"newton_per_point": 4.0, "krylov_per_newton": 250.0}
 # iterative semantics on the GPU kernels: every Newton step's BiCGStab solved
 # to the fixed rtol 1e-10 on (dpsi, dn, dp) with node-block Jacobi.
 METHODS = {
-    "plain": dict(precision="fp64", forcing="fixed", krylov_unknowns="absolute"),
-    "fp64": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative"),
-    "mixed": dict(precision="mixed", forcing="adaptive", krylov_unknowns="relative"),
+    "plain": dict(precision="fp64", forcing="fixed", krylov_unknowns="absolute",
+                  predictor="none"),
+    "fp64": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative",
+                 predictor="secant"),
+    "mixed": dict(precision="mixed", forcing="adaptive", krylov_unknowns="relative",
+                  predictor="secant"),
 }
 METHOD_DESC = {
     "plain": "plain FP64: fused SG assembly, node-block-Jacobi BiCGStab to rtol 1e-10 on "
              "(dpsi, dn, dp) every Newton step, damped Newton",
     "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the block-scaled system in "
             "relative unknowns (dpsi, dn/n, dp/p) with forcing eta_k = clamp(0.1 "
-            "update_{k-1}, 1e-10, 1e-3)",
+            "update_{k-1}, 1e-10, 1e-3); secant predictor along the sweep",
     "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
              "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
-             "relative unknowns, adaptive forcing; per-instance FP64 fallback when an "
-             "FP32-solved step is rejected",
+             "relative unknowns, adaptive forcing, secant predictor; per-instance FP64 "
+             "fallback when an FP32-solved step is rejected",
 }
 
 

@@ -168,6 +168,17 @@ int tcad_set_contacts(const tcad_pack_t* pk, const int64_t* nodes, int64_t count
 int tcad_stamp_contacts(const tcad_pack_t* pk, const int64_t* nodes, int64_t count,
                         double* psi, double* n, double* p, void* stream);
 
+/* Secant predictor for a bias sweep (no counterpart in the reference, which
+ * warm-starts every point from the previous converged state,
+ * pytcad/device2d.py:1949-1953; the converged state does not depend on the
+ * start).  Per instance, ratio[inst] (device memory) = the new bias step over
+ * the previous one when the two are parallel: psi moves linearly, n and p
+ * geometrically (factor held to [0.1, 10]); ratio 0 leaves the state.  The
+ * state before the call is saved into *_prev (all [n_nodes]). */
+int tcad_state_extrapolate(const tcad_pack_t* pk, double* psi, double* n, double* p,
+                           double* psi_prev, double* n_prev, double* p_prev,
+                           const double* ratio, void* stream);
+
 /* ---- linear algebra on the node-block layout ---------------------------
  * Workspace size in bytes for tcad_block_krylov / tcad_newton_solve. */
 size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart);

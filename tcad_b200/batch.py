@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 from .options import NewtonOptions
-from .pack import Pack
+from .pack import Pack, bias_vector, secant_ratio
 
 
 class DeviceBatch:
@@ -31,6 +31,8 @@ class DeviceBatch:
         self.pack = Pack([d.setup for d in self.devices])
         self.n = len(self.devices)
         self.have_state = np.zeros(self.n, dtype=bool)
+        self.bias_prev = [None] * self.n     # per instance: bias of the prev / current state
+        self.bias_cur = [None] * self.n
         self.last = None
         self._guess = None   # bulk-guess potential, resident after first use
 
@@ -52,6 +54,8 @@ class DeviceBatch:
         pk.psi.copy_(self._guess)
         res = pk.equilibrium(opts)
         self.have_state[:] = True
+        self.bias_prev = [None] * self.n
+        self.bias_cur = [np.zeros(len(d.bcs)) for d in self.devices]
         self.last = res
         return res
 
@@ -65,8 +69,37 @@ class DeviceBatch:
         self._ctypes_voltages(voltages)
         pk = self.pack
         pk.set_bias()
+        act = np.ones(self.n, dtype=bool) if active is None else np.asarray(active, bool)
+        new = [bias_vector(d.setup) for d in self.devices]
+        use_pred = getattr(opts, "predictor", "none") == "secant"
+        ratios = [secant_ratio(self.bias_prev[i], self.bias_cur[i], new[i])
+                  if (use_pred and act[i]) else 0.0 for i in range(self.n)]
+        if use_pred:
+            # inactive instances: ratio 0 (their state is saved, not moved)
+            pk.predict(ratios)
         pk.stamp_contacts(active)
         res = pk.newton(opts, active=active)
+        retry = [i for i in range(self.n) if act[i] and ratios[i] != 0.0
+                 and not res[i]["converged"]]
+        if retry:
+            pk.restore_prev(retry)
+            mask = np.zeros(self.n, dtype=bool)
+            mask[retry] = True
+            pk.stamp_contacts(mask)
+            res2 = pk.newton(opts, active=mask)
+            for i in retry:
+                r = res2[i]
+                r["iters"] += res[i]["iters"]
+                r["krylov_iters"] += res[i]["krylov_iters"]
+                r["predictor_retry"] = True
+                res[i] = r
+        for i in range(self.n):
+            if not act[i]:
+                if use_pred:       # its prev buffer now holds its current state
+                    self.bias_prev[i] = None
+                continue
+            self.bias_prev[i] = self.bias_cur[i] if use_pred else None
+            self.bias_cur[i] = new[i] if res[i]["converged"] else None
         self.last = res
         return res
 

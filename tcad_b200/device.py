@@ -22,7 +22,7 @@ import scipy.sparse as sp
 
 from . import _lib
 from .options import Models, NewtonOptions
-from .pack import Contact, Gate, Pack, Setup
+from .pack import Contact, Gate, Pack, Setup, bias_vector, secant_ratio
 from .physics import SILICON
 
 
@@ -52,6 +52,7 @@ class _Device:
             setattr(self, a, getattr(s, a))
         self.bcs = s.bcs
         self._pack = None
+        self._bias_prev = self._bias_cur = None   # biases of the prev / current state
         self._have_state = False
         self._host = {}
         self.last_converged = None
@@ -87,6 +88,7 @@ class _Device:
         return self._host[name]
 
     def _set(self, name, value):
+        self._bias_prev = self._bias_cur = None
         if value is None:
             self._have_state = False
             self._host.clear()
@@ -157,6 +159,8 @@ class _Device:
         self.last_equilibrium = res
         self._have_state = True
         self._host.clear()
+        # the equilibrium state is the state at zero applied bias
+        self._bias_prev, self._bias_cur = None, np.zeros(len(self.bcs))
         if not res["converged"]:
             warnings.warn(f"{self.dim}D equilibrium Poisson solve did not converge "
                           f"(last |d| {res['err']:.2e}, linear status "
@@ -172,11 +176,33 @@ class _Device:
         self._apply_voltages(voltages)
         pk = self.pack
         pk.set_bias()
+        new = bias_vector(self.setup)
+        use_pred = getattr(opts, "predictor", "none") == "secant"
+        ratio = secant_ratio(self._bias_prev, self._bias_cur, new) if use_pred else 0.0
+        if use_pred:
+            pk.predict([ratio])
         pk.stamp_contacts()
         self.last_auto_method = "bicgstab" if opts.linsolve == "auto" else None
         self.last_auto_reason = ("GPU path: node-block-scaled BiCGStab for every coupled "
                                  "Newton system" if opts.linsolve == "auto" else None)
         res = pk.newton(opts)[0]
+        res["predictor_ratio"] = ratio
+        if ratio != 0.0 and not res["converged"]:
+            # the predicted start did not converge: solve again from the
+            # previous converged state
+            pk.restore_prev()
+            pk.stamp_contacts()
+            first = res
+            res = pk.newton(opts)[0]
+            res["iters"] += first["iters"]
+            res["krylov_iters"] += first["krylov_iters"]
+            res["predictor_ratio"] = 0.0
+            res["predictor_retry"] = True
+        if use_pred:
+            self._bias_prev = self._bias_cur
+        else:
+            self._bias_prev = None
+        self._bias_cur = new if res["converged"] else None
         self._host.clear()
         self.last_newton = res
         self.last_converged = bool(res["converged"])

@@ -97,6 +97,13 @@ class NewtonOptions:
     # through a similarity transform of the block-scaled Jacobian; "absolute"
     # for (dpsi, dn, dp).
     krylov_unknowns: str = "relative"
+    # GPU-only: start of a sweep point.  "secant" extrapolates the state
+    # along the sweep when the new bias step is parallel to the previous one
+    # (psi linearly, n and p in log space); "none" starts from the previous
+    # converged state as the reference does.  The converged state is the
+    # same discrete solution either way; a predicted start that fails to
+    # converge is retried from the previous state.
+    predictor: str = "secant"
 
     def __post_init__(self):
         if self.precond not in ("auto", "block_jacobi", "schur"):
@@ -109,5 +116,7 @@ class NewtonOptions:
         if self.linsolve not in ("auto", "direct", "gmres", "bicgstab", "gpu_direct",
                                  "petsc", "mumps"):
             raise ValueError(f"unknown linsolve {self.linsolve!r}")
+        if self.predictor not in ("none", "secant"):
+            raise ValueError(f"NewtonOptions.predictor={self.predictor!r}: 'none' or 'secant'")
         if self.precision not in ("fp64", "mixed"):
             raise ValueError(f"NewtonOptions.precision={self.precision!r}: 'fp64' or 'mixed'")

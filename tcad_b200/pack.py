@@ -336,6 +336,29 @@ def gate_values(gm):
     return gv
 
 
+def bias_vector(setup):
+    """Every contact's V and gate's Vg, in BC order: the bias of a state."""
+    return np.array([b.V if b.kind == "contact" else b.Vg for b in setup.bcs.values()],
+                    dtype=float)
+
+
+def secant_ratio(prev, cur, new, smax=2.0):
+    """Step ratio s of the secant predictor: new - cur = s (cur - prev) with
+    0 < s <= smax, else 0 (no prediction)."""
+    if prev is None or cur is None or len(prev) != len(new) or len(cur) != len(new):
+        return 0.0
+    d1, d2 = cur - prev, new - cur
+    n1 = float(d1 @ d1)
+    if not n1 > 0.0:
+        return 0.0
+    s = float(d1 @ d2) / n1
+    if not 0.0 < s <= smax:
+        return 0.0
+    if np.abs(d2 - s * d1).max() > 1e-9 * max(np.abs(d2).max(), 1e-12):
+        return 0.0
+    return s
+
+
 class Pack:
     """Device-memory image of a list of Setups of one dimension, packed back
     to back."""
@@ -376,6 +399,28 @@ class Pack:
         self.work = torch.empty(wb, dtype=torch.uint8, device=self.device)
         self.active = torch.ones(len(self.setups), dtype=torch.uint8, device=self.device)
         self.refresh_bcs()
+
+    def predict(self, ratios):
+        """Secant predictor per instance (tcad_state_extrapolate); saves the
+        current state into the prev buffers first."""
+        torch = self.torch
+        if getattr(self, "_prev", None) is None:
+            self._prev = tuple(torch.zeros_like(self.psi) for _ in range(3))
+        r = self._up(np.asarray(ratios, dtype=float))
+        rc = self.lib.tcad_state_extrapolate(
+            self.pref, _lib.ptr(self.psi), _lib.ptr(self.n), _lib.ptr(self.p),
+            *(_lib.ptr(t) for t in self._prev), _lib.ptr(r), self.sp())
+        _lib.check(rc, "tcad_state_extrapolate")
+        self._ratio_keep = r
+
+    def restore_prev(self, insts=None):
+        """State of the listed instances (all by default) back from the prev
+        buffers (the state before the last prediction)."""
+        insts = range(len(self.setups)) if insts is None else insts
+        for i in insts:
+            a, b = int(self.node_off[i]), int(self.node_off[i]) + self.setups[i].N
+            for cur, prev in zip((self.psi, self.n, self.p), self._prev):
+                cur[a:b].copy_(prev[a:b])
 
     def _init_common(self, setups, device):
         import torch
