@@ -32,8 +32,8 @@ import numpy as np
 
 from . import _lib
 from .options import NewtonOptions
-from .pack import (BC_ARRAYS, NODE_ARRAYS, Pack, axis_arrays, bc_node_arrays, gate_map,
-                   instance_tables, instance_tiles, node_arrays)
+from .pack import (BC_ARRAYS, NODE_ARRAYS, Pack, axis_arrays, bc_node_arrays, bias_vector,
+                   gate_map, instance_tables, instance_tiles, node_arrays, secant_ratio)
 
 TILE_Z = 4          # 3D tile depth of resident devices (rounds mix device sizes)
 
@@ -44,9 +44,9 @@ def bytes_per_node(dim):
     """HBM bytes one resident node costs: coefficients, BC arrays, state, F,
     the node-block Jacobian, the Newton update and the Krylov workspace
     (FP64 BiCGStab vectors and the FP32 extension of the mixed-precision
-    path)."""
+    path), and the previous state the sweep predictor extrapolates from."""
     ne = _lib.NE[dim]
-    doubles = len(NODE_ARRAYS) + 3 * dim + len(BC_ARRAYS) + 3 + 3 + ne + 3
+    doubles = len(NODE_ARRAYS) + 3 * dim + len(BC_ARRAYS) + 3 + 3 + 3 + ne + 3
     work64 = 6 * 3 * 8 + 4 * 8 / 256
     work32 = 6 * 3 * 4 + ne * 4 + 2 * 3 * 4
     return int(np.ceil(doubles * 8 + 1 + work64 + work32))
@@ -135,6 +135,7 @@ class Arena:
             t[f"dv{a}"] = torch.ones(self.axcap, **f64)
         self.t = t
         self.psi, self.n, self.p = (torch.zeros(cap, **f64) for _ in range(3))
+        self.prev = tuple(torch.zeros(cap, **f64) for _ in range(3))
         self.F = torch.zeros(3 * cap, **f64)
         self.J = torch.zeros(_lib.NE[dim] * cap, **f64)
         self.du = torch.zeros(3 * cap, **f64)
@@ -153,7 +154,7 @@ class Arena:
 
     def hbm_bytes(self):
         tot = sum(v.numel() * v.element_size() for v in self.t.values())
-        for v in (self.psi, self.n, self.p, self.F, self.J, self.du, self.work):
+        for v in (self.psi, self.n, self.p, self.F, self.J, self.du, self.work) + self.prev:
             tot += v.numel() * v.element_size()
         return tot
 
@@ -241,6 +242,7 @@ class RoundPack(Pack):
             tile_z=TILE_Z if dim == 3 else 1))
         self.psi, self.n, self.p = arena.psi, arena.n, arena.p
         self.F, self.J, self.du, self.work = arena.F, arena.J, arena.du, arena.work
+        self._prev = arena.prev
         self.active = self.torch.ones(len(sessions), dtype=self.torch.uint8,
                                       device=self.device)
         self._contact_tables([s.pl.ctab for s in sessions])
@@ -257,6 +259,7 @@ class Session:
         self.key = key
         self.setup = setup
         self.pl = None
+        self.bias_prev = self.bias_cur = None
         self.need_eq = True
         self.fresh_guess = False
         self.busy = False
@@ -433,6 +436,7 @@ class Worker(threading.Thread):
             RoundPack(self.arena, new).equilibrium(self.opts)
             for s in new:
                 s.need_eq = False
+                s.bias_prev, s.bias_cur = None, np.zeros(len(s.setup.bcs))
         sessions = [r._session for r in self.active]
         for r in self.active:
             for name, V in r.points[r.next].items():
@@ -444,8 +448,29 @@ class Worker(threading.Thread):
         rp = RoundPack(self.arena, sessions)
         rp.set_bias()
         self.h2d_bytes += rp.last_h2d_bytes
+        opts = self.opts
+        use_pred = getattr(opts, "predictor", "none") == "secant"
+        newb = [bias_vector(s.setup) for s in rp.sessions]
+        ratios = [secant_ratio(s.bias_prev, s.bias_cur, b) if use_pred else 0.0
+                  for s, b in zip(rp.sessions, newb)]
+        if use_pred:
+            rp.predict(ratios)
         rp.stamp_contacts()
-        res = rp.newton(self.opts)
+        res = rp.newton(opts)
+        retry = [i for i, r in enumerate(ratios) if r != 0.0 and not res[i]["converged"]]
+        if retry:      # predicted starts that failed: again from the previous state
+            rp.restore_prev(retry)
+            mask = np.zeros(len(rp.sessions), dtype=bool)
+            mask[retry] = True
+            rp.stamp_contacts(mask)
+            res2 = rp.newton(opts, active=mask)
+            for i in retry:
+                res2[i]["iters"] += res[i]["iters"]
+                res2[i]["krylov_iters"] += res[i]["krylov_iters"]
+                res[i] = res2[i]
+        for s, b, rr in zip(rp.sessions, newb, res):
+            s.bias_prev = s.bias_cur if use_pred else None
+            s.bias_cur = b if rr["converged"] else None
         by_session = {id(s): (i, res[i]) for i, s in enumerate(rp.sessions)}
         outs = []
         for r in self.active:
