@@ -788,47 +788,47 @@ def cpu_baseline(dev, args, newton_iters, krylov_iters):
                 "sample": f"failed: {exc!r}"}
 
 
-def run_reference(args):
-    """The oracle's CPU implementation on the host cores (rank 0 only)."""
-    if int(os.environ.get("RANK", "0")) != 0:
-        return None
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count() or 1))
-    from tcad_b200 import workloads as W
-    from tcad_b200.pack import Setup, Contact, Gate
-    import tcad_b200 as tb
+class HostDevice:
+    """Device-shaped host set-up (no GPU touched): the workload builders fill
+    its BCs, then the oracle takes it over."""
+    dim = 3
 
-    class HostOnly:
-        """Device-shaped host set-up (no GPU touched): the workload builders
-        fill its BCs, then the oracle takes it over."""
-        dim = 3
+    def __init__(self, mesh, doping, Ntotal=None, models=None, **kw):
+        import tcad_b200 as tb
+        from tcad_b200.pack import Setup
+        coords = (mesh.x, mesh.y) if not hasattr(mesh, "z") else (mesh.x, mesh.y, mesh.z)
+        self.dim = len(coords)
+        self.setup = Setup(coords, doping, Ntotal=Ntotal, models=models or tb.Models(), **kw)
+        self.bcs = self.setup.bcs
 
-        def __init__(self, mesh, doping, Ntotal=None, models=None, **kw):
-            coords = (mesh.x, mesh.y) if not hasattr(mesh, "z") else (mesh.x, mesh.y, mesh.z)
-            self.dim = len(coords)
-            self.setup = Setup(coords, doping, Ntotal=Ntotal, models=models or tb.Models(),
-                               **kw)
-            self.bcs = self.setup.bcs
+    def add_contact(self, name, *ijk, V=0.0):
+        from tcad_b200.pack import Contact
+        self.bcs[name] = Contact(self.setup.flat(*ijk), V)
 
-        def add_contact(self, name, *ijk, V=0.0):
-            self.bcs[name] = Contact(self.setup.flat(*ijk), V)
+    def add_gate(self, name, *ijk, tox_cm, Vfb, Vg=0.0, normal_axis="z"):
+        from tcad_b200.pack import Gate
+        idx = [np.atleast_1d(np.asarray(a, dtype=np.int64)) for a in ijk]
+        self.bcs[name] = Gate(self.setup.flat(*ijk), self.setup.gate_kappa(tox_cm), Vfb,
+                              Vg, self.setup.gate_weight(idx, normal_axis), normal_axis)
 
-        def add_gate(self, name, *ijk, tox_cm, Vfb, Vg=0.0, normal_axis="z"):
-            idx = [np.atleast_1d(np.asarray(a, dtype=np.int64)) for a in ijk]
-            self.bcs[name] = Gate(self.setup.flat(*ijk), self.setup.gate_kappa(tox_cm), Vfb,
-                                  Vg, self.setup.gate_weight(idx, normal_axis), normal_axis)
 
-    dev, sched, desc, contact = build_workload(args.workload, args.small, HostOnly, HostOnly)
+def reference_worker(workload, small, steps, warmup, wid):
+    """One host process of the reference arm: its own oracle device, timed
+    over warmup + steps bounded samples; returns (seconds per bias point of
+    each timed step, sample description, workload description)."""
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    dev, sched, desc, contact = build_workload(workload, small, HostDevice, HostDevice)
     ora = oracle_from(dev)
-    ora.solve_equilibrium() if args.workload == "diode2d" else None
-    if args.workload == "diode2d":
+    lat = []
+    if workload == "diode2d":
         # full solves: every step is one real warm-started bias point
-        lat = []
+        ora.solve_equilibrium()
         pts = [v for v, _ in sched]
-        for q in range(args.warmup + args.steps):
+        for q in range(warmup + steps):
             t0 = time.perf_counter()
-            ora.solve_bias(pts[q % len(pts)])
+            ora.solve_bias(pts[(q + wid) % len(pts)])
             ora.terminal_current(contact)
-            if q >= args.warmup:
+            if q >= warmup:
                 lat.append(time.perf_counter() - t0)
         sample = "full oracle bias points (scipy SuperLU), warm-started sweep"
     else:
@@ -837,28 +837,62 @@ def run_reference(args):
         psi = ora.bulk_guess()
         n = ora.nie_s * np.exp(psi)
         p = ora.nie_s * np.exp(-psi)
-        lat = []
-        for q in range(args.warmup + args.steps):
+        for q in range(warmup + steps):
             t_asm, t_bj, t_it = cpu_costs(ora, psi, n, p, krylov_iters=5)
             sec = (TRIGATE_ITERS["newton_per_point"] * (t_asm + t_bj)
                    + TRIGATE_ITERS["newton_per_point"] * TRIGATE_ITERS["krylov_per_newton"]
                    * t_it)
-            if q >= args.warmup:
+            if q >= warmup:
                 lat.append(sec)
-        sample = ("per step: one full-mesh oracle assembly + elimination + "
+        sample = ("per step and process: one full-mesh oracle assembly + elimination + "
                   "node-block-Jacobi set-up + 5 scipy BiCGStab iterations, scaled to a "
                   f"bias point with {TRIGATE_ITERS['newton_per_point']} Newton x "
                   f"{TRIGATE_ITERS['krylov_per_newton']} BiCGStab iterations")
-    sec = float(np.mean(lat))
-    value = 1.0 / sec
-    cores = int(os.environ.get("OPENBLAS_NUM_THREADS", "1"))
+    return lat, sample, desc
+
+
+def reference_processes(workload, small):
+    """Host processes for the reference arm: every core, bounded by memory
+    (about 3 GB per full-size 3D oracle, 0.5 GB per 2D one)."""
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 16e9
+    per = 0.5e9 if (workload == "diode2d" or small) else 3.0e9
+    return max(1, min(cores, int(0.7 * avail // per)))
+
+
+def run_reference(args):
+    """The oracle's CPU implementation on the host cores (rank 0 only): one
+    process per core, each an independent stream of bias points (the
+    reference's own parallel pattern for independent points); the rate is
+    the sum over processes."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return None
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    nproc = reference_processes(args.workload, args.small)
+    with cf.ProcessPoolExecutor(nproc, mp_context=mp.get_context("spawn")) as ex:
+        futs = [ex.submit(reference_worker, args.workload, args.small, args.steps,
+                          args.warmup, w) for w in range(nproc)]
+        outs = [f.result() for f in futs]
+    lats = [np.asarray(o[0]) for o in outs]
+    sample, desc = outs[0][1], outs[0][2]
+    # aggregate rate of each timed step: sum over processes of 1 / seconds
+    rates = np.sum([1.0 / l for l in lats], axis=0)
+    value = float(np.mean(rates))
+    sec = 1.0 / value
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic device",
             "config": {"workload": desc, "method": "oracle CPU port (numpy/scipy)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
+                             "sample": sample + f"; {nproc} processes x 1 thread",
+                             "per_process_sec_per_point": float(np.mean(
+                                 [l.mean() for l in lats]))},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
