@@ -80,7 +80,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="trigate3d",
-                    choices=["trigate3d", "diode2d", "mosfet2d_batch", "serve"])
+                    choices=["trigate3d", "diode2d", "pin3d", "mosfet2d_batch", "serve"])
     ap.add_argument("--duration", type=float, default=60.0,
                     help="serve: seconds of Poisson arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: mean requests/s")
@@ -187,6 +187,14 @@ class Clocks:
 # ---------------------------------------------------------------------------
 def build_workload(name, small, dev_cls_2d, dev_cls_3d):
     from tcad_b200 import workloads as W
+    if name == "pin3d":
+        dims = (64, 32, 16) if small else (256, 256, 128)
+        dev = W.pin3d(dev_cls_3d, *dims)
+        sched = [({"anode": v}, i == 0) for i, v in enumerate(W.PIN_SWEEP)]
+        desc = (f"pin3d {dims[0]}x{dims[1]}x{dims[2]} ({int(np.prod(dims)):,} nodes) p+ 1e19 / "
+                "i 1e14 / n+ 1e19, 20 nm erfc transitions, SRH + Auger, forward 0..0.9 V "
+                "step 0.1")
+        return dev, sched, desc, "anode"
     if name == "diode2d":
         nx, ny = (41, 11) if small else (201, 101)
         dev = W.diode2d(dev_cls_2d, nx, ny)

@@ -161,6 +161,35 @@ def mosfet_batch_params(count=512, seed=2026, nx=(80, 400), ny=(40, 200), Lg=(30
     return out
 
 
+def pin3d(dev_cls, nx=256, ny=256, nz=128, L=1.0e-4, W=0.5e-4, H=0.25e-4, x1=0.3e-4,
+          x2=0.7e-4, NA=1e19, ND=1e19, Ni=1e14, lam=20e-7, ratio=1.03, models=None):
+    """3D p-i-n diode on an exact nx x ny x nz tensor mesh: p+ (NA) for
+    x < x1, intrinsic background Ni (n-type) between, n+ (ND) for x > x2,
+    each transition an erfc of length lam; x graded toward the two
+    junctions, y and z uniform; ohmic anode on the x = 0 face and cathode on
+    the x = L face.  SRH + Auger with doping mobility (BGN off)."""
+    x = graded_nodes(nx, L, [x1, x2], ratio)
+    y = np.linspace(0.0, W, ny)
+    z = np.linspace(0.0, H, nz)
+    pa = 0.5 * NA * erfc((x - x1) / lam)
+    nd = 0.5 * ND * erfc((x2 - x) / lam)
+    net1 = nd + Ni - pa
+    tot1 = nd + Ni + pa
+    shape = (nz, ny, nx)
+    dop = np.broadcast_to(net1[None, None, :], shape).copy()
+    ntot = np.broadcast_to(tot1[None, None, :], shape).copy()
+    m = models or Models(doping_mobility=True, srh=True, auger=True, bgn=False)
+    dev = dev_cls(Mesh3D(x, y, z), dop, Ntotal=ntot, models=m)
+    J, K = np.meshgrid(np.arange(ny), np.arange(nz), indexing="xy")
+    J, K = J.ravel(), K.ravel()
+    dev.add_contact("anode", np.zeros_like(J), J, K)
+    dev.add_contact("cathode", np.full_like(J, nx - 1), J, K)
+    return dev
+
+
+PIN_SWEEP = [round(0.1 * k, 10) for k in range(10)]
+
+
 def ramp(target, steps):
     """The explicit bias ramp both sides use: equal steps from 0 to the
     target, `steps` of them (the reference has no ramp of its own; every

@@ -135,3 +135,21 @@ def current_err(I, g, floor_frac=1e-9):
     scale = np.maximum(np.abs(ref), floor_frac * np.abs(ref).max())
     scale = np.where(scale == 0, 1.0, scale)
     return float((np.minimum(np.abs(I - ref), np.abs(I - alt)) / scale).max())
+
+
+def oracle_from_device(dev):
+    """The oracle device with the same set-up, contacts and gates as a
+    tcad_b200 device (built by a workload builder)."""
+    from oracle import OracleDevice, OracleModels
+    s = dev.setup
+    m = s.models
+    mat = {k: getattr(s.mat, k) for k in s.mat.__dataclass_fields__ if k != "name"}
+    ora = OracleDevice(s.coords, s.doping, Ntotal=s.Ntot, T=s.T,
+                       models=OracleModels(m.doping_mobility, m.srh, m.auger, m.bgn),
+                       material=mat)
+    for name, b in dev.bcs.items():
+        if b.kind == "contact":
+            ora.contacts[name] = [b.nodes.copy(), b.V]
+        else:
+            ora.gates[name] = [b.nodes.copy(), b.kappa, b.Vfb, b.Vg, b.w.copy()]
+    return ora
