@@ -9,6 +9,9 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtcad_b200.so")
+# A different build of the same library (same ABI) can be selected with
+# TCAD_B200_LIB, e.g. to compare compile options of the kernels.
+LIB_PATH = os.environ.get("TCAD_B200_LIB", LIB_PATH)
 
 TCAD_OK = 0
 TCAD_ERR_ARG = 1

@@ -250,8 +250,9 @@ k_bi_init(const tcad_pack_t pk, const T* __restrict__ b, T* __restrict__ x, BiVe
 // p = r + beta (p - omega v)   (restart: rh = r, p = r)
 template <class T>
 __global__ void __launch_bounds__(NT)
-k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
   const KState s = ks[fb.inst];
   if (!s.active) return;
   const int64_t NN = pk.n_nodes;
@@ -275,8 +276,9 @@ k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks) {
 template <int DIM, class T>
 __global__ void __launch_bounds__(NT)
 k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
-       double* partial, unsigned* ticket) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+       double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
   if (!ks[fb.inst].active) return;
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
@@ -290,7 +292,7 @@ k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
     v[0] += (double)w.rh[k] * y0 + (double)w.rh[NN + k] * y1 + (double)w.rh[2 * NN + k] * y2;
   }
   double tot[1];
-  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+  if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     KState& s = ks[fb.inst];
     s.restart = 0;
     s.rv = tot[0];
@@ -306,8 +308,10 @@ k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
 // s = r - alpha v, (s, s)
 template <class T>
 __global__ void __launch_bounds__(NT)
-k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned* ticket) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned* ticket,
+       const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
   const KState s0 = ks[fb.inst];
   if (!s0.active) return;
   const int64_t NN = pk.n_nodes;
@@ -323,7 +327,7 @@ k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned*
     }
   }
   double tot[1];
-  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+  if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     KState& s = ks[fb.inst];
     s.ss = tot[0];
     s.early = tot[0] <= s.tol2 ? 1 : 0;
@@ -334,8 +338,9 @@ k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned*
 template <int DIM, class T>
 __global__ void __launch_bounds__(NT)
 k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
-       double* partial, unsigned* ticket) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+       double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
   if (!ks[fb.inst].active) return;
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
@@ -350,7 +355,7 @@ k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
     v[1] += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
   }
   double tot[2];
-  if (Reduce<2>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+  if (Reduce<2>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     KState& s = ks[fb.inst];
     s.omega = (s.early || !(tot[1] > 0.0)) ? 0.0 : tot[0] / tot[1];
   }
@@ -360,8 +365,9 @@ k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
 template <class T>
 __global__ void __launch_bounds__(NT)
 k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double* partial,
-       unsigned* ticket) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+       unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
   const KState s0 = ks[fb.inst];
   if (!s0.active) return;
   const int64_t NN = pk.n_nodes;
@@ -381,7 +387,7 @@ k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double*
     }
   }
   double tot[3];
-  if (Reduce<3>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+  if (Reduce<3>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     KState& s = ks[fb.inst];
     s.it += 1;
     s.rr = tot[1];
@@ -746,6 +752,7 @@ struct Work {
   int32_t* status;
   unsigned long long* err;
   double* eta;
+  int32_t* blk;  // compact list of the flat blocks still iterating
   size_t bytes;
 };
 
@@ -802,6 +809,7 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   w.status = c.take<int32_t>(pk->n_inst);
   w.err = c.take<unsigned long long>(pk->n_inst);
   w.eta = c.take<double>(pk->n_inst);
+  w.blk = c.take<int32_t>(pk->n_flat);
   w.bytes = c.used;
   return w;
 }
@@ -822,23 +830,39 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
   int check = 4;
   int done_iters = 0;
   int rechecks = 0;
+  // Launch grid: every flat block, or -- once the instances still iterating
+  // cover under 3/4 of them -- only those instances' blocks (a compact list
+  // rebuilt whenever the active set changes), so a batch's stragglers do
+  // not pay for launches over finished instances.
+  unsigned ng = nb;
+  const int32_t* dlist = nullptr;
+  std::vector<int64_t> hfoff;
+  std::vector<int32_t> hlist;
+  std::vector<uint8_t> was_active;
+  if (ni > 1) {
+    hfoff.resize(ni + 1);
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(hfoff.data(), pk->flat_off, sizeof(int64_t) * (ni + 1),
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    was_active.assign(ni, 1);
+  }
   for (;;) {
     for (int q = 0; q < check; ++q) {
-      k_bi_p<<<nb, NT, 0, s>>>(*pk, bi, w.ks);
+      k_bi_p<<<ng, NT, 0, s>>>(*pk, bi, w.ks, dlist);
       note_launch();
       if (pk->dim == 2)
-        k_bi_v<2><<<nb, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket);
+        k_bi_v<2><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
       else
-        k_bi_v<3><<<nb, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket);
+        k_bi_v<3><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
       note_launch();
-      k_bi_s<<<nb, NT, 0, s>>>(*pk, bi, w.ks, w.partial, w.ticket);
+      k_bi_s<<<ng, NT, 0, s>>>(*pk, bi, w.ks, w.partial, w.ticket, dlist);
       note_launch();
       if (pk->dim == 2)
-        k_bi_t<2><<<nb, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket);
+        k_bi_t<2><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
       else
-        k_bi_t<3><<<nb, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket);
+        k_bi_t<3><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
       note_launch();
-      k_bi_x<<<nb, NT, 0, s>>>(*pk, x, bi, w.ks, w.partial, w.ticket);
+      k_bi_x<<<ng, NT, 0, s>>>(*pk, x, bi, w.ks, w.partial, w.ticket, dlist);
       note_launch();
     }
     TCAD_LAUNCH_CHECK();
@@ -848,6 +872,30 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
     TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
     bool any = false;
     for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+    if (any && ni > 1) {
+      bool changed = false;
+      int64_t act_blocks = 0;
+      for (int i = 0; i < ni; ++i) {
+        changed = changed || (was_active[i] != (hks[i].active ? 1 : 0));
+        if (hks[i].active) act_blocks += hfoff[i + 1] - hfoff[i];
+      }
+      if (changed) {
+        for (int i = 0; i < ni; ++i) was_active[i] = hks[i].active ? 1 : 0;
+        if (4 * act_blocks < 3 * (int64_t)nb) {
+          hlist.clear();
+          for (int i = 0; i < ni; ++i)
+            if (hks[i].active)
+              for (int64_t b = hfoff[i]; b < hfoff[i + 1]; ++b) hlist.push_back((int32_t)b);
+          TCAD_CUDA_CHECK(cudaMemcpyAsync(w.blk, hlist.data(), sizeof(int32_t) * hlist.size(),
+                                          cudaMemcpyHostToDevice, s));
+          ng = (unsigned)hlist.size();
+          dlist = w.blk;
+        } else {
+          ng = nb;
+          dlist = nullptr;
+        }
+      }
+    }
     if (!any) {
       // true-residual check; instances whose recursive residual drifted are
       // re-armed from the true residual (bounded number of re-checks)
@@ -1408,17 +1456,17 @@ extern "C" int tcad_block_krylov_noalloc(const tcad_pack_t* pk, const double* J,
   int check = 4, done_iters = 0, rechecks = 0;
   for (;;) {
     for (int q = 0; q < check; ++q) {
-      k_bi_p<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks);
+      k_bi_p<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks, nullptr);
       if (pk->dim == 2)
-        k_bi_v<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+        k_bi_v<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket, nullptr);
       else
-        k_bi_v<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
-      k_bi_s<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks, w.partial, w.ticket);
+        k_bi_v<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket, nullptr);
+      k_bi_s<<<nb, NT, 0, s>>>(*pk, w.bi, w.ks, w.partial, w.ticket, nullptr);
       if (pk->dim == 2)
-        k_bi_t<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
+        k_bi_t<2><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket, nullptr);
       else
-        k_bi_t<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket);
-      k_bi_x<<<nb, NT, 0, s>>>(*pk, x, w.bi, w.ks, w.partial, w.ticket);
+        k_bi_t<3><<<nb, NT, 0, s>>>(*pk, J, w.bi, w.ks, w.partial, w.ticket, nullptr);
+      k_bi_x<<<nb, NT, 0, s>>>(*pk, x, w.bi, w.ks, w.partial, w.ticket, nullptr);
       note_launch(5);
     }
     TCAD_LAUNCH_CHECK();
