@@ -27,14 +27,15 @@ template <int DIM>
 __global__ void __launch_bounds__(kTileThreads, 3)
 k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
               const double* __restrict__ nn, const double* __restrict__ pp,
-              double* __restrict__ F, double* __restrict__ J, int mode) {
+              double* __restrict__ F, double* __restrict__ J, int mode,
+              const int32_t* __restrict__ tiles) {
   constexpr int NE = DIM == 2 ? TCAD_NE2 : TCAD_NE3;
   __shared__ double s_psi[TY + 2][TX + 2], s_n[TY + 2][TX + 2], s_p[TY + 2][TX + 2];
   __shared__ uint8_t s_flag[TY + 2][TX + 2];
   __shared__ Edge s_ex[TY][TX + 1];  // x-edge slot a: nodes (i0-1+a, i0+a)
   __shared__ Edge s_ey[TY + 1][TX];  // y-edge slot b: nodes (j0-1+b, j0+b)
 
-  const int64_t t = blockIdx.x;
+  const int64_t t = tiles ? (int64_t)tiles[blockIdx.x] : (int64_t)blockIdx.x;
   const int inst = pk.tile[4 * t + 0], i0 = pk.tile[4 * t + 1];
   const int j0 = pk.tile[4 * t + 2], k0 = pk.tile[4 * t + 3];
   const Inst g = load_inst(pk, inst);
@@ -466,6 +467,21 @@ k_poisson_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
   }
 }
 
+int sg_assemble_tiles(const tcad_pack_t* pk, const double* psi, const double* n,
+                      const double* p, double* F, double* J, int mode, const int32_t* tiles,
+                      int64_t n_list, cudaStream_t s) {
+  if (!pack_ok(pk) || pk->n_tiles <= 0) return TCAD_ERR_ARG;
+  const unsigned nt = (unsigned)(tiles ? n_list : pk->n_tiles);
+  if (nt == 0) return TCAD_OK;
+  if (pk->dim == 2)
+    k_sg_assemble<2><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode, tiles);
+  else
+    k_sg_assemble<3><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode, tiles);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
 }  // namespace tcad
 
 using namespace tcad;
@@ -473,16 +489,7 @@ using namespace tcad;
 extern "C" int tcad_sg_assemble(const tcad_pack_t* pk, const double* psi, const double* n,
                                 const double* p, double* F, double* J, int mode,
                                 void* stream) {
-  if (!pack_ok(pk) || pk->n_tiles <= 0) return TCAD_ERR_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
-  const unsigned nt = (unsigned)pk->n_tiles;
-  if (pk->dim == 2)
-    k_sg_assemble<2><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode);
-  else
-    k_sg_assemble<3><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode);
-  note_launch();
-  TCAD_LAUNCH_CHECK();
-  return TCAD_OK;
+  return sg_assemble_tiles(pk, psi, n, p, F, J, mode, nullptr, 0, (cudaStream_t)stream);
 }
 
 extern "C" int tcad_contact_current(const tcad_pack_t* pk, const double* psi,

@@ -102,4 +102,10 @@ __device__ __forceinline__ FlatBlock flat_block(const tcad_pack_t& pk, int64_t b
   return fb;
 }
 
+// Coupled assembly over a list of tiles (nullptr: all n_tiles); the Newton
+// driver uses it to assemble only the instances still iterating.
+int sg_assemble_tiles(const tcad_pack_t* pk, const double* psi, const double* n,
+                      const double* p, double* F, double* J, int mode, const int32_t* tiles,
+                      int64_t n_list, cudaStream_t s);
+
 }  // namespace tcad

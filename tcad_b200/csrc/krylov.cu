@@ -96,8 +96,8 @@ template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_bj_setup(const tcad_pack_t pk, double* __restrict__ J, double* __restrict__ F,
            int32_t* __restrict__ status, const double* __restrict__ nn,
-           const double* __restrict__ pp, double floor_) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+           const double* __restrict__ pp, double floor_, const int32_t* __restrict__ blk) {
+  const FlatBlock fb = flat_block(pk, blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x);
   const int64_t NN = pk.n_nodes;
   const bool rel = nn != nullptr;
   int64_t off[6];
@@ -641,8 +641,9 @@ k_slaved(const tcad_pack_t pk, const double* __restrict__ psi, double* __restric
 // mixed precision: FP32 copy of the block-scaled operator, FP64 iterative
 // refinement around FP32 BiCGStab (the residual always uses the FP64 A^)
 __global__ void __launch_bounds__(NT)
-k_to_f32(const tcad_pack_t pk, int ne, const double* __restrict__ J, float* __restrict__ J32) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+k_to_f32(const tcad_pack_t pk, int ne, const double* __restrict__ J, float* __restrict__ J32,
+         const int32_t* __restrict__ blk) {
+  const FlatBlock fb = flat_block(pk, blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x);
   const int64_t NN = pk.n_nodes;
   for (int e = 0; e < ne; ++e)
     for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT)
@@ -752,7 +753,9 @@ struct Work {
   int32_t* status;
   unsigned long long* err;
   double* eta;
-  int32_t* blk;  // compact list of the flat blocks still iterating
+  int32_t* blk;  // compact list of the flat blocks still iterating (Krylov)
+  int32_t* fl;   // flat blocks / tiles of the instances a Newton step still
+  int32_t* tl;   //   solves (assembly and block-Jacobi set-up)
   size_t bytes;
 };
 
@@ -810,6 +813,8 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   w.err = c.take<unsigned long long>(pk->n_inst);
   w.eta = c.take<double>(pk->n_inst);
   w.blk = c.take<int32_t>(pk->n_flat);
+  w.fl = c.take<int32_t>(pk->n_flat);
+  w.tl = c.take<int32_t>(pk->n_tiles);
   w.bytes = c.used;
   return w;
 }
@@ -936,11 +941,12 @@ static int solve_mixed(const tcad_pack_t* pk, const double* J, const double* b, 
                        const double* eta, int inner_maxiter, int max_ir, const Work& w,
                        const Work32& w32, const int32_t* pre_status_host,
                        std::vector<KState>& hks, int32_t* res_iters, int32_t* res_status,
-                       double* res_relres, cudaStream_t s) {
+                       double* res_relres, cudaStream_t s, const int32_t* fl = nullptr,
+                       unsigned nfl = 0) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   const int ne = pk->dim == 2 ? TCAD_NE2 : TCAD_NE3;
-  k_to_f32<<<nb, NT, 0, s>>>(*pk, ne, J, w32.J32);
+  k_to_f32<<<fl ? nfl : nb, NT, 0, s>>>(*pk, ne, J, w32.J32, fl);
   note_launch();
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
   k_ir_init<<<nb, NT, 0, s>>>(*pk, b, x, w32.irs, w.partial, w.ticket);
@@ -1058,10 +1064,12 @@ extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double*
   if (!pack_ok(pk) || !J || !F || !status) return TCAD_ERR_ARG;
   if (pk->dim == 2)
     k_bj_setup<2><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status,
-                                                                         nullptr, nullptr, 0.0);
+                                                                         nullptr, nullptr, 0.0,
+                                                                         nullptr);
   else
     k_bj_setup<3><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status,
-                                                                         nullptr, nullptr, 0.0);
+                                                                         nullptr, nullptr, 0.0,
+                                                                         nullptr);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1074,10 +1082,10 @@ extern "C" int tcad_block_jacobi_setup_rel(const tcad_pack_t* pk, double* J, dou
     return TCAD_ERR_ARG;
   if (pk->dim == 2)
     k_bj_setup<2><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status, n,
-                                                                         p, dens_floor);
+                                                                         p, dens_floor, nullptr);
   else
     k_bj_setup<3><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status, n,
-                                                                         p, dens_floor);
+                                                                         p, dens_floor, nullptr);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1166,18 +1174,65 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   std::vector<uint8_t> use64(ni, 0);  // precision 32: instances switched to FP64
   std::vector<int32_t> last_kit(ni, 0);
   std::vector<double> heta(ni, opts->forcing ? std::max(opts->eta_max, opts->rtol) : opts->rtol);
+  // Per-step launch lists: once the instances still iterating cover under
+  // 3/4 of the pack, the assembly and the block-Jacobi set-up cover only
+  // their tiles / flat blocks (rebuilt when that set changes).
+  std::vector<int64_t> hfoff;
+  std::vector<int32_t> htile_inst, lt, lf;
+  std::vector<uint8_t> listed;
+  const int32_t* tl = nullptr;
+  const int32_t* fl = nullptr;
+  int64_t ntl = 0, nfl = 0;
+  if (ni > 1) {
+    hfoff.resize(ni + 1);
+    std::vector<int32_t> htile(4 * (size_t)pk->n_tiles);
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(hfoff.data(), pk->flat_off, sizeof(int64_t) * (ni + 1),
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(htile.data(), pk->tile, sizeof(int32_t) * htile.size(),
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    htile_inst.resize(pk->n_tiles);
+    for (int64_t t = 0; t < pk->n_tiles; ++t) htile_inst[t] = htile[4 * t];
+    listed.assign(ni, 2);  // forces a first decision
+  }
   for (int it = 0; it < opts->max_iter; ++it) {
-    int rc = tcad_sg_assemble(pk, psi, n, p, F, J, TCAD_MODE_ELIMINATE, stream);
+    if (ni > 1 && listed != hact) {
+      listed = hact;
+      int64_t act_blocks = 0;
+      for (int i = 0; i < ni; ++i)
+        if (hact[i]) act_blocks += hfoff[i + 1] - hfoff[i];
+      if (4 * act_blocks < 3 * (int64_t)nb) {
+        lt.clear();
+        lf.clear();
+        for (int64_t t = 0; t < pk->n_tiles; ++t)
+          if (hact[htile_inst[t]]) lt.push_back((int32_t)t);
+        for (int i = 0; i < ni; ++i)
+          if (hact[i])
+            for (int64_t b = hfoff[i]; b < hfoff[i + 1]; ++b) lf.push_back((int32_t)b);
+        if (!lt.empty())
+          TCAD_CUDA_CHECK(cudaMemcpyAsync(w.tl, lt.data(), sizeof(int32_t) * lt.size(),
+                                          cudaMemcpyHostToDevice, s));
+        if (!lf.empty())
+          TCAD_CUDA_CHECK(cudaMemcpyAsync(w.fl, lf.data(), sizeof(int32_t) * lf.size(),
+                                          cudaMemcpyHostToDevice, s));
+        tl = w.tl; ntl = (int64_t)lt.size();
+        fl = w.fl; nfl = (int64_t)lf.size();
+      } else {
+        tl = nullptr; fl = nullptr; ntl = 0; nfl = 0;
+      }
+    }
+    int rc = sg_assemble_tiles(pk, psi, n, p, F, J, TCAD_MODE_ELIMINATE, tl, ntl, s);
     if (rc != TCAD_OK) return rc;
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int32_t) * ni, s));
-    {
+    if (!fl || nfl > 0) {
       const bool rel = opts->density_scaling != 0;
       const double* sn_ = rel ? n : nullptr;
       const double* sp_ = rel ? p : nullptr;
+      const unsigned g = fl ? (unsigned)nfl : nb;
       if (pk->dim == 2)
-        k_bj_setup<2><<<nb, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, opts->dens_floor);
+        k_bj_setup<2><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, opts->dens_floor, fl);
       else
-        k_bj_setup<3><<<nb, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, opts->dens_floor);
+        k_bj_setup<3><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, opts->dens_floor, fl);
     }
     note_launch();
     TCAD_LAUNCH_CHECK();
@@ -1207,7 +1262,8 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       std::vector<int32_t> st32(ni);
       for (int i = 0; i < ni; ++i) st32[i] = grp32[i] ? TCAD_OK : -1;
       rc = solve_mixed(pk, J, F, du, heta.data(), opts->krylov_maxiter, 30, w, w32,
-                       st32.data(), hks, mix_it.data(), mix_st.data(), mix_rr.data(), s);
+                       st32.data(), hks, mix_it.data(), mix_st.data(), mix_rr.data(), s, fl,
+                       (unsigned)nfl);
       if (rc != TCAD_OK) return rc;
       // Acceptance test before the step is applied (a dry-run update): an
       // FP32-solved step is rejected when its refinement failed (breakdown,
