@@ -538,6 +538,9 @@ def run_batch(args):
         "converged_points": n_conv, "points_per_step": batch.n,
         "newton_iters_mean_per_instance": float(iters.mean()),
         "krylov_iters_mean_per_instance": float(kits.mean()),
+        "newton_iters_max_per_instance": float(iters.max()),
+        "krylov_iters_max_per_instance": float(kits.max()),
+        "step_ms": [float(x) for x in lat],
         "plain_fp64_gpu": {"value": plain_rate, "unit": UNIT,
                            "sample_instances": [int(j) for j in sample],
                            "p50_ms_per_instance": statistics.median(plain_lat),

@@ -49,7 +49,7 @@ extern "C" {
 
 #define TCAD_NE2 29
 #define TCAD_NE3 39
-#define TCAD_FLAT_NODES 1024 /* default nodes per flat (vector-kernel) block */
+#define TCAD_FLAT_NODES 256  /* default nodes per flat (vector-kernel) block */
 #define TCAD_TILE_X 32       /* stencil tile: 32 x 8 nodes (x, y) */
 #define TCAD_TILE_Y 8
 #define TCAD_TILE_Z 16       /* largest z depth of a 3D stencil tile (tile_z <= this) */
@@ -274,13 +274,16 @@ typedef struct tcad_newton_opts {
   int32_t verbose;
   int32_t polish;        /* extra Newton steps after the update test passes */
   double eta_max;        /* forcing: loosest Krylov tolerance of an early step */
-  int32_t forcing;       /* 0: every step at rtol; 1: eta_k = clamp(0.1 err_{k-1}, rtol, eta_max) */
+  int32_t forcing;       /* 0: every step at rtol; 1: eta_k = clamp(0.1 err_{k-1}, eta_min,
+                            eta_max) */
   int32_t precision;     /* 64: FP64 Krylov; 32: FP32 Krylov on an FP32 copy of the scaled
                             operator inside FP64 iterative refinement (residual, Newton,
                             convergence test stay FP64) */
   int32_t density_scaling; /* 1: Krylov unknowns are (dpsi, dn/s_n, dp/s_p), s = max(n|p,
-                              dens_floor) -- the quantities of the Newton update test */
+                              scale_floor) -- the quantities of the Newton update test */
   int32_t pad;
+  double eta_min;        /* forcing 1: tightest Krylov tolerance of a step (>= rtol) */
+  double scale_floor;    /* density_scaling: floor of s (dens_floor when <= 0) */
 } tcad_newton_opts_t;
 
 /* Per-instance result of a Newton solve (host memory). */

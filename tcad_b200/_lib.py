@@ -25,7 +25,7 @@ STATUS_NAMES = {0: "ok", 1: "bad argument", 2: "singular node block",
                 6: "Krylov breakdown", -1: "idle"}
 
 NE = {2: 29, 3: 39}
-FLAT_NODES = 1024
+FLAT_NODES = 256
 TILE_X, TILE_Y, TILE_Z_MAX = 32, 8, 16
 NPAR = 8
 MODE_RAW, MODE_ELIMINATE = 0, 1
@@ -60,7 +60,8 @@ class NewtonOpts(ctypes.Structure):
                 ("verbose", ctypes.c_int32), ("polish", ctypes.c_int32),
                 ("eta_max", ctypes.c_double), ("forcing", ctypes.c_int32),
                 ("precision", ctypes.c_int32),
-                ("density_scaling", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("density_scaling", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("eta_min", ctypes.c_double), ("scale_floor", ctypes.c_double)]
 
 
 class NewtonResult(ctypes.Structure):

@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(NT)
 k_newton_update(const tcad_pack_t pk, double* __restrict__ psi, double* __restrict__ nn,
                 double* __restrict__ pp, const double* __restrict__ du, double max_dpsi,
                 double floor_, const uint8_t* __restrict__ active,
-                unsigned long long* __restrict__ err, int relative, int dry) {
+                unsigned long long* __restrict__ err, int relative, int dry, double sfloor) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   if (active && !active[fb.inst]) return;
   __shared__ double sm[32];
@@ -462,8 +462,8 @@ k_newton_update(const tcad_pack_t pk, double* __restrict__ psi, double* __restri
     const double n0 = nn[k], p0 = pp[k];
     const double u0 = du[k];
     // relative-update unknowns come back scaled by max(density, floor)
-    const double u1 = relative ? du[NN + k] * fmax(n0, floor_) : du[NN + k];
-    const double u2 = relative ? du[2 * NN + k] * fmax(p0, floor_) : du[2 * NN + k];
+    const double u1 = relative ? du[NN + k] * fmax(n0, sfloor) : du[NN + k];
+    const double u2 = relative ? du[2 * NN + k] * fmax(p0, sfloor) : du[2 * NN + k];
     const bool finite = isfinite(u0) && isfinite(u1) && isfinite(u2);
     double dpsi = u0 < -max_dpsi ? -max_dpsi : (u0 > max_dpsi ? max_dpsi : u0);
     double n1 = n0 + u1, p1 = p0 + u2;
@@ -1135,7 +1135,7 @@ extern "C" int tcad_newton_update(const tcad_pack_t* pk, double* psi, double* n,
   TCAD_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(double) * pk->n_inst, s));
   k_newton_update<<<(unsigned)pk->n_flat, NT, 0, s>>>(
       *pk, psi, n, p, du, max_dpsi, dens_floor, active,
-      reinterpret_cast<unsigned long long*>(err), 0, 0);
+      reinterpret_cast<unsigned long long*>(err), 0, 0, dens_floor);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1174,6 +1174,8 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   std::vector<uint8_t> use64(ni, 0);  // precision 32: instances switched to FP64
   std::vector<int32_t> last_kit(ni, 0);
   std::vector<double> heta(ni, opts->forcing ? std::max(opts->eta_max, opts->rtol) : opts->rtol);
+  const double sfloor = opts->scale_floor > 0.0 ? opts->scale_floor : opts->dens_floor;
+  const double eta_lo = std::max(opts->rtol, opts->eta_min);
   // Per-step launch lists: once the instances still iterating cover under
   // 3/4 of the pack, the assembly and the block-Jacobi set-up cover only
   // their tiles / flat blocks (rebuilt when that set changes).
@@ -1230,9 +1232,9 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       const double* sp_ = rel ? p : nullptr;
       const unsigned g = fl ? (unsigned)nfl : nb;
       if (pk->dim == 2)
-        k_bj_setup<2><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, opts->dens_floor, fl);
+        k_bj_setup<2><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, sfloor, fl);
       else
-        k_bj_setup<3><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, opts->dens_floor, fl);
+        k_bj_setup<3><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, sfloor, fl);
     }
     note_launch();
     TCAD_LAUNCH_CHECK();
@@ -1274,7 +1276,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       // stays in FP64 for the rest of the call.
       TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp32.data(), ni, cudaMemcpyHostToDevice, s));
       k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
-                                        active, w.err, opts->density_scaling, 1);
+                                        active, w.err, opts->density_scaling, 1, sfloor);
       note_launch();
       TCAD_LAUNCH_CHECK();
       TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
@@ -1313,7 +1315,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
         TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp32.data(), ni, cudaMemcpyHostToDevice, s));
         k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi,
                                           opts->dens_floor, active, w.err,
-                                          opts->density_scaling, 0);
+                                          opts->density_scaling, 0, sfloor);
         note_launch();
         TCAD_LAUNCH_CHECK();
       }
@@ -1338,7 +1340,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       }
       TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp64.data(), ni, cudaMemcpyHostToDevice, s));
       k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
-                                        active, w.err, opts->density_scaling, 0);
+                                        active, w.err, opts->density_scaling, 0, sfloor);
       note_launch();
       TCAD_LAUNCH_CHECK();
     }
@@ -1361,8 +1363,8 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       // forcing term of the next step (inexact Newton): quadratic convergence
       // is kept while the linear tolerance tracks the update size
       if (opts->forcing)
-        heta[i] = std::min(std::max(opts->eta_max, opts->rtol),
-                           std::max(opts->rtol, 0.1 * (std::isfinite(e) ? e : 1.0)));
+        heta[i] = std::min(std::max(opts->eta_max, eta_lo),
+                           std::max(eta_lo, 0.1 * (std::isfinite(e) ? e : 1.0)));
       if (polish_left[i] > 0) {
         // post-convergence polishing step (already counted as converged)
         if (--polish_left[i] == 0) hact[i] = 0;

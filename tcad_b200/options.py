@@ -87,6 +87,7 @@ class NewtonOptions:
     # every step to linsolve_rtol like the reference's iterative branch.
     forcing: str = "adaptive"
     eta_max: float = 1e-3
+    eta_min: float | None = None      # None: linsolve_rtol
     # GPU-only: "fp64" solves the Newton systems in FP64; "mixed" runs the
     # Krylov iterations in FP32 on an FP32 copy of the block-scaled Jacobian
     # inside FP64 iterative refinement -- residual, Newton update and the
@@ -97,6 +98,9 @@ class NewtonOptions:
     # through a similarity transform of the block-scaled Jacobian; "absolute"
     # for (dpsi, dn, dp).
     krylov_unknowns: str = "relative"
+    # GPU-only: floor of the density scale of the relative Krylov unknowns
+    # (a similarity transform: it changes the conditioning, not the solution)
+    krylov_scale_floor: float = 1e-10
     # GPU-only: start of a sweep point.  "secant" extrapolates the state
     # along the sweep when the new bias step is parallel to the previous one
     # (psi linearly, n and p in log space); "none" starts from the previous

@@ -236,7 +236,7 @@ def instance_par(s):
     return par
 
 
-def choose_tile_z(setups, dim, sm_count=148, ctas_per_sm=3, waves=2.0):
+def choose_tile_z(setups, dim, sm_count=148, ctas_per_sm=3, waves=4.0):
     """Z depth of the 3D assembly tiles: the deepest of 16, 8, 4, 2 planes
     whose tile count still fills `waves` waves of the GPU's CTA slots (a
     deeper tile re-evaluates fewer z-edges at its first plane; a shallower
@@ -663,6 +663,9 @@ class Pack:
         o.eta_max = float(getattr(opts, "eta_max", 1e-3))
         o.precision = 32 if getattr(opts, "precision", "fp64") == "mixed" and not equilibrium else 64
         o.density_scaling = 1 if getattr(opts, "krylov_unknowns", "relative") == "relative" else 0
+        em = getattr(opts, "eta_min", None)
+        o.eta_min = float(opts.linsolve_rtol if em is None else em)
+        o.scale_floor = float(getattr(opts, "krylov_scale_floor", 1e-10))
         return o
 
     def newton(self, opts, active=None):

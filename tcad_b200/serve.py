@@ -309,7 +309,10 @@ class Worker(threading.Thread):
         self.torch = torch
         self.dim = dim
         self.opts = opts
-        self.device = torch.device(device)
+        dev = torch.device(device)
+        if dev.type == "cuda" and dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
         self.arena = Arena(dim, budget_bytes, device, max_inst)
         self.max_round_nodes = max_round_nodes or self.arena.cap
         self.stream = torch.cuda.Stream(device=self.device)
@@ -512,34 +515,33 @@ class Worker(threading.Thread):
 
     def run(self):
         torch = self.torch
-        torch.cuda.set_device(self.device)
-        with torch.cuda.stream(self.stream):
-            while True:
-                with self.cv:
-                    while self.running and not self.queue and not self.active:
-                        self.cv.wait(0.05)
-                    if not self.running and not self.active and not self.queue:
-                        break
-                    if self.aborting:
-                        for r in self.active:
-                            r.error = "cancelled"
-                            r._session.busy = False
-                        self.active = []
-                        break
-                try:
-                    self.run_round()
-                except Exception as exc:     # fail what is in flight and queued, stop
-                    self.error = exc
+        try:
+            torch.cuda.set_device(self.device)
+            with torch.cuda.stream(self.stream):
+                while True:
                     with self.cv:
-                        failed = self.active + list(self.queue)
-                        self.queue.clear()
-                    for r in failed:
-                        r.error = repr(exc)
-                        r.finished = time.perf_counter()
-                        r.done.set()
-                    self.active = []
-                    break
-            self.stream.synchronize()
+                        while self.running and not self.queue and not self.active:
+                            self.cv.wait(0.05)
+                        if not self.running and not self.active and not self.queue:
+                            break
+                        if self.aborting:
+                            for r in self.active:
+                                r.error = "cancelled"
+                                r._session.busy = False
+                            self.active = []
+                            break
+                    self.run_round()
+                self.stream.synchronize()
+        except Exception as exc:     # fail what is in flight and queued, stop
+            self.error = exc
+            with self.cv:
+                failed = self.active + list(self.queue)
+                self.queue.clear()
+            for r in failed:
+                r.error = repr(exc)
+                r.finished = time.perf_counter()
+                r.done.set()
+            self.active = []
 
 
 # Default cap of the nodes one round solves: large enough that every kernel
@@ -584,4 +586,7 @@ class Server:
             if t_end is not None and time.perf_counter() > t_end:
                 return False
             time.sleep(0.002)
+        for w in self.workers.values():
+            if w.error is not None:
+                raise RuntimeError(f"{w.dim}D worker failed") from w.error
         return True
