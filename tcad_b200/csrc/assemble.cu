@@ -23,8 +23,13 @@ struct NodeVals {
 // Neighbour-block entry offsets: 9 + 5*d + m.
 __device__ __forceinline__ int nb(int d, int m) { return 9 + 5 * d + m; }
 
+// CTAs per SM the coupled assembly is compiled for (register budget)
+#ifndef TCAD_ASM_MIN_CTAS
+#define TCAD_ASM_MIN_CTAS 3
+#endif
+
 template <int DIM>
-__global__ void __launch_bounds__(kTileThreads, 3)
+__global__ void __launch_bounds__(kTileThreads, TCAD_ASM_MIN_CTAS)
 k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
               const double* __restrict__ nn, const double* __restrict__ pp,
               double* __restrict__ F, double* __restrict__ J, int mode,
