@@ -64,8 +64,8 @@ METHOD_DESC = {
     "plain": "plain FP64: fused SG assembly, node-block-Jacobi BiCGStab to rtol 1e-10 on "
              "(dpsi, dn, dp) every Newton step, damped Newton",
     "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the block-scaled system in "
-            "relative unknowns (dpsi, dn/n, dp/p) with forcing eta_k = clamp(0.1 "
-            "update_{k-1}, 1e-10, 1e-3); secant predictor along the sweep",
+            "relative unknowns (dpsi, dn/n, dp/p) solved to 1e-3 every Newton step, one "
+            "polishing step, secant predictor along the sweep",
     "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
              "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
              "relative unknowns, adaptive forcing, secant predictor; per-instance FP64 "

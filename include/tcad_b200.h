@@ -49,7 +49,7 @@ extern "C" {
 
 #define TCAD_NE2 29
 #define TCAD_NE3 39
-#define TCAD_FLAT_NODES 256  /* default nodes per flat (vector-kernel) block */
+#define TCAD_FLAT_NODES 512  /* default nodes per flat (vector-kernel) block */
 #define TCAD_TILE_X 32       /* stencil tile: 32 x 8 nodes (x, y) */
 #define TCAD_TILE_Y 8
 #define TCAD_TILE_Z 16       /* largest z depth of a 3D stencil tile (tile_z <= this) */

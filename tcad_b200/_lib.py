@@ -25,7 +25,7 @@ STATUS_NAMES = {0: "ok", 1: "bad argument", 2: "singular node block",
                 6: "Krylov breakdown", -1: "idle"}
 
 NE = {2: 29, 3: 39}
-FLAT_NODES = 256
+FLAT_NODES = 512
 TILE_X, TILE_Y, TILE_Z_MAX = 32, 8, 16
 NPAR = 8
 MODE_RAW, MODE_ELIMINATE = 0, 1

@@ -87,7 +87,10 @@ class NewtonOptions:
     # every step to linsolve_rtol like the reference's iterative branch.
     forcing: str = "adaptive"
     eta_max: float = 1e-3
-    eta_min: float | None = None      # None: linsolve_rtol
+    # tightest forcing term; None: eta_max for precision "fp64" (every step
+    # to 1e-3: once Newton converges quadratically the step's size, not the
+    # linear tolerance, decides the next update), linsolve_rtol for "mixed"
+    eta_min: float | None = None
     # GPU-only: "fp64" solves the Newton systems in FP64; "mixed" runs the
     # Krylov iterations in FP32 on an FP32 copy of the block-scaled Jacobian
     # inside FP64 iterative refinement -- residual, Newton update and the

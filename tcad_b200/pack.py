@@ -664,7 +664,9 @@ class Pack:
         o.precision = 32 if getattr(opts, "precision", "fp64") == "mixed" and not equilibrium else 64
         o.density_scaling = 1 if getattr(opts, "krylov_unknowns", "relative") == "relative" else 0
         em = getattr(opts, "eta_min", None)
-        o.eta_min = float(opts.linsolve_rtol if em is None else em)
+        if em is None:
+            em = o.eta_max if o.precision == 64 else opts.linsolve_rtol
+        o.eta_min = float(em)
         o.scale_floor = float(getattr(opts, "krylov_scale_floor", 1e-10))
         return o
 
