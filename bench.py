@@ -46,7 +46,7 @@ BYTES_ASM = {2: (13 + 32) * 8 + 1, 3: (16 + 42) * 8 + 1}
 # Newton iterations / BiCGStab iterations per bias point of the plain FP64
 # path on this workload, from its own bench runs; used only to scale the
 # CPU oracle's measured per-iteration costs to a bias point.
-TRIGATE_ITERS = {"newton_per_point": 4.0, "krylov_per_newton": 250.0}
+TRIGATE_ITERS = {"newton_per_point": 6.0, "krylov_per_newton": 1078.0}
 
 
 # The Newton/Krylov methods the bench can time.  "plain" is the reference's
