@@ -96,7 +96,7 @@ def parse():
                     help="mosfet2d_batch: instances of the sequential plain run")
     ap.add_argument("--small", action="store_true", help="down-scaled mesh (testing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--method", default="mixed", choices=list(METHODS),
+    ap.add_argument("--method", default="fp64", choices=list(METHODS),
                     help="the timed (chosen) path; the plain FP64 path is always run "
                          "beside it on the same points for the current check")
     ap.add_argument("--verbose", action="store_true")
