@@ -200,6 +200,20 @@ int tcad_block_jacobi_setup_rel(const tcad_pack_t* pk, double* J, double* F,
                                 int32_t* status, const double* n, const double* p,
                                 double dens_floor, void* stream);
 
+/* Block ILU(0) of the block-scaled 2D operator A^ (J prepared by either
+ * set-up above), the stronger preconditioner the reference reaches for on
+ * hard 2D systems (pytcad/linsolve.py:430-525 builds an ILU-based one on
+ * the CPU).  For the 5-point block stencil ILU(0) keeps the off-diagonal
+ * blocks and replaces the diagonal ones: Q [9][n_nodes] receives their
+ * inverses (tcad_block_ilu_bytes).  status[inst] gets TCAD_ERR_SINGULAR for
+ * a singular block.  One CTA per instance sweeps its anti-diagonals. */
+size_t tcad_block_ilu_bytes(const tcad_pack_t* pk);
+int tcad_block_ilu_setup(const tcad_pack_t* pk, const double* J, double* Q,
+                         int32_t* status, void* stream);
+/* out = M^-1 r for the ILU(0) factor Q (r and out distinct, [3][n_nodes]). */
+int tcad_block_ilu_apply(const tcad_pack_t* pk, const double* J, const double* Q,
+                         const double* r, double* out, void* stream);
+
 /* y = A^ x with A^ = I + D^-1 (off-diagonal blocks), J prepared by
  * tcad_block_jacobi_setup; x, y are [3][n_nodes]. */
 int tcad_block_spmv(const tcad_pack_t* pk, const double* J, const double* x,
@@ -281,7 +295,8 @@ typedef struct tcad_newton_opts {
                             convergence test stay FP64) */
   int32_t density_scaling; /* 1: Krylov unknowns are (dpsi, dn/s_n, dp/s_p), s = max(n|p,
                               scale_floor) -- the quantities of the Newton update test */
-  int32_t pad;
+  int32_t precond;       /* 0: node-block Jacobi; 1: + block ILU(0) right preconditioner on
+                            2D packs (FP64 Krylov; 3D packs use node-block Jacobi) */
   double eta_min;        /* forcing 1: tightest Krylov tolerance of a step (>= rtol) */
   double scale_floor;    /* density_scaling: floor of s (dens_floor when <= 0) */
 } tcad_newton_opts_t;

@@ -60,7 +60,7 @@ class NewtonOpts(ctypes.Structure):
                 ("verbose", ctypes.c_int32), ("polish", ctypes.c_int32),
                 ("eta_max", ctypes.c_double), ("forcing", ctypes.c_int32),
                 ("precision", ctypes.c_int32),
-                ("density_scaling", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("density_scaling", ctypes.c_int32), ("precond", ctypes.c_int32),
                 ("eta_min", ctypes.c_double), ("scale_floor", ctypes.c_double)]
 
 
@@ -87,6 +87,9 @@ _SIGS = {
     "tcad_block_jacobi_setup_rel": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, ctypes.c_double,
                                                    _p]),
     "tcad_block_spmv": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "tcad_block_ilu_bytes": (ctypes.c_size_t, [_p]),
+    "tcad_block_ilu_setup": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "tcad_block_ilu_apply": (ctypes.c_int, [_p, _p, _p, _p, _p, _p]),
     "tcad_block_krylov": (ctypes.c_int, [_p, _p, _p, _p, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_int, ctypes.c_int, _p, ctypes.c_size_t,
                                          _p, _p, _p, _p]),

@@ -1,0 +1,217 @@
+// Block ILU(0) of the node-block-scaled 2D operator, as a right
+// preconditioner of the BiCGStab in krylov.cu.
+//
+// The scaled operator is A^ = I + G_k sum_d B_kd (node k, neighbours
+// d = W, E, S, N): G_k is the (row-scaled) inverse diagonal block stored in
+// J entries 0..8, B_kd the 5-entry neighbour block (psi<-psi, n<-psi, n<-n,
+// p<-psi, p<-p) in entries 9 + 5d + m.  For the 5-point block stencil
+// ILU(0) keeps the off-diagonal blocks of A^ and changes only the diagonal
+// ones (no fill survives), i.e. M = (D~ + L^) D~^-1 (D~ + U^) with
+//   D~_k = I - G_k (B_kW D~_W^-1 G_W B_WE + B_kS D~_S^-1 G_S B_SN)
+// (W, S the lower neighbours in the x-fastest natural order).  Q_k = D~_k^-1
+// is stored (9 doubles per node).  Applying M^-1 r:
+//   forward  a_k = Q_k (r_k - G_k (B_kW a_W + B_kS a_S))
+//   backward x_k = a_k - Q_k G_k (B_kE x_E + B_kN x_N)
+// Node (i, j) depends on (i-1, j) and (i, j-1) only, so all nodes of an
+// anti-diagonal i + j = d are independent: one CTA per instance sweeps the
+// nx + ny - 1 anti-diagonals with a block barrier between them (global
+// writes of a level are visible to the block after the barrier).
+#pragma once
+
+namespace tcad {
+
+constexpr int kIluThreads = 256;
+
+// C = M * B with B the sparse neighbour block (b0..b4)
+__device__ __forceinline__ void mul_dense_nb(const double* M, const double* b, double* C) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    C[3 * r + 0] = M[3 * r + 0] * b[0] + M[3 * r + 1] * b[1] + M[3 * r + 2] * b[3];
+    C[3 * r + 1] = M[3 * r + 1] * b[2];
+    C[3 * r + 2] = M[3 * r + 2] * b[4];
+  }
+}
+
+// C = B * M with B the sparse neighbour block
+__device__ __forceinline__ void mul_nb_dense(const double* b, const double* M, double* C) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    C[0 + c] = b[0] * M[0 + c];
+    C[3 + c] = b[1] * M[0 + c] + b[2] * M[3 + c];
+    C[6 + c] = b[3] * M[0 + c] + b[4] * M[6 + c];
+  }
+}
+
+__device__ __forceinline__ void mul33(const double* A, const double* B, double* C) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      C[3 * r + c] = A[3 * r + 0] * B[0 + c] + A[3 * r + 1] * B[3 + c] + A[3 * r + 2] * B[6 + c];
+}
+
+__device__ __forceinline__ void load9(const double* __restrict__ X, int64_t NN, int64_t k,
+                                      int e0, double* out) {
+#pragma unroll
+  for (int e = 0; e < 9; ++e) out[e] = X[(int64_t)(e0 + e) * NN + k];
+}
+
+__device__ __forceinline__ void load_nb(const double* __restrict__ J, int64_t NN, int64_t k,
+                                        int d, double* b) {
+#pragma unroll
+  for (int m = 0; m < 5; ++m) b[m] = J[(int64_t)(9 + 5 * d + m) * NN + k];
+}
+
+// y += B v (sparse neighbour block)
+__device__ __forceinline__ void add_nb_vec(const double* b, double v0, double v1, double v2,
+                                           double& y0, double& y1, double& y2) {
+  y0 += b[0] * v0;
+  y1 += b[1] * v0 + b[2] * v1;
+  y2 += b[3] * v0 + b[4] * v2;
+}
+
+// Factor: Q_k for every node of each instance whose pre_status is TCAD_OK;
+// status[inst] = TCAD_ERR_SINGULAR when a D~ block is singular.
+__global__ void __launch_bounds__(kIluThreads)
+k_ilu2d_factor(const tcad_pack_t pk, const double* __restrict__ J, double* __restrict__ Q,
+               const int32_t* __restrict__ pre_status, int32_t* __restrict__ status) {
+  const int inst = blockIdx.x;
+  if (pre_status && pre_status[inst] != TCAD_OK) return;
+  const Inst g = load_inst(pk, inst);
+  const int64_t NN = pk.n_nodes;
+  const int nx = g.nx, ny = g.ny;
+  for (int d = 0; d < nx + ny - 1; ++d) {
+    const int jlo = d - (nx - 1) > 0 ? d - (nx - 1) : 0;
+    const int jhi = d < ny - 1 ? d : ny - 1;
+    for (int j = jlo + threadIdx.x; j <= jhi; j += kIluThreads) {
+      const int i = d - j;
+      const int64_t k = g.off + (int64_t)j * nx + i;
+      double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      double b[5], G[9], Qm[9], T1[9], T2[9], T3[9];
+      if (i > 0) {  // W: term B_kW Q_W G_W B_WE
+        const int64_t m = k - 1;
+        load9(J, NN, m, 0, G);
+        load_nb(J, NN, m, 1, b);
+        mul_dense_nb(G, b, T1);
+        load9(Q, NN, m, 0, Qm);
+        mul33(Qm, T1, T2);
+        load_nb(J, NN, k, 0, b);
+        mul_nb_dense(b, T2, T3);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) S[e] += T3[e];
+      }
+      if (j > 0) {  // S: term B_kS Q_S G_S B_SN
+        const int64_t m = k - nx;
+        load9(J, NN, m, 0, G);
+        load_nb(J, NN, m, 3, b);
+        mul_dense_nb(G, b, T1);
+        load9(Q, NN, m, 0, Qm);
+        mul33(Qm, T1, T2);
+        load_nb(J, NN, k, 2, b);
+        mul_nb_dense(b, T2, T3);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) S[e] += T3[e];
+      }
+      load9(J, NN, k, 0, G);
+      double D[9];
+      mul33(G, S, D);
+#pragma unroll
+      for (int e = 0; e < 9; ++e) D[e] = (e % 4 == 0 ? 1.0 : 0.0) - D[e];
+      const double c00 = D[4] * D[8] - D[5] * D[7];
+      const double c01 = D[5] * D[6] - D[3] * D[8];
+      const double c02 = D[3] * D[7] - D[4] * D[6];
+      const double det = D[0] * c00 + D[1] * c01 + D[2] * c02;
+      double inv[9];
+      if (isfinite(det) && fabs(det) >= 1e-300) {
+        const double id = 1.0 / det;
+        inv[0] = c00 * id;
+        inv[1] = (D[2] * D[7] - D[1] * D[8]) * id;
+        inv[2] = (D[1] * D[5] - D[2] * D[4]) * id;
+        inv[3] = c01 * id;
+        inv[4] = (D[0] * D[8] - D[2] * D[6]) * id;
+        inv[5] = (D[2] * D[3] - D[0] * D[5]) * id;
+        inv[6] = c02 * id;
+        inv[7] = (D[1] * D[6] - D[0] * D[7]) * id;
+        inv[8] = (D[0] * D[4] - D[1] * D[3]) * id;
+      } else {
+        if (status) atomicExch(&status[inst], TCAD_ERR_SINGULAR);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) inv[e] = (e % 4 == 0) ? 1.0 : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 9; ++e) Q[(int64_t)e * NN + k] = inv[e];
+    }
+    __syncthreads();
+  }
+}
+
+// out = M^-1 rin for every instance still iterating (ks[inst].active).
+template <class T>
+__global__ void __launch_bounds__(kIluThreads)
+k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ Q,
+              const T* __restrict__ rin, T* __restrict__ out, const KState* ks) {
+  const int inst = blockIdx.x;
+  if (ks && !ks[inst].active) return;
+  const Inst g = load_inst(pk, inst);
+  const int64_t NN = pk.n_nodes;
+  const int nx = g.nx, ny = g.ny;
+  const int nd = nx + ny - 1;
+  // forward: a_k = Q_k (r_k - G_k (B_kW a_W + B_kS a_S))
+  for (int d = 0; d < nd; ++d) {
+    const int jlo = d - (nx - 1) > 0 ? d - (nx - 1) : 0;
+    const int jhi = d < ny - 1 ? d : ny - 1;
+    for (int j = jlo + threadIdx.x; j <= jhi; j += kIluThreads) {
+      const int i = d - j;
+      const int64_t k = g.off + (int64_t)j * nx + i;
+      double u0 = 0.0, u1 = 0.0, u2 = 0.0, b[5];
+      if (i > 0) {
+        load_nb(J, NN, k, 0, b);
+        add_nb_vec(b, out[k - 1], out[NN + k - 1], out[2 * NN + k - 1], u0, u1, u2);
+      }
+      if (j > 0) {
+        load_nb(J, NN, k, 2, b);
+        add_nb_vec(b, out[k - nx], out[NN + k - nx], out[2 * NN + k - nx], u0, u1, u2);
+      }
+      double G[9], Qk[9];
+      load9(J, NN, k, 0, G);
+      load9(Q, NN, k, 0, Qk);
+      const double t0 = rin[k] - (G[0] * u0 + G[1] * u1 + G[2] * u2);
+      const double t1 = rin[NN + k] - (G[3] * u0 + G[4] * u1 + G[5] * u2);
+      const double t2 = rin[2 * NN + k] - (G[6] * u0 + G[7] * u1 + G[8] * u2);
+      out[k] = (T)(Qk[0] * t0 + Qk[1] * t1 + Qk[2] * t2);
+      out[NN + k] = (T)(Qk[3] * t0 + Qk[4] * t1 + Qk[5] * t2);
+      out[2 * NN + k] = (T)(Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2);
+    }
+    __syncthreads();
+  }
+  // backward: x_k = a_k - Q_k G_k (B_kE x_E + B_kN x_N), in place
+  for (int d = nd - 1; d >= 0; --d) {
+    const int jlo = d - (nx - 1) > 0 ? d - (nx - 1) : 0;
+    const int jhi = d < ny - 1 ? d : ny - 1;
+    for (int j = jlo + threadIdx.x; j <= jhi; j += kIluThreads) {
+      const int i = d - j;
+      const int64_t k = g.off + (int64_t)j * nx + i;
+      double u0 = 0.0, u1 = 0.0, u2 = 0.0, b[5];
+      if (i < nx - 1) {
+        load_nb(J, NN, k, 1, b);
+        add_nb_vec(b, out[k + 1], out[NN + k + 1], out[2 * NN + k + 1], u0, u1, u2);
+      }
+      if (j < ny - 1) {
+        load_nb(J, NN, k, 3, b);
+        add_nb_vec(b, out[k + nx], out[NN + k + nx], out[2 * NN + k + nx], u0, u1, u2);
+      }
+      double G[9], Qk[9];
+      load9(J, NN, k, 0, G);
+      load9(Q, NN, k, 0, Qk);
+      const double t0 = G[0] * u0 + G[1] * u1 + G[2] * u2;
+      const double t1 = G[3] * u0 + G[4] * u1 + G[5] * u2;
+      const double t2 = G[6] * u0 + G[7] * u1 + G[8] * u2;
+      out[k] = (T)((double)out[k] - (Qk[0] * t0 + Qk[1] * t1 + Qk[2] * t2));
+      out[NN + k] = (T)((double)out[NN + k] - (Qk[3] * t0 + Qk[4] * t1 + Qk[5] * t2));
+      out[2 * NN + k] = (T)((double)out[2 * NN + k] - (Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2));
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace tcad

@@ -82,6 +82,10 @@ struct Reduce {
   }
 };
 
+}  // namespace tcad
+#include "ilu.cuh"
+namespace tcad {
+
 // --------------------------------------------------------------------------
 // block-Jacobi set-up: invert the 3x3 diagonal blocks, scale the rhs
 //
@@ -212,6 +216,7 @@ k_spmv(const tcad_pack_t pk, const double* __restrict__ J, const double* __restr
 template <class T>
 struct BiVecT {
   T *r, *rh, *p, *v, *s, *t;
+  T *ph, *sh;  // M^-1 p and M^-1 s (right preconditioner); = p, s without one
 };
 using BiVec = BiVecT<double>;
 
@@ -287,7 +292,7 @@ k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
   double v[1] = {0.0};
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
     T y0, y1, y2;
-    spmv_node<DIM, true, T>(J, w.p, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    spmv_node<DIM, true, T>(J, w.ph, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
     w.v[k] = y0; w.v[NN + k] = y1; w.v[2 * NN + k] = y2;
     v[0] += (double)w.rh[k] * y0 + (double)w.rh[NN + k] * y1 + (double)w.rh[2 * NN + k] * y2;
   }
@@ -349,7 +354,7 @@ k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
   double v[2] = {0.0, 0.0};
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
     T y0, y1, y2;
-    spmv_node<DIM, true, T>(J, w.s, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    spmv_node<DIM, true, T>(J, w.sh, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
     w.t[k] = y0; w.t[NN + k] = y1; w.t[2 * NN + k] = y2;
     v[0] += (double)y0 * w.s[k] + (double)y1 * w.s[NN + k] + (double)y2 * w.s[2 * NN + k];
     v[1] += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
@@ -377,7 +382,7 @@ k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double*
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t q = c * NN + k;
-      x[q] = x[q] + alpha * w.p[q] + omega * w.s[q];
+      x[q] = x[q] + alpha * w.ph[q] + omega * w.sh[q];
       const T r = w.s[q] - omega * w.t[q];
       w.r[q] = r;
       const double rh = w.rh[q];
@@ -781,12 +786,34 @@ static Work32 carve32(const tcad_pack_t* pk, void* base) {
   w.bi.v = c.take<float>(v3);
   w.bi.s = c.take<float>(v3);
   w.bi.t = c.take<float>(v3);
+  w.bi.ph = w.bi.p;
+  w.bi.sh = w.bi.s;
   w.J32 = c.take<float>((size_t)(pk->dim == 2 ? TCAD_NE2 : TCAD_NE3) * pk->n_nodes);
   w.r32 = c.take<float>(v3);
   w.d32 = c.take<float>(v3);
   w.irs = c.take<KState>(pk->n_inst);
   w.eta_in = c.take<double>(pk->n_inst);
   w.pre = c.take<int32_t>(pk->n_inst);
+  w.bytes = c.used;
+  return w;
+}
+
+// ILU(0) extension (2D packs): Q = D~^-1 per node, M^-1 p and M^-1 s
+struct WorkIlu {
+  double* Q;
+  double* ph;
+  double* sh;
+  size_t bytes;
+};
+
+static WorkIlu carve_ilu(const tcad_pack_t* pk, void* base) {
+  Carve c{reinterpret_cast<char*>(base), 0, 0};
+  WorkIlu w{nullptr, nullptr, nullptr, 0};
+  if (pk->dim != 2) return w;
+  const size_t v3 = 3 * (size_t)pk->n_nodes;
+  w.Q = c.take<double>(9 * (size_t)pk->n_nodes);
+  w.ph = c.take<double>(v3);
+  w.sh = c.take<double>(v3);
   w.bytes = c.used;
   return w;
 }
@@ -801,6 +828,8 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   w.bi.v = c.take<double>(v3);
   w.bi.s = c.take<double>(v3);
   w.bi.t = c.take<double>(v3);
+  w.bi.ph = w.bi.p;
+  w.bi.sh = w.bi.s;
   // the scalar PCG reuses the first vector's storage (3 x n_nodes)
   w.cg.r = w.bi.r;
   w.cg.z = w.bi.r + pk->n_nodes;
@@ -823,7 +852,8 @@ template <class T>
 static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x, double rtol,
                              int maxiter, const BiVecT<T>& bi, const Work& w,
                              const int32_t* pre_status, std::vector<KState>& hks,
-                             cudaStream_t s, const double* rtol_inst) {
+                             cudaStream_t s, const double* rtol_inst,
+                             const double* Jilu = nullptr, const double* Qilu = nullptr) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
@@ -855,6 +885,11 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
     for (int q = 0; q < check; ++q) {
       k_bi_p<<<ng, NT, 0, s>>>(*pk, bi, w.ks, dlist);
       note_launch();
+      if (Qilu) {  // ph = M^-1 p (one CTA per instance)
+        k_ilu2d_apply<T><<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, Jilu, Qilu, bi.p, bi.ph,
+                                                               w.ks);
+        note_launch();
+      }
       if (pk->dim == 2)
         k_bi_v<2><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
       else
@@ -862,6 +897,11 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
       note_launch();
       k_bi_s<<<ng, NT, 0, s>>>(*pk, bi, w.ks, w.partial, w.ticket, dlist);
       note_launch();
+      if (Qilu) {  // sh = M^-1 s
+        k_ilu2d_apply<T><<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, Jilu, Qilu, bi.s, bi.sh,
+                                                               w.ks);
+        note_launch();
+      }
       if (pk->dim == 2)
         k_bi_t<2><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
       else
@@ -927,7 +967,15 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
 static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double* b,
                            double* x, double rtol, int maxiter, const Work& w,
                            const int32_t* pre_status, std::vector<KState>& hks,
-                           cudaStream_t s, const double* rtol_inst = nullptr) {
+                           cudaStream_t s, const double* rtol_inst = nullptr,
+                           const WorkIlu* ilu = nullptr) {
+  if (ilu && ilu->Q) {
+    BiVec bi = w.bi;
+    bi.ph = ilu->ph;
+    bi.sh = ilu->sh;
+    return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, bi, w, pre_status, hks, s,
+                                     rtol_inst, J, ilu->Q);
+  }
   return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, w.bi, w, pre_status, hks, s,
                                    rtol_inst);
 }
@@ -1056,7 +1104,10 @@ extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, 
   (void)method; (void)restart;
   Work w = carve(pk, nullptr, 0);
   Work32 w32 = carve32(pk, nullptr);
-  return w.bytes + w32.bytes + 512;  // FP64 work, then the FP32 extension
+  WorkIlu wi = carve_ilu(pk, nullptr);
+  // FP64 work, then the FP32 extension, then the ILU(0) extension (2D)
+  return ((w.bytes + 255) & ~(size_t)255) + ((w32.bytes + 255) & ~(size_t)255) + wi.bytes +
+         512;
 }
 
 extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
@@ -1086,6 +1137,33 @@ extern "C" int tcad_block_jacobi_setup_rel(const tcad_pack_t* pk, double* J, dou
   else
     k_bj_setup<3><<<(unsigned)pk->n_flat, NT, 0, (cudaStream_t)stream>>>(*pk, J, F, status, n,
                                                                          p, dens_floor, nullptr);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" size_t tcad_block_ilu_bytes(const tcad_pack_t* pk) {
+  if (!pack_ok(pk) || pk->dim != 2) return 0;
+  return 9 * sizeof(double) * (size_t)pk->n_nodes;
+}
+
+extern "C" int tcad_block_ilu_setup(const tcad_pack_t* pk, const double* J, double* Q,
+                                    int32_t* status, void* stream) {
+  if (!pack_ok(pk) || pk->dim != 2 || !J || !Q || !status) return TCAD_ERR_ARG;
+  if (pk->n_inst < 1) return TCAD_OK;
+  k_ilu2d_factor<<<(unsigned)pk->n_inst, kIluThreads, 0, (cudaStream_t)stream>>>(
+      *pk, J, Q, nullptr, status);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_block_ilu_apply(const tcad_pack_t* pk, const double* J, const double* Q,
+                                    const double* r, double* out, void* stream) {
+  if (!pack_ok(pk) || pk->dim != 2 || !J || !Q || !r || !out || r == out) return TCAD_ERR_ARG;
+  if (pk->n_inst < 1) return TCAD_OK;
+  k_ilu2d_apply<double><<<(unsigned)pk->n_inst, kIluThreads, 0, (cudaStream_t)stream>>>(
+      *pk, J, Q, r, out, nullptr);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1169,6 +1247,13 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   if (opts->precision == 32 && work_bytes < tcad_block_workspace_bytes(pk, 0, 0))
     return TCAD_ERR_ARG;
   const Work32 w32 = carve32(pk, reinterpret_cast<char*>(work) + ((w.bytes + 255) & ~(size_t)255));
+  // ILU(0) right preconditioner (2D): its region follows the FP32 extension
+  const bool use_ilu = opts->precond == 1 && pk->dim == 2;
+  if (use_ilu && work_bytes < tcad_block_workspace_bytes(pk, 0, 0)) return TCAD_ERR_ARG;
+  const WorkIlu wilu = use_ilu ? carve_ilu(pk, reinterpret_cast<char*>(work) +
+                                                   ((w.bytes + 255) & ~(size_t)255) +
+                                                   ((w32.bytes + 255) & ~(size_t)255))
+                               : WorkIlu{nullptr, nullptr, nullptr, 0};
   std::vector<int32_t> mix_it(ni), mix_st(ni), mix_grew(ni, 0), mix_steps(ni, 0);
   std::vector<double> mix_rr(ni), mix_prev(ni, -1.0);
   std::vector<uint8_t> use64(ni, 0);  // precision 32: instances switched to FP64
@@ -1327,8 +1412,13 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       for (int i = 0; i < ni; ++i) st64[i] = grp64[i] ? hstat[i] : -1;
       TCAD_CUDA_CHECK(cudaMemcpyAsync(w.status, st64.data(), sizeof(int32_t) * ni,
                                       cudaMemcpyHostToDevice, s));
+      if (use_ilu) {  // factor once per Newton step, for the FP64 group
+        k_ilu2d_factor<<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, J, wilu.Q, w.status, nullptr);
+        note_launch();
+        TCAD_LAUNCH_CHECK();
+      }
       rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
-                           w.eta);
+                           w.eta, use_ilu ? &wilu : nullptr);
       if (rc != TCAD_OK) return rc;
       // instances whose linear solve broke down / diverged keep their state
       for (int i = 0; i < ni; ++i) {

@@ -113,7 +113,7 @@ class NewtonOptions:
     predictor: str = "secant"
 
     def __post_init__(self):
-        if self.precond not in ("auto", "block_jacobi", "schur"):
+        if self.precond not in ("auto", "block_jacobi", "schur", "ilu"):
             raise ValueError(f"NewtonOptions.precond={self.precond!r} is not a known "
                              "preconditioner flavor")
         if self.block_size is not None and (

@@ -668,6 +668,7 @@ class Pack:
             em = o.eta_max if o.precision == 64 else opts.linsolve_rtol
         o.eta_min = float(em)
         o.scale_floor = float(getattr(opts, "krylov_scale_floor", 1e-10))
+        o.precond = 1 if getattr(opts, "precond", "auto") == "ilu" else 0
         return o
 
     def newton(self, opts, active=None):
