@@ -299,6 +299,8 @@ typedef struct tcad_newton_opts {
                             2D packs (FP64 Krylov; 3D packs use node-block Jacobi) */
   double eta_min;        /* forcing 1: tightest Krylov tolerance of a step (>= rtol) */
   double scale_floor;    /* density_scaling: floor of s (dens_floor when <= 0) */
+  double polish_eta;     /* forcing 1: Krylov tolerance of the polishing steps (<= 0: the
+                            forcing rule's) */
 } tcad_newton_opts_t;
 
 /* Per-instance result of a Newton solve (host memory). */

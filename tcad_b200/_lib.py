@@ -61,7 +61,8 @@ class NewtonOpts(ctypes.Structure):
                 ("eta_max", ctypes.c_double), ("forcing", ctypes.c_int32),
                 ("precision", ctypes.c_int32),
                 ("density_scaling", ctypes.c_int32), ("precond", ctypes.c_int32),
-                ("eta_min", ctypes.c_double), ("scale_floor", ctypes.c_double)]
+                ("eta_min", ctypes.c_double), ("scale_floor", ctypes.c_double),
+                ("polish_eta", ctypes.c_double)]
 
 
 class NewtonResult(ctypes.Structure):

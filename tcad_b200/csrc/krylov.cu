@@ -1462,6 +1462,10 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
         result[i].converged = 1;
         polish_left[i] = opts->polish > 0 ? opts->polish : 0;
         if (polish_left[i] == 0) hact[i] = 0;
+        // the polishing steps resolve what the floored update test cannot
+        // see (sub-floor densities, low-bias currents): their own tolerance
+        else if (opts->forcing && opts->polish_eta > 0.0)
+          heta[i] = std::max(opts->rtol, opts->polish_eta);
       } else if (hard || !(e == e) || e == INFINITY) {
         hact[i] = 0;  // singular block / non-finite state: this instance failed
       }

@@ -81,6 +81,10 @@ class NewtonOptions:
     # (and low-bias currents) are converged only to ~1e-5 when it first
     # passes; one more quadratic step brings them to round-off.
     polish: int = 1
+    # GPU-only: Krylov tolerance of the polishing steps.  Low-bias currents
+    # are small differences of large drift and diffusion fluxes, so the
+    # state after the last step must be accurate well beyond the update test.
+    polish_eta: float = 1e-10
     # GPU-only: inexact-Newton forcing.  "adaptive" solves step k to
     # eta_k = clamp(0.1 * update_{k-1}, linsolve_rtol, eta_max) (quadratic
     # convergence is kept; the converged state is the same); "fixed" solves

@@ -669,6 +669,7 @@ class Pack:
         o.eta_min = float(em)
         o.scale_floor = float(getattr(opts, "krylov_scale_floor", 1e-10))
         o.precond = 1 if getattr(opts, "precond", "auto") == "ilu" else 0
+        o.polish_eta = float(getattr(opts, "polish_eta", 1e-10))
         return o
 
     def newton(self, opts, active=None):
