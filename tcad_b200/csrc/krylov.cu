@@ -253,8 +253,11 @@ k_bi_init(const tcad_pack_t pk, const T* __restrict__ b, T* __restrict__ x, BiVe
 }
 
 // p = r + beta (p - omega v)   (restart: rh = r, p = r)
+// The vector kernels read through restrict-qualified locals and issue every
+// load of two nodes before any store, so each thread keeps a dozen loads in
+// flight (the struct members alone would force load-store serialisation).
 template <class T>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
 k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __restrict__ blk) {
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
   const FlatBlock fb = flat_block(pk, fbi);
@@ -262,16 +265,36 @@ k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __res
   if (!s.active) return;
   const int64_t NN = pk.n_nodes;
   const T beta = (T)s.beta, omega = (T)s.omega;
-  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+  const T* __restrict__ R = w.r;
+  const T* __restrict__ V = w.v;
+  T* __restrict__ P = w.p;
+  T* __restrict__ RH = w.rh;
+  for (int64_t k0 = fb.begin + threadIdx.x; k0 < fb.end; k0 += 2 * NT) {
+    const int64_t k1 = k0 + NT;
+    const bool two = k1 < fb.end;
+    T r[6], pv[6], vv[6];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int64_t q = c * NN + k;
-      const T r = w.r[q];
-      if (s.restart) {
-        w.rh[q] = r;
-        w.p[q] = r;
-      } else {
-        w.p[q] = r + beta * (w.p[q] - omega * w.v[q]);
+      r[c] = R[c * NN + k0];
+      if (!s.restart) { pv[c] = P[c * NN + k0]; vv[c] = V[c * NN + k0]; }
+      if (two) {
+        r[3 + c] = R[c * NN + k1];
+        if (!s.restart) { pv[3 + c] = P[c * NN + k1]; vv[3 + c] = V[c * NN + k1]; }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !two) break;
+      const int64_t k = h ? k1 : k0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int q = 3 * h + c;
+        if (s.restart) {
+          RH[c * NN + k] = r[q];
+          P[c * NN + k] = r[q];
+        } else {
+          P[c * NN + k] = r[q] + beta * (pv[q] - omega * vv[q]);
+        }
       }
     }
   }
@@ -312,7 +335,7 @@ k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
 
 // s = r - alpha v, (s, s)
 template <class T>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
 k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned* ticket,
        const int32_t* __restrict__ blk) {
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
@@ -321,14 +344,30 @@ k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned*
   if (!s0.active) return;
   const int64_t NN = pk.n_nodes;
   const T alpha = (T)s0.alpha;
+  const T* __restrict__ R = w.r;
+  const T* __restrict__ V = w.v;
+  T* __restrict__ S = w.s;
   double v[1] = {0.0};
-  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+  for (int64_t k0 = fb.begin + threadIdx.x; k0 < fb.end; k0 += 2 * NT) {
+    const int64_t k1 = k0 + NT;
+    const bool two = k1 < fb.end;
+    T r[6], vv[6];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int64_t q = c * NN + k;
-      const T sv = w.r[q] - alpha * w.v[q];
-      w.s[q] = sv;
-      v[0] += (double)sv * (double)sv;
+      r[c] = R[c * NN + k0];
+      vv[c] = V[c * NN + k0];
+      if (two) { r[3 + c] = R[c * NN + k1]; vv[3 + c] = V[c * NN + k1]; }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !two) break;
+      const int64_t k = h ? k1 : k0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T sv = r[3 * h + c] - alpha * vv[3 * h + c];
+        S[c * NN + k] = sv;
+        v[0] += (double)sv * (double)sv;
+      }
     }
   }
   double tot[1];
@@ -367,8 +406,9 @@ k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
 }
 
 // x += alpha p + omega s; r = s - omega t; rho = (rh, r); (r, r)
+// (with a right preconditioner x moves along M^-1 p and M^-1 s)
 template <class T>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 3)
 k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double* partial,
        unsigned* ticket, const int32_t* __restrict__ blk) {
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
@@ -377,18 +417,42 @@ k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double*
   if (!s0.active) return;
   const int64_t NN = pk.n_nodes;
   const T alpha = (T)s0.alpha, omega = (T)s0.omega;
+  const T* __restrict__ PH = w.ph;
+  const T* __restrict__ SH = w.sh;
+  const T* __restrict__ S = w.s;
+  const T* __restrict__ Tt = w.t;
+  const T* __restrict__ RH = w.rh;
+  T* __restrict__ R = w.r;
   double v[3] = {0.0, 0.0, 0.0};
-  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+  for (int64_t k0 = fb.begin + threadIdx.x; k0 < fb.end; k0 += 2 * NT) {
+    const int64_t k1 = k0 + NT;
+    const bool two = k1 < fb.end;
+    T xv[6], ph[6], sh[6], sv[6], tv[6], rh[6];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int64_t q = c * NN + k;
-      x[q] = x[q] + alpha * w.ph[q] + omega * w.sh[q];
-      const T r = w.s[q] - omega * w.t[q];
-      w.r[q] = r;
-      const double rh = w.rh[q];
-      v[0] += rh * r;
-      v[1] += (double)r * r;
-      v[2] += rh * rh;
+      const int64_t q0 = c * NN + k0;
+      xv[c] = x[q0]; ph[c] = PH[q0]; sh[c] = SH[q0]; sv[c] = S[q0]; tv[c] = Tt[q0];
+      rh[c] = RH[q0];
+      if (two) {
+        const int64_t q1 = c * NN + k1;
+        xv[3 + c] = x[q1]; ph[3 + c] = PH[q1]; sh[3 + c] = SH[q1]; sv[3 + c] = S[q1];
+        tv[3 + c] = Tt[q1]; rh[3 + c] = RH[q1];
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !two) break;
+      const int64_t k = h ? k1 : k0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int q = 3 * h + c;
+        x[c * NN + k] = xv[q] + alpha * ph[q] + omega * sh[q];
+        const T r = sv[q] - omega * tv[q];
+        R[c * NN + k] = r;
+        v[0] += (double)rh[q] * r;
+        v[1] += (double)r * r;
+        v[2] += (double)rh[q] * rh[q];
+      }
     }
   }
   double tot[3];
