@@ -313,11 +313,15 @@ k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
   nbr_offsets(g, off);
   const int64_t NN = pk.n_nodes;
   double v[1] = {0.0};
+  const T* __restrict__ X = w.ph;
+  const T* __restrict__ RH = w.rh;
+  T* __restrict__ Vo = w.v;
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
     T y0, y1, y2;
-    spmv_node<DIM, true, T>(J, w.ph, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
-    w.v[k] = y0; w.v[NN + k] = y1; w.v[2 * NN + k] = y2;
-    v[0] += (double)w.rh[k] * y0 + (double)w.rh[NN + k] * y1 + (double)w.rh[2 * NN + k] * y2;
+    spmv_node<DIM, true, T>(J, X, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    const T h0 = RH[k], h1 = RH[NN + k], h2 = RH[2 * NN + k];
+    Vo[k] = y0; Vo[NN + k] = y1; Vo[2 * NN + k] = y2;
+    v[0] += (double)h0 * y0 + (double)h1 * y1 + (double)h2 * y2;
   }
   double tot[1];
   if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
@@ -391,11 +395,15 @@ k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
   nbr_offsets(g, off);
   const int64_t NN = pk.n_nodes;
   double v[2] = {0.0, 0.0};
+  const T* __restrict__ X = w.sh;
+  const T* __restrict__ S = w.s;
+  T* __restrict__ To = w.t;
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
     T y0, y1, y2;
-    spmv_node<DIM, true, T>(J, w.sh, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
-    w.t[k] = y0; w.t[NN + k] = y1; w.t[2 * NN + k] = y2;
-    v[0] += (double)y0 * w.s[k] + (double)y1 * w.s[NN + k] + (double)y2 * w.s[2 * NN + k];
+    spmv_node<DIM, true, T>(J, X, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    const T s0 = S[k], s1 = S[NN + k], s2 = S[2 * NN + k];
+    To[k] = y0; To[NN + k] = y1; To[2 * NN + k] = y2;
+    v[0] += (double)y0 * s0 + (double)y1 * s1 + (double)y2 * s2;
     v[1] += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
   }
   double tot[2];
