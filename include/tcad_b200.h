@@ -296,7 +296,10 @@ typedef struct tcad_newton_opts {
   int32_t density_scaling; /* 1: Krylov unknowns are (dpsi, dn/s_n, dp/s_p), s = max(n|p,
                               scale_floor) -- the quantities of the Newton update test */
   int32_t precond;       /* 0: node-block Jacobi; 1: + block ILU(0) right preconditioner on
-                            2D packs (FP64 Krylov; 3D packs use node-block Jacobi) */
+                            2D packs; 2: automatic -- ILU(0) for the instances of a 2D
+                            batch (n_inst > 1) and for any 2D instance whose
+                            node-block-Jacobi solve fails (solved again with it).
+                            FP64 Krylov only; 3D packs use node-block Jacobi */
   double eta_min;        /* forcing 1: tightest Krylov tolerance of a step (>= rtol) */
   double scale_floor;    /* density_scaling: floor of s (dens_floor when <= 0) */
   double polish_eta;     /* forcing 1: Krylov tolerance of the polishing steps (<= 0: the

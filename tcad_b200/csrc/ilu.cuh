@@ -145,15 +145,25 @@ k_ilu2d_factor(const tcad_pack_t pk, const double* __restrict__ J, double* __res
   }
 }
 
-// out = M^-1 rin for every instance still iterating (ks[inst].active).
+// out = M^-1 rin for every instance still iterating (ks[inst].active);
+// instances with mask[inst] == 0 are not preconditioned (out = rin).
 template <class T>
 __global__ void __launch_bounds__(kIluThreads)
 k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ Q,
-              const T* __restrict__ rin, T* __restrict__ out, const KState* ks) {
+              const T* __restrict__ rin, T* __restrict__ out, const KState* ks,
+              const uint8_t* __restrict__ mask) {
   const int inst = blockIdx.x;
   if (ks && !ks[inst].active) return;
   const Inst g = load_inst(pk, inst);
   const int64_t NN = pk.n_nodes;
+  if (mask && !mask[inst]) {
+    for (int64_t k = g.off + threadIdx.x; k < g.off + g.n; k += kIluThreads) {
+      out[k] = rin[k];
+      out[NN + k] = rin[NN + k];
+      out[2 * NN + k] = rin[2 * NN + k];
+    }
+    return;
+  }
   const int nx = g.nx, ny = g.ny;
   const int nd = nx + ny - 1;
   // forward: a_k = Q_k (r_k - G_k (B_kW a_W + B_kS a_S))

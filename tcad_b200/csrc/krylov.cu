@@ -875,17 +875,21 @@ struct WorkIlu {
   double* Q;
   double* ph;
   double* sh;
+  uint8_t* mask;    // instances preconditioned with ILU(0)
+  int32_t* pre;     // factor pre-status (-1: skip)
   size_t bytes;
 };
 
 static WorkIlu carve_ilu(const tcad_pack_t* pk, void* base) {
   Carve c{reinterpret_cast<char*>(base), 0, 0};
-  WorkIlu w{nullptr, nullptr, nullptr, 0};
+  WorkIlu w{nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   if (pk->dim != 2) return w;
   const size_t v3 = 3 * (size_t)pk->n_nodes;
   w.Q = c.take<double>(9 * (size_t)pk->n_nodes);
   w.ph = c.take<double>(v3);
   w.sh = c.take<double>(v3);
+  w.mask = c.take<uint8_t>(pk->n_inst);
+  w.pre = c.take<int32_t>(pk->n_inst);
   w.bytes = c.used;
   return w;
 }
@@ -925,7 +929,8 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
                              int maxiter, const BiVecT<T>& bi, const Work& w,
                              const int32_t* pre_status, std::vector<KState>& hks,
                              cudaStream_t s, const double* rtol_inst,
-                             const double* Jilu = nullptr, const double* Qilu = nullptr) {
+                             const double* Jilu = nullptr, const double* Qilu = nullptr,
+                             const uint8_t* ilu_mask = nullptr) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
@@ -959,7 +964,7 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
       note_launch();
       if (Qilu) {  // ph = M^-1 p (one CTA per instance)
         k_ilu2d_apply<T><<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, Jilu, Qilu, bi.p, bi.ph,
-                                                               w.ks);
+                                                               w.ks, ilu_mask);
         note_launch();
       }
       if (pk->dim == 2)
@@ -971,7 +976,7 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
       note_launch();
       if (Qilu) {  // sh = M^-1 s
         k_ilu2d_apply<T><<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, Jilu, Qilu, bi.s, bi.sh,
-                                                               w.ks);
+                                                               w.ks, ilu_mask);
         note_launch();
       }
       if (pk->dim == 2)
@@ -1046,7 +1051,7 @@ static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double*
     bi.ph = ilu->ph;
     bi.sh = ilu->sh;
     return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, bi, w, pre_status, hks, s,
-                                     rtol_inst, J, ilu->Q);
+                                     rtol_inst, J, ilu->Q, ilu->mask);
   }
   return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, w.bi, w, pre_status, hks, s,
                                    rtol_inst);
@@ -1235,7 +1240,7 @@ extern "C" int tcad_block_ilu_apply(const tcad_pack_t* pk, const double* J, cons
   if (!pack_ok(pk) || pk->dim != 2 || !J || !Q || !r || !out || r == out) return TCAD_ERR_ARG;
   if (pk->n_inst < 1) return TCAD_OK;
   k_ilu2d_apply<double><<<(unsigned)pk->n_inst, kIluThreads, 0, (cudaStream_t)stream>>>(
-      *pk, J, Q, r, out, nullptr);
+      *pk, J, Q, r, out, nullptr, nullptr);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1319,13 +1324,18 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   if (opts->precision == 32 && work_bytes < tcad_block_workspace_bytes(pk, 0, 0))
     return TCAD_ERR_ARG;
   const Work32 w32 = carve32(pk, reinterpret_cast<char*>(work) + ((w.bytes + 255) & ~(size_t)255));
-  // ILU(0) right preconditioner (2D): its region follows the FP32 extension
-  const bool use_ilu = opts->precond == 1 && pk->dim == 2;
+  // ILU(0) right preconditioner (2D): its region follows the FP32 extension.
+  // precond 1: every instance; 2 (automatic): the instances of a batch
+  // (more than one), and any instance whose node-block-Jacobi solve fails
+  const bool use_ilu = (opts->precond == 1 || opts->precond == 2) && pk->dim == 2;
+  std::vector<uint8_t> ilu_on(ni, 0);
+  if (use_ilu)
+    for (int i = 0; i < ni; ++i) ilu_on[i] = (opts->precond == 1 || ni > 1) ? 1 : 0;
   if (use_ilu && work_bytes < tcad_block_workspace_bytes(pk, 0, 0)) return TCAD_ERR_ARG;
   const WorkIlu wilu = use_ilu ? carve_ilu(pk, reinterpret_cast<char*>(work) +
                                                    ((w.bytes + 255) & ~(size_t)255) +
                                                    ((w32.bytes + 255) & ~(size_t)255))
-                               : WorkIlu{nullptr, nullptr, nullptr, 0};
+                               : WorkIlu{nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   std::vector<int32_t> mix_it(ni), mix_st(ni), mix_grew(ni, 0), mix_steps(ni, 0);
   std::vector<double> mix_rr(ni), mix_prev(ni, -1.0);
   std::vector<uint8_t> use64(ni, 0);  // precision 32: instances switched to FP64
@@ -1478,33 +1488,66 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       }
     }
     for (int i = 0; i < ni; ++i) { any64 = any64 || grp64[i]; }
-    if (any64) {
-      // FP64 BiCGStab for the FP64 group; the other instances stay idle
+    // FP64 BiCGStab for the FP64 group (the other instances stay idle); in
+    // automatic preconditioning an instance whose node-block-Jacobi solve
+    // failed is solved again with ILU(0) before its update is applied
+    std::vector<uint8_t> solve_set(grp64), done_set(ni, 0);
+    for (int pass = 0; pass < 2 && any64; ++pass) {
       std::vector<int32_t> st64(ni);
-      for (int i = 0; i < ni; ++i) st64[i] = grp64[i] ? hstat[i] : -1;
+      bool any_ilu = false;
+      for (int i = 0; i < ni; ++i) {
+        st64[i] = solve_set[i] ? hstat[i] : -1;
+        any_ilu = any_ilu || (solve_set[i] && ilu_on[i]);
+      }
       TCAD_CUDA_CHECK(cudaMemcpyAsync(w.status, st64.data(), sizeof(int32_t) * ni,
                                       cudaMemcpyHostToDevice, s));
-      if (use_ilu) {  // factor once per Newton step, for the FP64 group
-        k_ilu2d_factor<<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, J, wilu.Q, w.status, nullptr);
+      if (any_ilu) {  // factor the ILU instances of this solve
+        std::vector<int32_t> pre(ni);
+        std::vector<uint8_t> msk(ni);
+        for (int i = 0; i < ni; ++i) {
+          msk[i] = (solve_set[i] && ilu_on[i]) ? 1 : 0;
+          pre[i] = msk[i] ? st64[i] : -1;
+        }
+        TCAD_CUDA_CHECK(cudaMemcpyAsync(wilu.pre, pre.data(), sizeof(int32_t) * ni,
+                                        cudaMemcpyHostToDevice, s));
+        TCAD_CUDA_CHECK(cudaMemcpyAsync(wilu.mask, msk.data(), ni, cudaMemcpyHostToDevice, s));
+        k_ilu2d_factor<<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, J, wilu.Q, wilu.pre, nullptr);
         note_launch();
         TCAD_LAUNCH_CHECK();
       }
       rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
-                           w.eta, use_ilu ? &wilu : nullptr);
+                           w.eta, any_ilu ? &wilu : nullptr);
       if (rc != TCAD_OK) return rc;
-      // instances whose linear solve broke down / diverged keep their state
+      std::vector<uint8_t> apply(ni, 0), retry(ni, 0);
+      bool any_retry = false;
       for (int i = 0; i < ni; ++i) {
-        if (!grp64[i]) continue;
+        if (!solve_set[i]) continue;
         last_kit[i] = hks[i].it;
         result[i].krylov_iters += hks[i].it;
         result[i].status = hks[i].status;
         result[i].relres = hks[i].bb > 0.0 ? std::sqrt(hks[i].rr / hks[i].bb) : 0.0;
+        const bool failed = hks[i].status == TCAD_ERR_NOCONV ||
+                            hks[i].status == TCAD_ERR_BREAKDOWN;
+        if (pass == 0 && failed && opts->precond == 2 && use_ilu && !ilu_on[i]) {
+          ilu_on[i] = 1;  // from now on this instance is ILU-preconditioned
+          retry[i] = 1;
+          any_retry = true;
+          if (opts->verbose)
+            std::fprintf(stderr, "    [gpu] inst %d it %2d  block-Jacobi solve failed (st=%d)"
+                                 " -> ILU(0)\n", i, it, hks[i].status);
+        } else {
+          apply[i] = 1;  // instances whose solve broke down keep the partial step
+        }
       }
-      TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp64.data(), ni, cudaMemcpyHostToDevice, s));
+      // apply this pass's accepted steps (the retried ones are solved again;
+      // their du is overwritten by the next pass)
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(active, apply.data(), ni, cudaMemcpyHostToDevice, s));
       k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
                                         active, w.err, opts->density_scaling, 0, sfloor);
       note_launch();
       TCAD_LAUNCH_CHECK();
+      if (!any_retry) break;
+      solve_set = retry;
     }
     TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
                                     cudaMemcpyDeviceToHost, s));
