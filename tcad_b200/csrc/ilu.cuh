@@ -166,6 +166,116 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
   }
   const int nx = g.nx, ny = g.ny;
   const int nd = nx + ny - 1;
+  // Fast path when every anti-diagonal fits the block (min(nx, ny) <=
+  // threads): thread t owns the t-th node of each level, the previous
+  // level's results sit in a shared-memory front indexed by row (j, or i
+  // when nx < ny), and the next level's node data is loaded into registers
+  // before the level barrier, so only the dependent arithmetic is serial.
+  const bool byj = ny <= nx;
+  if ((byj ? ny : nx) <= kIluThreads) {
+    __shared__ double fr[2][kIluThreads][3];
+    const int t = threadIdx.x;
+    int i = 0, j = 0;
+    bool have = false;
+    double G[9], Qk[9], b1[5], b2[5], r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    // node of thread t on level d (false when the level is shorter)
+    auto node_of = [&](int d) -> bool {
+      if (d < 0 || d >= nd) return false;
+      if (byj) {
+        const int jlo = d - (nx - 1) > 0 ? d - (nx - 1) : 0;
+        const int jhi = d < ny - 1 ? d : ny - 1;
+        j = jlo + t;
+        i = d - j;
+        return j <= jhi;
+      }
+      const int ilo = d - (ny - 1) > 0 ? d - (ny - 1) : 0;
+      const int ihi = d < nx - 1 ? d : nx - 1;
+      i = ilo + t;
+      j = d - i;
+      return i <= ihi;
+    };
+    // ---- forward: a_k = Q_k (r_k - G_k (B_kW a_W + B_kS a_S))
+    auto load_fwd = [&](int d) {
+      have = node_of(d);
+      if (!have) return;
+      const int64_t k = g.off + (int64_t)j * nx + i;
+      load9(J, NN, k, 0, G);
+      load9(Q, NN, k, 0, Qk);
+      if (i > 0) load_nb(J, NN, k, 0, b1);
+      if (j > 0) load_nb(J, NN, k, 2, b2);
+      r0 = rin[k]; r1 = rin[NN + k]; r2 = rin[2 * NN + k];
+    };
+    int cur = 0;
+    load_fwd(0);
+    for (int d = 0; d < nd; ++d) {
+      if (have) {
+        const int pv = cur ^ 1;
+        double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+        if (i > 0) {
+          const double* f = fr[pv][byj ? j : i - 1];
+          add_nb_vec(b1, f[0], f[1], f[2], u0, u1, u2);
+        }
+        if (j > 0) {
+          const double* f = fr[pv][byj ? j - 1 : i];
+          add_nb_vec(b2, f[0], f[1], f[2], u0, u1, u2);
+        }
+        const double t0 = r0 - (G[0] * u0 + G[1] * u1 + G[2] * u2);
+        const double t1 = r1 - (G[3] * u0 + G[4] * u1 + G[5] * u2);
+        const double t2 = r2 - (G[6] * u0 + G[7] * u1 + G[8] * u2);
+        const double a0 = Qk[0] * t0 + Qk[1] * t1 + Qk[2] * t2;
+        const double a1 = Qk[3] * t0 + Qk[4] * t1 + Qk[5] * t2;
+        const double a2 = Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2;
+        double* w = fr[cur][byj ? j : i];
+        w[0] = a0; w[1] = a1; w[2] = a2;
+        const int64_t k = g.off + (int64_t)j * nx + i;
+        out[k] = (T)a0; out[NN + k] = (T)a1; out[2 * NN + k] = (T)a2;
+      }
+      load_fwd(d + 1);
+      __syncthreads();
+      cur ^= 1;
+    }
+    // ---- backward: x_k = a_k - Q_k G_k (B_kE x_E + B_kN x_N)
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    auto load_bwd = [&](int d) {
+      have = node_of(d);
+      if (!have) return;
+      const int64_t k = g.off + (int64_t)j * nx + i;
+      load9(J, NN, k, 0, G);
+      load9(Q, NN, k, 0, Qk);
+      if (i < nx - 1) load_nb(J, NN, k, 1, b1);
+      if (j < ny - 1) load_nb(J, NN, k, 3, b2);
+      a0 = out[k]; a1 = out[NN + k]; a2 = out[2 * NN + k];
+    };
+    load_bwd(nd - 1);
+    for (int d = nd - 1; d >= 0; --d) {
+      if (have) {
+        const int pv = cur ^ 1;
+        double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+        if (i < nx - 1) {
+          const double* f = fr[pv][byj ? j : i + 1];
+          add_nb_vec(b1, f[0], f[1], f[2], u0, u1, u2);
+        }
+        if (j < ny - 1) {
+          const double* f = fr[pv][byj ? j + 1 : i];
+          add_nb_vec(b2, f[0], f[1], f[2], u0, u1, u2);
+        }
+        const double t0 = G[0] * u0 + G[1] * u1 + G[2] * u2;
+        const double t1 = G[3] * u0 + G[4] * u1 + G[5] * u2;
+        const double t2 = G[6] * u0 + G[7] * u1 + G[8] * u2;
+        const double x0 = a0 - (Qk[0] * t0 + Qk[1] * t1 + Qk[2] * t2);
+        const double x1 = a1 - (Qk[3] * t0 + Qk[4] * t1 + Qk[5] * t2);
+        const double x2 = a2 - (Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2);
+        double* w = fr[cur][byj ? j : i];
+        w[0] = x0; w[1] = x1; w[2] = x2;
+        const int64_t k = g.off + (int64_t)j * nx + i;
+        out[k] = (T)x0; out[NN + k] = (T)x1; out[2 * NN + k] = (T)x2;
+      }
+      load_bwd(d - 1);
+      __syncthreads();
+      cur ^= 1;
+    }
+    return;
+  }
   // forward: a_k = Q_k (r_k - G_k (B_kW a_W + B_kS a_S))
   for (int d = 0; d < nd; ++d) {
     const int jlo = d - (nx - 1) > 0 ? d - (nx - 1) : 0;

@@ -94,6 +94,69 @@ def test_ilu_factor_and_apply_match_host():
     assert np.abs(w - rh).max() <= 1e-9 * np.abs(rh).max()
 
 
+def _apply_M_host(Jh, Qg, x, nx, ny):
+    """M x = (D~ + L^) D~^-1 (D~ + U^) x, vectorised over nodes (x: [N, 3])."""
+    N = nx * ny
+    G = Jh[0:9].T.reshape(N, 3, 3)
+    Q = Qg.T.reshape(N, 3, 3)
+    Dt = np.linalg.inv(Q)
+
+    def nbmat(d):
+        b = Jh[9 + 5 * d: 14 + 5 * d].T
+        B = np.zeros((N, 3, 3))
+        B[:, 0, 0], B[:, 1, 0], B[:, 1, 1], B[:, 2, 0], B[:, 2, 2] = b.T
+        return B
+
+    idx = np.arange(N).reshape(ny, nx)
+    def shift(v, di, dj):       # value of node (i+di, j+dj), zero outside
+        out = np.zeros_like(v)
+        vv = v.reshape(ny, nx, 3)
+        oo = out.reshape(ny, nx, 3)
+        oo[max(0, -dj):ny - max(0, dj), max(0, -di):nx - max(0, di)] = \
+            vv[max(0, dj):ny - max(0, -dj), max(0, di):nx - max(0, -di)]
+        return out
+    mv = lambda A, v: np.einsum("nij,nj->ni", A, v)  # noqa: E731
+    u = mv(Dt, x) + mv(G, mv(nbmat(1), shift(x, 1, 0)) + mv(nbmat(3), shift(x, 0, 1)))
+    v = mv(Q, u)
+    return mv(Dt, v) + mv(G, mv(nbmat(0), shift(v, -1, 0)) + mv(nbmat(2), shift(v, 0, -1)))
+
+
+@pytest.mark.parametrize("shape", [(64, 40), (300, 270)])
+def test_ilu_apply_inverts_M(shape):
+    """M (M^-1 r) = r on a MOSFET at a biased Newton state; (300, 270) has
+    anti-diagonals longer than a block (the general sweep), (64, 40) the
+    register-pipelined one."""
+    import torch
+    import tcad_b200 as tb
+    from tcad_b200 import _lib, workloads as W
+    dev = W.mosfet2d(tb.Device2D, *shape, Lg=60e-7)
+    dev.solve_equilibrium()
+    dev._apply_voltages({"gate": 0.6, "drain": 0.4})
+    pk = dev.pack
+    pk.set_bias()
+    pk.stamp_contacts()
+    pk.assemble(_lib.MODE_ELIMINATE)
+    st = torch.zeros(1, dtype=torch.int32, device=pk.device)
+    sp = _lib.stream_ptr()
+    assert pk.lib.tcad_block_jacobi_setup_rel(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F),
+                                              _lib.ptr(st), _lib.ptr(pk.n), _lib.ptr(pk.p),
+                                              1e-10, sp) == 0
+    N = pk.N
+    Q = torch.zeros(9 * N, dtype=torch.float64, device=pk.device)
+    assert pk.lib.tcad_block_ilu_setup(pk.pref, _lib.ptr(pk.J), _lib.ptr(Q), _lib.ptr(st),
+                                       sp) == 0
+    assert int(st.item()) == 0
+    r = torch.randn(3 * N, dtype=torch.float64, device=pk.device)
+    out = torch.zeros_like(r)
+    assert pk.lib.tcad_block_ilu_apply(pk.pref, _lib.ptr(pk.J), _lib.ptr(Q), _lib.ptr(r),
+                                       _lib.ptr(out), sp) == 0
+    Jh = pk.J.cpu().numpy().reshape(-1, N)
+    x = out.cpu().numpy().reshape(3, N).T
+    w = _apply_M_host(Jh, Q.cpu().numpy().reshape(9, N), x, *shape)
+    rh = r.cpu().numpy().reshape(3, N).T
+    assert np.abs(w - rh).max() <= 1e-8 * np.abs(rh).max()
+
+
 def test_ilu_newton_sweep_parity_and_fewer_iterations():
     import tcad_b200 as tb
     g = fx.load("mosfet_small")
