@@ -84,7 +84,7 @@ class NewtonOptions:
     # GPU-only: Krylov tolerance of the polishing steps.  Low-bias currents
     # are small differences of large drift and diffusion fluxes, so the
     # state after the last step must be accurate well beyond the update test.
-    polish_eta: float = 1e-6
+    polish_eta: float = 1e-10
     # GPU-only: inexact-Newton forcing.  "adaptive" solves step k to
     # eta_k = clamp(0.1 * update_{k-1}, linsolve_rtol, eta_max) (quadratic
     # convergence is kept; the converged state is the same); "fixed" solves
