@@ -1,5 +1,8 @@
 // Block ILU(0) of the node-block-scaled 2D operator, as a right
-// preconditioner of the BiCGStab in krylov.cu.
+// preconditioner of the BiCGStab in krylov.cu.  On 3D packs the same
+// factorisation is taken plane by plane (the in-plane W/E/S/N couplings of
+// each z-plane; the D/U couplings are left to the Krylov iteration): a
+// block-diagonal-over-planes preconditioner, one CTA per (instance, plane).
 //
 // The scaled operator is A^ = I + G_k sum_d B_kd (node k, neighbours
 // d = W, E, S, N): G_k is the (row-scaled) inverse diagonal block stored in
@@ -74,10 +77,13 @@ __device__ __forceinline__ void add_nb_vec(const double* b, double v0, double v1
 // status[inst] = TCAD_ERR_SINGULAR when a D~ block is singular.
 __global__ void __launch_bounds__(kIluThreads)
 k_ilu2d_factor(const tcad_pack_t pk, const double* __restrict__ J, double* __restrict__ Q,
-               const int32_t* __restrict__ pre_status, int32_t* __restrict__ status) {
-  const int inst = blockIdx.x;
+               const int32_t* __restrict__ pre_status, int32_t* __restrict__ status,
+               int nzmax) {
+  const int inst = blockIdx.x / nzmax, z = blockIdx.x % nzmax;
   if (pre_status && pre_status[inst] != TCAD_OK) return;
   const Inst g = load_inst(pk, inst);
+  if (z >= g.nz) return;
+  const int64_t base = g.off + (int64_t)z * g.nx * g.ny;  // this z-plane (2D: the instance)
   const int64_t NN = pk.n_nodes;
   const int nx = g.nx, ny = g.ny;
   for (int d = 0; d < nx + ny - 1; ++d) {
@@ -85,7 +91,7 @@ k_ilu2d_factor(const tcad_pack_t pk, const double* __restrict__ J, double* __res
     const int jhi = d < ny - 1 ? d : ny - 1;
     for (int j = jlo + threadIdx.x; j <= jhi; j += kIluThreads) {
       const int i = d - j;
-      const int64_t k = g.off + (int64_t)j * nx + i;
+      const int64_t k = base + (int64_t)j * nx + i;
       double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       double b[5], G[9], Qm[9], T1[9], T2[9], T3[9];
       if (i > 0) {  // W: term B_kW Q_W G_W B_WE
@@ -151,13 +157,16 @@ template <class T>
 __global__ void __launch_bounds__(kIluThreads)
 k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ Q,
               const T* __restrict__ rin, T* __restrict__ out, const KState* ks,
-              const uint8_t* __restrict__ mask) {
-  const int inst = blockIdx.x;
+              const uint8_t* __restrict__ mask, int nzmax) {
+  const int inst = blockIdx.x / nzmax, z = blockIdx.x % nzmax;
   if (ks && !ks[inst].active) return;
   const Inst g = load_inst(pk, inst);
+  if (z >= g.nz) return;
+  const int64_t base = g.off + (int64_t)z * g.nx * g.ny;  // this z-plane (2D: the instance)
   const int64_t NN = pk.n_nodes;
   if (mask && !mask[inst]) {
-    for (int64_t k = g.off + threadIdx.x; k < g.off + g.n; k += kIluThreads) {
+    const int64_t end = base + (int64_t)g.nx * g.ny;
+    for (int64_t k = base + threadIdx.x; k < end; k += kIluThreads) {
       out[k] = rin[k];
       out[NN + k] = rin[NN + k];
       out[2 * NN + k] = rin[2 * NN + k];
@@ -198,7 +207,7 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
     auto load_fwd = [&](int d) {
       have = node_of(d);
       if (!have) return;
-      const int64_t k = g.off + (int64_t)j * nx + i;
+      const int64_t k = base + (int64_t)j * nx + i;
       load9(J, NN, k, 0, G);
       load9(Q, NN, k, 0, Qk);
       if (i > 0) load_nb(J, NN, k, 0, b1);
@@ -227,7 +236,7 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
         const double a2 = Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2;
         double* w = fr[cur][byj ? j : i];
         w[0] = a0; w[1] = a1; w[2] = a2;
-        const int64_t k = g.off + (int64_t)j * nx + i;
+        const int64_t k = base + (int64_t)j * nx + i;
         out[k] = (T)a0; out[NN + k] = (T)a1; out[2 * NN + k] = (T)a2;
       }
       load_fwd(d + 1);
@@ -239,7 +248,7 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
     auto load_bwd = [&](int d) {
       have = node_of(d);
       if (!have) return;
-      const int64_t k = g.off + (int64_t)j * nx + i;
+      const int64_t k = base + (int64_t)j * nx + i;
       load9(J, NN, k, 0, G);
       load9(Q, NN, k, 0, Qk);
       if (i < nx - 1) load_nb(J, NN, k, 1, b1);
@@ -267,7 +276,7 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
         const double x2 = a2 - (Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2);
         double* w = fr[cur][byj ? j : i];
         w[0] = x0; w[1] = x1; w[2] = x2;
-        const int64_t k = g.off + (int64_t)j * nx + i;
+        const int64_t k = base + (int64_t)j * nx + i;
         out[k] = (T)x0; out[NN + k] = (T)x1; out[2 * NN + k] = (T)x2;
       }
       load_bwd(d - 1);
@@ -282,7 +291,7 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
     const int jhi = d < ny - 1 ? d : ny - 1;
     for (int j = jlo + threadIdx.x; j <= jhi; j += kIluThreads) {
       const int i = d - j;
-      const int64_t k = g.off + (int64_t)j * nx + i;
+      const int64_t k = base + (int64_t)j * nx + i;
       double u0 = 0.0, u1 = 0.0, u2 = 0.0, b[5];
       if (i > 0) {
         load_nb(J, NN, k, 0, b);
@@ -310,7 +319,7 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
     const int jhi = d < ny - 1 ? d : ny - 1;
     for (int j = jlo + threadIdx.x; j <= jhi; j += kIluThreads) {
       const int i = d - j;
-      const int64_t k = g.off + (int64_t)j * nx + i;
+      const int64_t k = base + (int64_t)j * nx + i;
       double u0 = 0.0, u1 = 0.0, u2 = 0.0, b[5];
       if (i < nx - 1) {
         load_nb(J, NN, k, 1, b);

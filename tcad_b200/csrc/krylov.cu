@@ -870,7 +870,7 @@ static Work32 carve32(const tcad_pack_t* pk, void* base) {
   return w;
 }
 
-// ILU(0) extension (2D packs): Q = D~^-1 per node, M^-1 p and M^-1 s
+// ILU(0) extension: Q = D~^-1 per node, M^-1 p and M^-1 s
 struct WorkIlu {
   double* Q;
   double* ph;
@@ -883,7 +883,6 @@ struct WorkIlu {
 static WorkIlu carve_ilu(const tcad_pack_t* pk, void* base) {
   Carve c{reinterpret_cast<char*>(base), 0, 0};
   WorkIlu w{nullptr, nullptr, nullptr, nullptr, nullptr, 0};
-  if (pk->dim != 2) return w;
   const size_t v3 = 3 * (size_t)pk->n_nodes;
   w.Q = c.take<double>(9 * (size_t)pk->n_nodes);
   w.ph = c.take<double>(v3);
@@ -930,7 +929,7 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
                              const int32_t* pre_status, std::vector<KState>& hks,
                              cudaStream_t s, const double* rtol_inst,
                              const double* Jilu = nullptr, const double* Qilu = nullptr,
-                             const uint8_t* ilu_mask = nullptr) {
+                             const uint8_t* ilu_mask = nullptr, int nzmax = 1) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
@@ -963,8 +962,8 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
       k_bi_p<<<ng, NT, 0, s>>>(*pk, bi, w.ks, dlist);
       note_launch();
       if (Qilu) {  // ph = M^-1 p (one CTA per instance)
-        k_ilu2d_apply<T><<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, Jilu, Qilu, bi.p, bi.ph,
-                                                               w.ks, ilu_mask);
+        k_ilu2d_apply<T><<<(unsigned)(ni * nzmax), kIluThreads, 0, s>>>(
+            *pk, Jilu, Qilu, bi.p, bi.ph, w.ks, ilu_mask, nzmax);
         note_launch();
       }
       if (pk->dim == 2)
@@ -975,8 +974,8 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
       k_bi_s<<<ng, NT, 0, s>>>(*pk, bi, w.ks, w.partial, w.ticket, dlist);
       note_launch();
       if (Qilu) {  // sh = M^-1 s
-        k_ilu2d_apply<T><<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, Jilu, Qilu, bi.s, bi.sh,
-                                                               w.ks, ilu_mask);
+        k_ilu2d_apply<T><<<(unsigned)(ni * nzmax), kIluThreads, 0, s>>>(
+            *pk, Jilu, Qilu, bi.s, bi.sh, w.ks, ilu_mask, nzmax);
         note_launch();
       }
       if (pk->dim == 2)
@@ -1045,13 +1044,13 @@ static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double*
                            double* x, double rtol, int maxiter, const Work& w,
                            const int32_t* pre_status, std::vector<KState>& hks,
                            cudaStream_t s, const double* rtol_inst = nullptr,
-                           const WorkIlu* ilu = nullptr) {
+                           const WorkIlu* ilu = nullptr, int nzmax = 1) {
   if (ilu && ilu->Q) {
     BiVec bi = w.bi;
     bi.ph = ilu->ph;
     bi.sh = ilu->sh;
     return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, bi, w, pre_status, hks, s,
-                                     rtol_inst, J, ilu->Q, ilu->mask);
+                                     rtol_inst, J, ilu->Q, ilu->mask, nzmax);
   }
   return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, w.bi, w, pre_status, hks, s,
                                    rtol_inst);
@@ -1220,16 +1219,31 @@ extern "C" int tcad_block_jacobi_setup_rel(const tcad_pack_t* pk, double* J, dou
 }
 
 extern "C" size_t tcad_block_ilu_bytes(const tcad_pack_t* pk) {
-  if (!pack_ok(pk) || pk->dim != 2) return 0;
+  if (!pack_ok(pk)) return 0;
   return 9 * sizeof(double) * (size_t)pk->n_nodes;
+}
+
+// largest Nz of the pack's instances (host read of the shape table)
+static int pack_nzmax(const tcad_pack_t* pk, cudaStream_t s) {
+  if (pk->dim == 2 || pk->n_inst < 1) return 1;
+  std::vector<int32_t> shp(3 * (size_t)pk->n_inst);
+  if (cudaMemcpyAsync(shp.data(), pk->shape, sizeof(int32_t) * shp.size(),
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return -1;
+  int m = 1;
+  for (int i = 0; i < pk->n_inst; ++i) m = std::max(m, (int)shp[3 * i + 2]);
+  return m;
 }
 
 extern "C" int tcad_block_ilu_setup(const tcad_pack_t* pk, const double* J, double* Q,
                                     int32_t* status, void* stream) {
-  if (!pack_ok(pk) || pk->dim != 2 || !J || !Q || !status) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || !J || !Q || !status) return TCAD_ERR_ARG;
   if (pk->n_inst < 1) return TCAD_OK;
-  k_ilu2d_factor<<<(unsigned)pk->n_inst, kIluThreads, 0, (cudaStream_t)stream>>>(
-      *pk, J, Q, nullptr, status);
+  const int nzm = pack_nzmax(pk, (cudaStream_t)stream);
+  if (nzm < 1) return TCAD_ERR_CUDA;
+  k_ilu2d_factor<<<(unsigned)(pk->n_inst * nzm), kIluThreads, 0, (cudaStream_t)stream>>>(
+      *pk, J, Q, nullptr, status, nzm);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1237,10 +1251,12 @@ extern "C" int tcad_block_ilu_setup(const tcad_pack_t* pk, const double* J, doub
 
 extern "C" int tcad_block_ilu_apply(const tcad_pack_t* pk, const double* J, const double* Q,
                                     const double* r, double* out, void* stream) {
-  if (!pack_ok(pk) || pk->dim != 2 || !J || !Q || !r || !out || r == out) return TCAD_ERR_ARG;
+  if (!pack_ok(pk) || !J || !Q || !r || !out || r == out) return TCAD_ERR_ARG;
   if (pk->n_inst < 1) return TCAD_OK;
-  k_ilu2d_apply<double><<<(unsigned)pk->n_inst, kIluThreads, 0, (cudaStream_t)stream>>>(
-      *pk, J, Q, r, out, nullptr, nullptr);
+  const int nzm = pack_nzmax(pk, (cudaStream_t)stream);
+  if (nzm < 1) return TCAD_ERR_CUDA;
+  k_ilu2d_apply<double><<<(unsigned)(pk->n_inst * nzm), kIluThreads, 0,
+                          (cudaStream_t)stream>>>(*pk, J, Q, r, out, nullptr, nullptr, nzm);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1327,8 +1343,10 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   // ILU(0) right preconditioner (2D): its region follows the FP32 extension.
   // precond 1: every instance; 2 (automatic): the instances of a batch
   // (more than one), and any instance whose node-block-Jacobi solve fails
-  const bool use_ilu = (opts->precond == 1 || opts->precond == 2) && pk->dim == 2;
+  const bool use_ilu = opts->precond == 1 || (opts->precond == 2 && pk->dim == 2);
   std::vector<uint8_t> ilu_on(ni, 0);
+  const int nzmax = use_ilu ? pack_nzmax(pk, s) : 1;
+  if (nzmax < 1) return TCAD_ERR_CUDA;
   if (use_ilu)
     for (int i = 0; i < ni; ++i) ilu_on[i] = (opts->precond == 1 || ni > 1) ? 1 : 0;
   if (use_ilu && work_bytes < tcad_block_workspace_bytes(pk, 0, 0)) return TCAD_ERR_ARG;
@@ -1511,12 +1529,13 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
         TCAD_CUDA_CHECK(cudaMemcpyAsync(wilu.pre, pre.data(), sizeof(int32_t) * ni,
                                         cudaMemcpyHostToDevice, s));
         TCAD_CUDA_CHECK(cudaMemcpyAsync(wilu.mask, msk.data(), ni, cudaMemcpyHostToDevice, s));
-        k_ilu2d_factor<<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, J, wilu.Q, wilu.pre, nullptr);
+        k_ilu2d_factor<<<(unsigned)(ni * nzmax), kIluThreads, 0, s>>>(*pk, J, wilu.Q, wilu.pre,
+                                                                       nullptr, nzmax);
         note_launch();
         TCAD_LAUNCH_CHECK();
       }
       rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
-                           w.eta, any_ilu ? &wilu : nullptr);
+                           w.eta, any_ilu ? &wilu : nullptr, nzmax);
       if (rc != TCAD_OK) return rc;
       std::vector<uint8_t> apply(ni, 0), retry(ni, 0);
       bool any_retry = false;

@@ -669,9 +669,9 @@ class Pack:
         o.eta_min = float(em)
         o.scale_floor = float(getattr(opts, "krylov_scale_floor", 1e-10))
         pc = getattr(opts, "precond", "auto")
-        # "ilu": ILU(0) everywhere (2D); "auto"/"schur": ILU(0) for batches and
-        # for any instance whose node-block-Jacobi solve fails; 3D packs keep
-        # node-block Jacobi
+        # "ilu": ILU(0) everywhere (3D: per z-plane); "auto"/"schur": on 2D
+        # packs ILU(0) for batches and for any instance whose node-block-Jacobi
+        # solve fails, 3D packs keep node-block Jacobi
         o.precond = {"ilu": 1, "auto": 2, "schur": 2}.get(pc, 0)
         o.polish_eta = float(getattr(opts, "polish_eta", 1e-10))
         return o

@@ -44,13 +44,13 @@ def bytes_per_node(dim):
     """HBM bytes one resident node costs: coefficients, BC arrays, state, F,
     the node-block Jacobian, the Newton update and the Krylov workspace
     (FP64 BiCGStab vectors and the FP32 extension of the mixed-precision
-    path), the ILU(0) preconditioner of 2D packs, and the previous state the
+    path), the ILU(0) preconditioner, and the previous state the
     sweep predictor extrapolates from."""
     ne = _lib.NE[dim]
     doubles = len(NODE_ARRAYS) + 3 * dim + len(BC_ARRAYS) + 3 + 3 + 3 + ne + 3
     work64 = 6 * 3 * 8 + 4 * 8 / 256
     work32 = 6 * 3 * 4 + ne * 4 + 2 * 3 * 4
-    ilu = (9 + 6) * 8 if dim == 2 else 0     # ILU(0) factor and two vectors (2D)
+    ilu = (9 + 6) * 8                        # ILU(0) factor and two vectors
     return int(np.ceil(doubles * 8 + 1 + work64 + work32 + ilu))
 
 

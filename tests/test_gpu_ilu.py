@@ -174,3 +174,57 @@ def test_ilu_newton_sweep_parity_and_fewer_iterations():
         assert fx.current_err(I, g) < 1e-6, pc
         res[pc] = kr
     assert res["ilu"] < res["block_jacobi"]
+
+
+def test_ilu_3d_planes_invert_their_blocks():
+    """On a 3D pack ILU(0) is taken per z-plane (in-plane couplings): M is
+    block-diagonal over planes and M (M^-1 r) = r holds plane by plane."""
+    import torch
+    import tcad_b200 as tb
+    from tcad_b200 import _lib, workloads as W
+    dev = W.trigate3d(tb.Device3D, 24, 16, 12)
+    dev.solve_equilibrium()
+    dev._apply_voltages(W.trigate_bias(0.3, 0.5))
+    pk = dev.pack
+    pk.set_bias()
+    pk.stamp_contacts()
+    pk.assemble(_lib.MODE_ELIMINATE)
+    st = torch.zeros(1, dtype=torch.int32, device=pk.device)
+    sp = _lib.stream_ptr()
+    assert pk.lib.tcad_block_jacobi_setup_rel(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F),
+                                              _lib.ptr(st), _lib.ptr(pk.n), _lib.ptr(pk.p),
+                                              1e-10, sp) == 0
+    N = pk.N
+    Q = torch.zeros(9 * N, dtype=torch.float64, device=pk.device)
+    assert pk.lib.tcad_block_ilu_setup(pk.pref, _lib.ptr(pk.J), _lib.ptr(Q), _lib.ptr(st),
+                                       sp) == 0
+    assert int(st.item()) == 0
+    r = torch.randn(3 * N, dtype=torch.float64, device=pk.device)
+    out = torch.zeros_like(r)
+    assert pk.lib.tcad_block_ilu_apply(pk.pref, _lib.ptr(pk.J), _lib.ptr(Q), _lib.ptr(r),
+                                       _lib.ptr(out), sp) == 0
+    nx, ny, nz = dev.setup.nax
+    Jh = pk.J.cpu().numpy().reshape(-1, N)
+    Qh = Q.cpu().numpy().reshape(9, N)
+    x = out.cpu().numpy().reshape(3, N).T
+    rh = r.cpu().numpy().reshape(3, N).T
+    P = nx * ny
+    for z in range(nz):
+        sl = slice(z * P, (z + 1) * P)
+        w = _apply_M_host(Jh[:, sl], Qh[:, sl], x[sl], nx, ny)
+        assert np.abs(w - rh[sl]).max() <= 1e-8 * np.abs(rh).max(), z
+
+
+def test_ilu_3d_newton_sweep_parity():
+    import tcad_b200 as tb
+    g = fx.load("trigate_small")
+    dev = fx.gpu_device(g)
+    dev.solve_equilibrium()
+    opts = tb.NewtonOptions(precond="ilu")
+    gates = [b for b in dev.bcs if b.startswith("gate")]
+    I = []
+    for v in g["Vg"]:
+        dev.solve_bias({"drain": float(g["Vd"]), **{gt: float(v) for gt in gates}}, opts)
+        assert dev.last_converged
+        I.append(dev.terminal_current("drain"))
+    assert fx.current_err(I, g) < 1e-6
