@@ -176,110 +176,106 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
   const int nx = g.nx, ny = g.ny;
   const int nd = nx + ny - 1;
   // Fast path when every anti-diagonal fits the block (min(nx, ny) <=
-  // threads): thread t owns the t-th node of each level, the previous
-  // level's results sit in a shared-memory front indexed by row (j, or i
-  // when nx < ny), and the next level's node data is loaded into registers
-  // before the level barrier, so only the dependent arithmetic is serial.
+  // threads).  Thread c owns one row of the shorter dimension (j, or i when
+  // nx < ny) and walks along it, one node per anti-diagonal level: the
+  // previous node of its own row is in a register, the other lower
+  // neighbour (row c-1, same position) comes from a shared-memory front,
+  // and the node data of the next two positions of its row is already in
+  // flight, so each level costs only the dependent arithmetic and a barrier.
   const bool byj = ny <= nx;
-  if ((byj ? ny : nx) <= kIluThreads) {
+  const int Lc = byj ? ny : nx, Lw = byj ? nx : ny;
+  if (Lc <= kIluThreads) {
     __shared__ double fr[2][kIluThreads][3];
-    const int t = threadIdx.x;
-    int i = 0, j = 0;
-    bool have = false;
-    double G[9], Qk[9], b1[5], b2[5], r0 = 0.0, r1 = 0.0, r2 = 0.0;
-    // node of thread t on level d (false when the level is shorter)
-    auto node_of = [&](int d) -> bool {
-      if (d < 0 || d >= nd) return false;
-      if (byj) {
-        const int jlo = d - (nx - 1) > 0 ? d - (nx - 1) : 0;
-        const int jhi = d < ny - 1 ? d : ny - 1;
-        j = jlo + t;
-        i = d - j;
-        return j <= jhi;
-      }
-      const int ilo = d - (ny - 1) > 0 ? d - (ny - 1) : 0;
-      const int ihi = d < nx - 1 ? d : nx - 1;
-      i = ilo + t;
-      j = d - i;
-      return i <= ihi;
+    const int c = threadIdx.x;
+    const bool lane = c < Lc;
+    // neighbour directions: along the row (walk) and across rows (cross)
+    const int dwp = byj ? 0 : 2, dcp = byj ? 2 : 0;   // forward: W/S
+    const int dwn = byj ? 1 : 3, dcn = byj ? 3 : 1;   // backward: E/N
+    auto node = [&](int w) -> int64_t {
+      return byj ? base + (int64_t)c * nx + w : base + (int64_t)w * nx + c;
     };
-    // ---- forward: a_k = Q_k (r_k - G_k (B_kW a_W + B_kS a_S))
-    auto load_fwd = [&](int d) {
-      have = node_of(d);
-      if (!have) return;
-      const int64_t k = base + (int64_t)j * nx + i;
-      load9(J, NN, k, 0, G);
-      load9(Q, NN, k, 0, Qk);
-      if (i > 0) load_nb(J, NN, k, 0, b1);
-      if (j > 0) load_nb(J, NN, k, 2, b2);
-      r0 = rin[k]; r1 = rin[NN + k]; r2 = rin[2 * NN + k];
+    struct Nd {
+      double G[9], Q[9], bw[5], bc[5], v[3];
     };
+    // forward data of position w (v = r)
+    auto load_f = [&](int w, Nd& o) {
+      if (!lane || w < 0 || w >= Lw) return;
+      const int64_t k = node(w);
+      load9(J, NN, k, 0, o.G);
+      load9(Q, NN, k, 0, o.Q);
+      if (w > 0) load_nb(J, NN, k, dwp, o.bw);
+      if (c > 0) load_nb(J, NN, k, dcp, o.bc);
+      o.v[0] = rin[k]; o.v[1] = rin[NN + k]; o.v[2] = rin[2 * NN + k];
+    };
+    // backward data of position w (v = a from the forward sweep)
+    auto load_b = [&](int w, Nd& o) {
+      if (!lane || w < 0 || w >= Lw) return;
+      const int64_t k = node(w);
+      load9(J, NN, k, 0, o.G);
+      load9(Q, NN, k, 0, o.Q);
+      if (w < Lw - 1) load_nb(J, NN, k, dwn, o.bw);
+      if (c < Lc - 1) load_nb(J, NN, k, dcn, o.bc);
+      o.v[0] = out[k]; o.v[1] = out[NN + k]; o.v[2] = out[2 * NN + k];
+    };
+    Nd A, B;
+    // ---- forward: a_k = Q_k (r_k - G_k (B_walk a_prev + B_cross a_cross))
+    double p0 = 0.0, p1 = 0.0, p2 = 0.0;   // own previous result
+    load_f(0, A);
+    load_f(1, B);
     int cur = 0;
-    load_fwd(0);
     for (int d = 0; d < nd; ++d) {
-      if (have) {
+      const int w = d - c;
+      if (lane && w >= 0 && w < Lw) {
         const int pv = cur ^ 1;
         double u0 = 0.0, u1 = 0.0, u2 = 0.0;
-        if (i > 0) {
-          const double* f = fr[pv][byj ? j : i - 1];
-          add_nb_vec(b1, f[0], f[1], f[2], u0, u1, u2);
+        if (w > 0) add_nb_vec(A.bw, p0, p1, p2, u0, u1, u2);
+        if (c > 0) {
+          const double* f = fr[pv][c - 1];
+          add_nb_vec(A.bc, f[0], f[1], f[2], u0, u1, u2);
         }
-        if (j > 0) {
-          const double* f = fr[pv][byj ? j - 1 : i];
-          add_nb_vec(b2, f[0], f[1], f[2], u0, u1, u2);
-        }
-        const double t0 = r0 - (G[0] * u0 + G[1] * u1 + G[2] * u2);
-        const double t1 = r1 - (G[3] * u0 + G[4] * u1 + G[5] * u2);
-        const double t2 = r2 - (G[6] * u0 + G[7] * u1 + G[8] * u2);
-        const double a0 = Qk[0] * t0 + Qk[1] * t1 + Qk[2] * t2;
-        const double a1 = Qk[3] * t0 + Qk[4] * t1 + Qk[5] * t2;
-        const double a2 = Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2;
-        double* w = fr[cur][byj ? j : i];
-        w[0] = a0; w[1] = a1; w[2] = a2;
-        const int64_t k = base + (int64_t)j * nx + i;
-        out[k] = (T)a0; out[NN + k] = (T)a1; out[2 * NN + k] = (T)a2;
+        const double t0 = A.v[0] - (A.G[0] * u0 + A.G[1] * u1 + A.G[2] * u2);
+        const double t1 = A.v[1] - (A.G[3] * u0 + A.G[4] * u1 + A.G[5] * u2);
+        const double t2 = A.v[2] - (A.G[6] * u0 + A.G[7] * u1 + A.G[8] * u2);
+        p0 = A.Q[0] * t0 + A.Q[1] * t1 + A.Q[2] * t2;
+        p1 = A.Q[3] * t0 + A.Q[4] * t1 + A.Q[5] * t2;
+        p2 = A.Q[6] * t0 + A.Q[7] * t1 + A.Q[8] * t2;
+        double* f = fr[cur][c];
+        f[0] = p0; f[1] = p1; f[2] = p2;
+        const int64_t k = node(w);
+        out[k] = (T)p0; out[NN + k] = (T)p1; out[2 * NN + k] = (T)p2;
+        A = B;
+        load_f(w + 2, B);
       }
-      load_fwd(d + 1);
       __syncthreads();
       cur ^= 1;
     }
-    // ---- backward: x_k = a_k - Q_k G_k (B_kE x_E + B_kN x_N)
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    auto load_bwd = [&](int d) {
-      have = node_of(d);
-      if (!have) return;
-      const int64_t k = base + (int64_t)j * nx + i;
-      load9(J, NN, k, 0, G);
-      load9(Q, NN, k, 0, Qk);
-      if (i < nx - 1) load_nb(J, NN, k, 1, b1);
-      if (j < ny - 1) load_nb(J, NN, k, 3, b2);
-      a0 = out[k]; a1 = out[NN + k]; a2 = out[2 * NN + k];
-    };
-    load_bwd(nd - 1);
+    __syncthreads();
+    // ---- backward: x_k = a_k - Q_k G_k (B_walk x_next + B_cross x_cross)
+    load_b(Lw - 1, A);
+    load_b(Lw - 2, B);
     for (int d = nd - 1; d >= 0; --d) {
-      if (have) {
+      const int w = d - c;
+      if (lane && w >= 0 && w < Lw) {
         const int pv = cur ^ 1;
         double u0 = 0.0, u1 = 0.0, u2 = 0.0;
-        if (i < nx - 1) {
-          const double* f = fr[pv][byj ? j : i + 1];
-          add_nb_vec(b1, f[0], f[1], f[2], u0, u1, u2);
+        if (w < Lw - 1) add_nb_vec(A.bw, p0, p1, p2, u0, u1, u2);
+        if (c < Lc - 1) {
+          const double* f = fr[pv][c + 1];
+          add_nb_vec(A.bc, f[0], f[1], f[2], u0, u1, u2);
         }
-        if (j < ny - 1) {
-          const double* f = fr[pv][byj ? j + 1 : i];
-          add_nb_vec(b2, f[0], f[1], f[2], u0, u1, u2);
-        }
-        const double t0 = G[0] * u0 + G[1] * u1 + G[2] * u2;
-        const double t1 = G[3] * u0 + G[4] * u1 + G[5] * u2;
-        const double t2 = G[6] * u0 + G[7] * u1 + G[8] * u2;
-        const double x0 = a0 - (Qk[0] * t0 + Qk[1] * t1 + Qk[2] * t2);
-        const double x1 = a1 - (Qk[3] * t0 + Qk[4] * t1 + Qk[5] * t2);
-        const double x2 = a2 - (Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2);
-        double* w = fr[cur][byj ? j : i];
-        w[0] = x0; w[1] = x1; w[2] = x2;
-        const int64_t k = base + (int64_t)j * nx + i;
-        out[k] = (T)x0; out[NN + k] = (T)x1; out[2 * NN + k] = (T)x2;
+        const double t0 = A.G[0] * u0 + A.G[1] * u1 + A.G[2] * u2;
+        const double t1 = A.G[3] * u0 + A.G[4] * u1 + A.G[5] * u2;
+        const double t2 = A.G[6] * u0 + A.G[7] * u1 + A.G[8] * u2;
+        p0 = A.v[0] - (A.Q[0] * t0 + A.Q[1] * t1 + A.Q[2] * t2);
+        p1 = A.v[1] - (A.Q[3] * t0 + A.Q[4] * t1 + A.Q[5] * t2);
+        p2 = A.v[2] - (A.Q[6] * t0 + A.Q[7] * t1 + A.Q[8] * t2);
+        double* f = fr[cur][c];
+        f[0] = p0; f[1] = p1; f[2] = p2;
+        const int64_t k = node(w);
+        out[k] = (T)p0; out[NN + k] = (T)p1; out[2 * NN + k] = (T)p2;
+        A = B;
+        load_b(w - 2, B);
       }
-      load_bwd(d - 1);
       __syncthreads();
       cur ^= 1;
     }
