@@ -176,8 +176,8 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
   const int nx = g.nx, ny = g.ny;
   const int nd = nx + ny - 1;
   // Fast path when every anti-diagonal fits the block (min(nx, ny) <=
-  // threads).  Thread c owns one row of the shorter dimension (j, or i when
-  // nx < ny) and walks along it, one node per anti-diagonal level: the
+  // threads).  Each thread owns one row c of the shorter dimension (j, or i
+  // when nx < ny) and walks along it, one node per anti-diagonal level: the
   // previous node of its own row is in a register, the other lower
   // neighbour (row c-1, same position) comes from a shared-memory front,
   // and the node data of the next two positions of its row is already in
@@ -186,7 +186,11 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
   const int Lc = byj ? ny : nx, Lw = byj ? nx : ny;
   if (Lc <= kIluThreads) {
     __shared__ double fr[2][kIluThreads][3];
-    const int c = threadIdx.x;
+    // rows by parity: warps 0..3 own the even rows, warps 4..7 the odd ones,
+    // so (d - c) has one parity across a warp and the slot choice below
+    // never diverges inside a warp
+    const int tid = threadIdx.x, half = kIluThreads / 2;
+    const int c = tid < half ? 2 * tid : 2 * (tid - half) + 1;
     const bool lane = c < Lc;
     // neighbour directions: along the row (walk) and across rows (cross)
     const int dwp = byj ? 0 : 2, dcp = byj ? 2 : 0;   // forward: W/S
@@ -217,64 +221,85 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
       if (c < Lc - 1) load_nb(J, NN, k, dcn, o.bc);
       o.v[0] = out[k]; o.v[1] = out[NN + k]; o.v[2] = out[2 * NN + k];
     };
+    // two register slots: position w lives in slot (w & 1); after a
+    // position is used its slot is reloaded with position w + 2 (no copies,
+    // so a pending load is waited for only where its data is used)
     Nd A, B;
-    // ---- forward: a_k = Q_k (r_k - G_k (B_walk a_prev + B_cross a_cross))
     double p0 = 0.0, p1 = 0.0, p2 = 0.0;   // own previous result
+    int cur = 0;
+    auto fstep = [&](const Nd& X, int w) {
+      const int pv = cur ^ 1;
+      double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+      if (w > 0) add_nb_vec(X.bw, p0, p1, p2, u0, u1, u2);
+      if (c > 0) {
+        const double* f = fr[pv][c - 1];
+        add_nb_vec(X.bc, f[0], f[1], f[2], u0, u1, u2);
+      }
+      const double t0 = X.v[0] - (X.G[0] * u0 + X.G[1] * u1 + X.G[2] * u2);
+      const double t1 = X.v[1] - (X.G[3] * u0 + X.G[4] * u1 + X.G[5] * u2);
+      const double t2 = X.v[2] - (X.G[6] * u0 + X.G[7] * u1 + X.G[8] * u2);
+      p0 = X.Q[0] * t0 + X.Q[1] * t1 + X.Q[2] * t2;
+      p1 = X.Q[3] * t0 + X.Q[4] * t1 + X.Q[5] * t2;
+      p2 = X.Q[6] * t0 + X.Q[7] * t1 + X.Q[8] * t2;
+      double* f = fr[cur][c];
+      f[0] = p0; f[1] = p1; f[2] = p2;
+      const int64_t k = node(w);
+      out[k] = (T)p0; out[NN + k] = (T)p1; out[2 * NN + k] = (T)p2;
+    };
+    auto bstep = [&](const Nd& X, int w) {
+      const int pv = cur ^ 1;
+      double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+      if (w < Lw - 1) add_nb_vec(X.bw, p0, p1, p2, u0, u1, u2);
+      if (c < Lc - 1) {
+        const double* f = fr[pv][c + 1];
+        add_nb_vec(X.bc, f[0], f[1], f[2], u0, u1, u2);
+      }
+      const double t0 = X.G[0] * u0 + X.G[1] * u1 + X.G[2] * u2;
+      const double t1 = X.G[3] * u0 + X.G[4] * u1 + X.G[5] * u2;
+      const double t2 = X.G[6] * u0 + X.G[7] * u1 + X.G[8] * u2;
+      p0 = X.v[0] - (X.Q[0] * t0 + X.Q[1] * t1 + X.Q[2] * t2);
+      p1 = X.v[1] - (X.Q[3] * t0 + X.Q[4] * t1 + X.Q[5] * t2);
+      p2 = X.v[2] - (X.Q[6] * t0 + X.Q[7] * t1 + X.Q[8] * t2);
+      double* f = fr[cur][c];
+      f[0] = p0; f[1] = p1; f[2] = p2;
+      const int64_t k = node(w);
+      out[k] = (T)p0; out[NN + k] = (T)p1; out[2 * NN + k] = (T)p2;
+    };
+    // ---- forward: a_k = Q_k (r_k - G_k (B_walk a_prev + B_cross a_cross))
     load_f(0, A);
     load_f(1, B);
-    int cur = 0;
     for (int d = 0; d < nd; ++d) {
       const int w = d - c;
       if (lane && w >= 0 && w < Lw) {
-        const int pv = cur ^ 1;
-        double u0 = 0.0, u1 = 0.0, u2 = 0.0;
-        if (w > 0) add_nb_vec(A.bw, p0, p1, p2, u0, u1, u2);
-        if (c > 0) {
-          const double* f = fr[pv][c - 1];
-          add_nb_vec(A.bc, f[0], f[1], f[2], u0, u1, u2);
+        if ((w & 1) == 0) {
+          fstep(A, w);
+          load_f(w + 2, A);
+        } else {
+          fstep(B, w);
+          load_f(w + 2, B);
         }
-        const double t0 = A.v[0] - (A.G[0] * u0 + A.G[1] * u1 + A.G[2] * u2);
-        const double t1 = A.v[1] - (A.G[3] * u0 + A.G[4] * u1 + A.G[5] * u2);
-        const double t2 = A.v[2] - (A.G[6] * u0 + A.G[7] * u1 + A.G[8] * u2);
-        p0 = A.Q[0] * t0 + A.Q[1] * t1 + A.Q[2] * t2;
-        p1 = A.Q[3] * t0 + A.Q[4] * t1 + A.Q[5] * t2;
-        p2 = A.Q[6] * t0 + A.Q[7] * t1 + A.Q[8] * t2;
-        double* f = fr[cur][c];
-        f[0] = p0; f[1] = p1; f[2] = p2;
-        const int64_t k = node(w);
-        out[k] = (T)p0; out[NN + k] = (T)p1; out[2 * NN + k] = (T)p2;
-        A = B;
-        load_f(w + 2, B);
       }
       __syncthreads();
       cur ^= 1;
     }
-    __syncthreads();
     // ---- backward: x_k = a_k - Q_k G_k (B_walk x_next + B_cross x_cross)
-    load_b(Lw - 1, A);
-    load_b(Lw - 2, B);
+    if (((Lw - 1) & 1) == 0) {
+      load_b(Lw - 1, A);
+      load_b(Lw - 2, B);
+    } else {
+      load_b(Lw - 1, B);
+      load_b(Lw - 2, A);
+    }
     for (int d = nd - 1; d >= 0; --d) {
       const int w = d - c;
       if (lane && w >= 0 && w < Lw) {
-        const int pv = cur ^ 1;
-        double u0 = 0.0, u1 = 0.0, u2 = 0.0;
-        if (w < Lw - 1) add_nb_vec(A.bw, p0, p1, p2, u0, u1, u2);
-        if (c < Lc - 1) {
-          const double* f = fr[pv][c + 1];
-          add_nb_vec(A.bc, f[0], f[1], f[2], u0, u1, u2);
+        if ((w & 1) == 0) {
+          bstep(A, w);
+          load_b(w - 2, A);
+        } else {
+          bstep(B, w);
+          load_b(w - 2, B);
         }
-        const double t0 = A.G[0] * u0 + A.G[1] * u1 + A.G[2] * u2;
-        const double t1 = A.G[3] * u0 + A.G[4] * u1 + A.G[5] * u2;
-        const double t2 = A.G[6] * u0 + A.G[7] * u1 + A.G[8] * u2;
-        p0 = A.v[0] - (A.Q[0] * t0 + A.Q[1] * t1 + A.Q[2] * t2);
-        p1 = A.v[1] - (A.Q[3] * t0 + A.Q[4] * t1 + A.Q[5] * t2);
-        p2 = A.v[2] - (A.Q[6] * t0 + A.Q[7] * t1 + A.Q[8] * t2);
-        double* f = fr[cur][c];
-        f[0] = p0; f[1] = p1; f[2] = p2;
-        const int64_t k = node(w);
-        out[k] = (T)p0; out[NN + k] = (T)p1; out[2 * NN + k] = (T)p2;
-        A = B;
-        load_b(w - 2, B);
       }
       __syncthreads();
       cur ^= 1;
