@@ -73,12 +73,85 @@ __device__ __forceinline__ void add_nb_vec(const double* b, double v0, double v1
   y2 += b[3] * v0 + b[4] * v2;
 }
 
+// ---------------------------------------------------------------------------
+// Coalesced sweep (2D packs whose shorter side fits the block).
+//
+// The sweeps touch one node per row per anti-diagonal level, so in node
+// order every access of a level is a separate memory sector.  The factor
+// therefore also writes what the sweeps read in ANTI-DIAGONAL-MAJOR order:
+// node (c, w) -- row c of the shorter side, position w along it -- of the
+// plane whose first node is `base` sits in slot 2*base + (c + w)*Lc + c.
+// A plane with Lc <= Lw rows has (Lc + Lw - 1) Lc <= 2 Lc Lw slots, so the
+// slots of all planes fit in 2 * n_nodes.  Per slot (FP32, a preconditioner
+// needs no more): forward Q, Q G B_walk, Q G B_cross (27 values),
+// backward Q G B_walk', Q G B_cross' (18) -- G folded in, so
+//   forward  a = Q r - (Q G B_walk) a_prev - (Q G B_cross) a_cross
+//   backward x = a - (Q G B_walk') x_next - (Q G B_cross') x_cross'.
+// The right-hand side is permuted into slot order and the result back by
+// two node-parallel kernels.
+struct IluGeo {
+  bool byj;      // rows are j (ny <= nx), walk along i
+  int Lc, Lw;    // rows, positions per row
+  int64_t soff;  // first slot of the plane
+};
+
+__device__ __forceinline__ IluGeo ilu_geo(const Inst& g, int64_t base) {
+  IluGeo q;
+  q.byj = g.ny <= g.nx;
+  q.Lc = q.byj ? g.ny : g.nx;
+  q.Lw = q.byj ? g.nx : g.ny;
+  q.soff = 2 * base;
+  return q;
+}
+
+// slot of node (i, j) of the plane
+__device__ __forceinline__ int64_t ilu_slot(const IluGeo& q, int i, int j) {
+  const int c = q.byj ? j : i, w = q.byj ? i : j;
+  return q.soff + (int64_t)(c + w) * q.Lc + c;
+}
+
+// store the forward / backward sweep data of node k (FP32, slot order)
+__device__ __forceinline__ void ilu_store_slot(const double* __restrict__ J, int64_t NN,
+                                               int64_t k, const IluGeo& q, int i, int j,
+                                               int nx, int ny, const double* Qk,
+                                               float* __restrict__ Mf, float* __restrict__ Mb,
+                                               int64_t NS) {
+  double G[9], QG[9], b[5], T1[9];
+  load9(J, NN, k, 0, G);
+  mul33(Qk, G, QG);
+  const int64_t sl = ilu_slot(q, i, j);
+  const int c = q.byj ? j : i, w = q.byj ? i : j;
+  // direction indices: W 0, E 1, S 2, N 3
+  const int dwp = q.byj ? 0 : 2, dcp = q.byj ? 2 : 0;
+  const int dwn = q.byj ? 1 : 3, dcn = q.byj ? 3 : 1;
+#pragma unroll
+  for (int e = 0; e < 9; ++e) Mf[(int64_t)e * NS + sl] = (float)Qk[e];
+  const bool has[4] = {w > 0, c > 0, w < q.Lw - 1, c < q.Lc - 1};
+  const int dir[4] = {dwp, dcp, dwn, dcn};
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    if (has[m]) {
+      load_nb(J, NN, k, dir[m], b);
+      mul_dense_nb(QG, b, T1);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) T1[e] = 0.0;
+    }
+    float* dst = m < 2 ? Mf + (int64_t)(9 + 9 * m) * NS : Mb + (int64_t)(9 * (m - 2)) * NS;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) dst[(int64_t)e * NS + sl] = (float)T1[e];
+  }
+  (void)nx; (void)ny;
+}
+
+// r (node order) -> rs (slot order) for the instances preconditioned here;
+// the others' ph = p is written by k_ilu_unperm.
 // Factor: Q_k for every node of each instance whose pre_status is TCAD_OK;
 // status[inst] = TCAD_ERR_SINGULAR when a D~ block is singular.
 __global__ void __launch_bounds__(kIluThreads)
 k_ilu2d_factor(const tcad_pack_t pk, const double* __restrict__ J, double* __restrict__ Q,
                const int32_t* __restrict__ pre_status, int32_t* __restrict__ status,
-               int nzmax) {
+               int nzmax, float* __restrict__ Mf, float* __restrict__ Mb) {
   const int inst = blockIdx.x / nzmax, z = blockIdx.x % nzmax;
   if (pre_status && pre_status[inst] != TCAD_OK) return;
   const Inst g = load_inst(pk, inst);
@@ -146,6 +219,7 @@ k_ilu2d_factor(const tcad_pack_t pk, const double* __restrict__ J, double* __res
       }
 #pragma unroll
       for (int e = 0; e < 9; ++e) Q[(int64_t)e * NN + k] = inv[e];
+      if (Mf) ilu_store_slot(J, NN, k, ilu_geo(g, base), i, j, nx, ny, inv, Mf, Mb, 2 * NN);
     }
     __syncthreads();
   }
@@ -361,6 +435,190 @@ k_ilu2d_apply(const tcad_pack_t pk, const double* __restrict__ J, const double* 
       out[2 * NN + k] = (T)((double)out[2 * NN + k] - (Qk[6] * t0 + Qk[7] * t1 + Qk[8] * t2));
     }
     __syncthreads();
+  }
+}
+
+}  // namespace tcad
+
+namespace tcad {
+
+constexpr int NT_ILU_FLAT = 256;  // flat (node-parallel) permutation kernels
+
+template <class T>
+__global__ void __launch_bounds__(NT_ILU_FLAT)
+k_ilu_perm(const tcad_pack_t pk, const T* __restrict__ r, double* __restrict__ rs,
+           const KState* ks, const uint8_t* __restrict__ mask, const int32_t* __restrict__ blk,
+           int64_t NS) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
+  if (ks && !ks[fb.inst].active) return;
+  if (mask && !mask[fb.inst]) return;
+  const Inst g = load_inst(pk, fb.inst);
+  const IluGeo q = ilu_geo(g, g.off);
+  const int64_t NN = pk.n_nodes;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT_ILU_FLAT) {
+    const int64_t loc = k - g.off;
+    const int i = (int)(loc % g.nx), j = (int)(loc / g.nx);
+    const int64_t sl = ilu_slot(q, i, j);
+    rs[sl] = (double)r[k];
+    rs[NS + sl] = (double)r[NN + k];
+    rs[2 * NS + sl] = (double)r[2 * NN + k];
+  }
+}
+
+// out (node order) = xs (slot order); instances not preconditioned: out = r
+template <class T>
+__global__ void __launch_bounds__(NT_ILU_FLAT)
+k_ilu_unperm(const tcad_pack_t pk, const double* __restrict__ xs, const T* __restrict__ r,
+             T* __restrict__ out, const KState* ks, const uint8_t* __restrict__ mask,
+             const int32_t* __restrict__ blk, int64_t NS) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
+  if (ks && !ks[fb.inst].active) return;
+  const int64_t NN = pk.n_nodes;
+  if (mask && !mask[fb.inst]) {
+    for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT_ILU_FLAT) {
+      out[k] = r[k]; out[NN + k] = r[NN + k]; out[2 * NN + k] = r[2 * NN + k];
+    }
+    return;
+  }
+  const Inst g = load_inst(pk, fb.inst);
+  const IluGeo q = ilu_geo(g, g.off);
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT_ILU_FLAT) {
+    const int64_t loc = k - g.off;
+    const int i = (int)(loc % g.nx), j = (int)(loc / g.nx);
+    const int64_t sl = ilu_slot(q, i, j);
+    out[k] = (T)xs[sl]; out[NN + k] = (T)xs[NS + sl]; out[2 * NN + k] = (T)xs[2 * NS + sl];
+  }
+}
+
+// The sweeps, one CTA per 2D instance (Lc <= kIluThreads): thread c owns
+// row c.  Level d's data of thread c is slot soff + d Lc + c, so a level's
+// loads are coalesced across the block; they are issued two levels ahead
+// into one of three register sets chosen by d mod 3 (uniform in the block).
+// xs holds a after the forward sweep and x after the backward one.
+__global__ void __launch_bounds__(kIluThreads)
+k_ilu_sweep(const tcad_pack_t pk, const float* __restrict__ Mf, const float* __restrict__ Mb,
+            const double* __restrict__ rs, double* __restrict__ xs, const KState* ks,
+            const uint8_t* __restrict__ mask, int64_t NS) {
+  const int inst = blockIdx.x;
+  if (ks && !ks[inst].active) return;
+  if (mask && !mask[inst]) return;
+  const Inst g = load_inst(pk, inst);
+  const IluGeo q = ilu_geo(g, g.off);
+  const int Lc = q.Lc, Lw = q.Lw, nd = Lc + Lw - 1;
+  const int c = threadIdx.x;
+  const bool lane = c < Lc;
+  __shared__ double fr[2][kIluThreads][3];
+  struct Fd {
+    float q[9], mw[9], mc[9];
+    double r[3];
+  };
+  struct Bd {
+    float mw[9], mc[9];
+    double a[3];
+  };
+  auto valid = [&](int d) { const int w = d - c; return lane && d >= 0 && d < nd && w >= 0 && w < Lw; };
+  auto fload = [&](int d, Fd& o) {
+    if (!valid(d)) return;
+    const int64_t sl = q.soff + (int64_t)d * Lc + c;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      o.q[e] = Mf[(int64_t)e * NS + sl];
+      o.mw[e] = Mf[(int64_t)(9 + e) * NS + sl];
+      o.mc[e] = Mf[(int64_t)(18 + e) * NS + sl];
+    }
+    o.r[0] = rs[sl]; o.r[1] = rs[NS + sl]; o.r[2] = rs[2 * NS + sl];
+  };
+  auto bload = [&](int d, Bd& o) {
+    if (!valid(d)) return;
+    const int64_t sl = q.soff + (int64_t)d * Lc + c;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      o.mw[e] = Mb[(int64_t)e * NS + sl];
+      o.mc[e] = Mb[(int64_t)(9 + e) * NS + sl];
+    }
+    o.a[0] = xs[sl]; o.a[1] = xs[NS + sl]; o.a[2] = xs[2 * NS + sl];
+  };
+  double p0 = 0.0, p1 = 0.0, p2 = 0.0;  // own previous result (same row)
+  int cur = 0;
+  auto fstep = [&](int d, const Fd& X) {
+    if (valid(d)) {
+      const int w = d - c;
+      const double* fc = fr[cur ^ 1][c > 0 ? c - 1 : 0];
+      const double c0 = c > 0 ? fc[0] : 0.0, c1 = c > 0 ? fc[1] : 0.0, c2 = c > 0 ? fc[2] : 0.0;
+      const double w0 = w > 0 ? p0 : 0.0, w1 = w > 0 ? p1 : 0.0, w2 = w > 0 ? p2 : 0.0;
+      double a[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        a[r] = ((double)X.q[3 * r] * X.r[0] + (double)X.q[3 * r + 1] * X.r[1] +
+                (double)X.q[3 * r + 2] * X.r[2]) -
+               ((double)X.mw[3 * r] * w0 + (double)X.mw[3 * r + 1] * w1 +
+                (double)X.mw[3 * r + 2] * w2) -
+               ((double)X.mc[3 * r] * c0 + (double)X.mc[3 * r + 1] * c1 +
+                (double)X.mc[3 * r + 2] * c2);
+      p0 = a[0]; p1 = a[1]; p2 = a[2];
+      double* f = fr[cur][c];
+      f[0] = a[0]; f[1] = a[1]; f[2] = a[2];
+      const int64_t sl = q.soff + (int64_t)d * Lc + c;
+      xs[sl] = a[0]; xs[NS + sl] = a[1]; xs[2 * NS + sl] = a[2];
+    }
+    __syncthreads();
+    cur ^= 1;
+  };
+  auto bstep = [&](int d, const Bd& X) {
+    if (valid(d)) {
+      const int w = d - c;
+      const double* fc = fr[cur ^ 1][c < Lc - 1 ? c + 1 : c];
+      const bool hc = c < Lc - 1, hw = w < Lw - 1;
+      const double c0 = hc ? fc[0] : 0.0, c1 = hc ? fc[1] : 0.0, c2 = hc ? fc[2] : 0.0;
+      const double w0 = hw ? p0 : 0.0, w1 = hw ? p1 : 0.0, w2 = hw ? p2 : 0.0;
+      double x[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        x[r] = X.a[r] -
+               ((double)X.mw[3 * r] * w0 + (double)X.mw[3 * r + 1] * w1 +
+                (double)X.mw[3 * r + 2] * w2) -
+               ((double)X.mc[3 * r] * c0 + (double)X.mc[3 * r + 1] * c1 +
+                (double)X.mc[3 * r + 2] * c2);
+      p0 = x[0]; p1 = x[1]; p2 = x[2];
+      double* f = fr[cur][c];
+      f[0] = x[0]; f[1] = x[1]; f[2] = x[2];
+      const int64_t sl = q.soff + (int64_t)d * Lc + c;
+      xs[sl] = x[0]; xs[NS + sl] = x[1]; xs[2 * NS + sl] = x[2];
+    }
+    __syncthreads();
+    cur ^= 1;
+  };
+  {  // forward, levels 0 .. nd-1, data two levels ahead
+    Fd S0, S1, S2;
+    fload(0, S0);
+    fload(1, S1);
+    for (int d = 0; d < nd; d += 3) {
+      fload(d + 2, S2);
+      fstep(d, S0);
+      if (d + 1 >= nd) break;
+      fload(d + 3, S0);
+      fstep(d + 1, S1);
+      if (d + 2 >= nd) break;
+      fload(d + 4, S1);
+      fstep(d + 2, S2);
+    }
+  }
+  {  // backward, levels nd-1 .. 0
+    Bd S0, S1, S2;
+    bload(nd - 1, S0);
+    bload(nd - 2, S1);
+    for (int d = nd - 1; d >= 0; d -= 3) {
+      bload(d - 2, S2);
+      bstep(d, S0);
+      if (d - 1 < 0) break;
+      bload(d - 3, S0);
+      bstep(d - 1, S1);
+      if (d - 2 < 0) break;
+      bload(d - 4, S1);
+      bstep(d - 2, S2);
+    }
   }
 }
 

@@ -877,18 +877,29 @@ struct WorkIlu {
   double* sh;
   uint8_t* mask;    // instances preconditioned with ILU(0)
   int32_t* pre;     // factor pre-status (-1: skip)
+  float* Mf;        // 2D: forward sweep data in anti-diagonal slot order [27][2n]
+  float* Mb;        //     backward sweep data [18][2n]
+  double* rs;       //     right-hand side in slot order [3][2n]
+  double* xs;       //     sweep result in slot order [3][2n]
   size_t bytes;
 };
 
 static WorkIlu carve_ilu(const tcad_pack_t* pk, void* base) {
   Carve c{reinterpret_cast<char*>(base), 0, 0};
-  WorkIlu w{nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+  WorkIlu w{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   const size_t v3 = 3 * (size_t)pk->n_nodes;
   w.Q = c.take<double>(9 * (size_t)pk->n_nodes);
   w.ph = c.take<double>(v3);
   w.sh = c.take<double>(v3);
   w.mask = c.take<uint8_t>(pk->n_inst);
   w.pre = c.take<int32_t>(pk->n_inst);
+  if (pk->dim == 2) {
+    const size_t ns = 2 * (size_t)pk->n_nodes;
+    w.Mf = c.take<float>(27 * ns);
+    w.Mb = c.take<float>(18 * ns);
+    w.rs = c.take<double>(3 * ns);
+    w.xs = c.take<double>(3 * ns);
+  }
   w.bytes = c.used;
   return w;
 }
@@ -923,13 +934,36 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   return w;
 }
 
+// out = M^-1 r: the coalesced slot-order sweeps when the factor wrote them
+// (2D, every shorter side <= kIluThreads), else the node-order sweeps
+template <class T>
+static void ilu_apply_t(const tcad_pack_t* pk, const double* J, const double* Q, const T* r,
+                        T* out, const Work& w, const uint8_t* mask, int nzmax,
+                        const WorkIlu* ilc, unsigned ng, const int32_t* dlist,
+                        cudaStream_t s) {
+  const int ni = pk->n_inst;
+  if (ilc && ilc->Mf) {
+    const int64_t NS = 2 * pk->n_nodes;
+    k_ilu_perm<T><<<ng, NT_ILU_FLAT, 0, s>>>(*pk, r, ilc->rs, w.ks, mask, dlist, NS);
+    k_ilu_sweep<<<(unsigned)ni, kIluThreads, 0, s>>>(*pk, ilc->Mf, ilc->Mb, ilc->rs, ilc->xs,
+                                                     w.ks, mask, NS);
+    k_ilu_unperm<T><<<ng, NT_ILU_FLAT, 0, s>>>(*pk, ilc->xs, r, out, w.ks, mask, dlist, NS);
+    note_launch(3);
+    return;
+  }
+  k_ilu2d_apply<T><<<(unsigned)(ni * nzmax), kIluThreads, 0, s>>>(*pk, J, Q, r, out, w.ks, mask,
+                                                                  nzmax);
+  note_launch();
+}
+
 template <class T>
 static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x, double rtol,
                              int maxiter, const BiVecT<T>& bi, const Work& w,
                              const int32_t* pre_status, std::vector<KState>& hks,
                              cudaStream_t s, const double* rtol_inst,
                              const double* Jilu = nullptr, const double* Qilu = nullptr,
-                             const uint8_t* ilu_mask = nullptr, int nzmax = 1) {
+                             const uint8_t* ilu_mask = nullptr, int nzmax = 1,
+                             const WorkIlu* ilc = nullptr) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
@@ -961,10 +995,8 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
     for (int q = 0; q < check; ++q) {
       k_bi_p<<<ng, NT, 0, s>>>(*pk, bi, w.ks, dlist);
       note_launch();
-      if (Qilu) {  // ph = M^-1 p (one CTA per instance)
-        k_ilu2d_apply<T><<<(unsigned)(ni * nzmax), kIluThreads, 0, s>>>(
-            *pk, Jilu, Qilu, bi.p, bi.ph, w.ks, ilu_mask, nzmax);
-        note_launch();
+      if (Qilu) {  // ph = M^-1 p
+        ilu_apply_t<T>(pk, Jilu, Qilu, bi.p, bi.ph, w, ilu_mask, nzmax, ilc, ng, dlist, s);
       }
       if (pk->dim == 2)
         k_bi_v<2><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
@@ -974,9 +1006,7 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
       k_bi_s<<<ng, NT, 0, s>>>(*pk, bi, w.ks, w.partial, w.ticket, dlist);
       note_launch();
       if (Qilu) {  // sh = M^-1 s
-        k_ilu2d_apply<T><<<(unsigned)(ni * nzmax), kIluThreads, 0, s>>>(
-            *pk, Jilu, Qilu, bi.s, bi.sh, w.ks, ilu_mask, nzmax);
-        note_launch();
+        ilu_apply_t<T>(pk, Jilu, Qilu, bi.s, bi.sh, w, ilu_mask, nzmax, ilc, ng, dlist, s);
       }
       if (pk->dim == 2)
         k_bi_t<2><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
@@ -1050,7 +1080,7 @@ static int launch_bicgstab(const tcad_pack_t* pk, const double* J, const double*
     bi.ph = ilu->ph;
     bi.sh = ilu->sh;
     return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, bi, w, pre_status, hks, s,
-                                     rtol_inst, J, ilu->Q, ilu->mask, nzmax);
+                                     rtol_inst, J, ilu->Q, ilu->mask, nzmax, ilu);
   }
   return launch_bicgstab_t<double>(pk, J, b, x, rtol, maxiter, w.bi, w, pre_status, hks, s,
                                    rtol_inst);
@@ -1223,6 +1253,19 @@ extern "C" size_t tcad_block_ilu_bytes(const tcad_pack_t* pk) {
   return 9 * sizeof(double) * (size_t)pk->n_nodes;
 }
 
+// largest shorter side min(Nx, Ny) of the pack's instances (host read)
+static int pack_max_short_side(const tcad_pack_t* pk, cudaStream_t s) {
+  if (pk->n_inst < 1) return 0;
+  std::vector<int32_t> shp(3 * (size_t)pk->n_inst);
+  if (cudaMemcpyAsync(shp.data(), pk->shape, sizeof(int32_t) * shp.size(),
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return 1 << 30;
+  int m = 0;
+  for (int i = 0; i < pk->n_inst; ++i) m = std::max(m, std::min((int)shp[3 * i], (int)shp[3 * i + 1]));
+  return m;
+}
+
 // largest Nz of the pack's instances (host read of the shape table)
 static int pack_nzmax(const tcad_pack_t* pk, cudaStream_t s) {
   if (pk->dim == 2 || pk->n_inst < 1) return 1;
@@ -1243,7 +1286,7 @@ extern "C" int tcad_block_ilu_setup(const tcad_pack_t* pk, const double* J, doub
   const int nzm = pack_nzmax(pk, (cudaStream_t)stream);
   if (nzm < 1) return TCAD_ERR_CUDA;
   k_ilu2d_factor<<<(unsigned)(pk->n_inst * nzm), kIluThreads, 0, (cudaStream_t)stream>>>(
-      *pk, J, Q, nullptr, status, nzm);
+      *pk, J, Q, nullptr, status, nzm, nullptr, nullptr);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;
@@ -1353,7 +1396,13 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   const WorkIlu wilu = use_ilu ? carve_ilu(pk, reinterpret_cast<char*>(work) +
                                                    ((w.bytes + 255) & ~(size_t)255) +
                                                    ((w32.bytes + 255) & ~(size_t)255))
-                               : WorkIlu{nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+                               : WorkIlu{nullptr, nullptr, nullptr, nullptr, nullptr,
+                                         nullptr, nullptr, nullptr, nullptr, 0};
+  WorkIlu wilu_use = wilu;
+  if (use_ilu && (pk->dim != 2 || pack_max_short_side(pk, s) > kIluThreads)) {
+    wilu_use.Mf = nullptr;  // node-order sweeps
+    wilu_use.Mb = nullptr;
+  }
   std::vector<int32_t> mix_it(ni), mix_st(ni), mix_grew(ni, 0), mix_steps(ni, 0);
   std::vector<double> mix_rr(ni), mix_prev(ni, -1.0);
   std::vector<uint8_t> use64(ni, 0);  // precision 32: instances switched to FP64
@@ -1529,13 +1578,13 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
         TCAD_CUDA_CHECK(cudaMemcpyAsync(wilu.pre, pre.data(), sizeof(int32_t) * ni,
                                         cudaMemcpyHostToDevice, s));
         TCAD_CUDA_CHECK(cudaMemcpyAsync(wilu.mask, msk.data(), ni, cudaMemcpyHostToDevice, s));
-        k_ilu2d_factor<<<(unsigned)(ni * nzmax), kIluThreads, 0, s>>>(*pk, J, wilu.Q, wilu.pre,
-                                                                       nullptr, nzmax);
+        k_ilu2d_factor<<<(unsigned)(ni * nzmax), kIluThreads, 0, s>>>(
+            *pk, J, wilu.Q, wilu.pre, nullptr, nzmax, wilu_use.Mf, wilu_use.Mb);
         note_launch();
         TCAD_LAUNCH_CHECK();
       }
       rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
-                           w.eta, any_ilu ? &wilu : nullptr, nzmax);
+                           w.eta, any_ilu ? &wilu_use : nullptr, nzmax);
       if (rc != TCAD_OK) return rc;
       std::vector<uint8_t> apply(ni, 0), retry(ni, 0);
       bool any_retry = false;

@@ -51,6 +51,8 @@ def bytes_per_node(dim):
     work64 = 6 * 3 * 8 + 4 * 8 / 256
     work32 = 6 * 3 * 4 + ne * 4 + 2 * 3 * 4
     ilu = (9 + 6) * 8                        # ILU(0) factor and two vectors
+    if dim == 2:                             # slot-order sweep data (FP32) and vectors
+        ilu += 2 * (27 + 18) * 4 + 2 * 2 * 3 * 8
     return int(np.ceil(doubles * 8 + 1 + work64 + work32 + ilu))
 
 

@@ -113,5 +113,5 @@ def test_arena_bytes_per_node():
     from tcad_b200.serve import bytes_per_node
     # coefficients + BC + state + previous state + F + J + du (doubles),
     # bcflag, FP64 and FP32 Krylov workspace, ILU(0) factor and vectors
-    assert 920 <= bytes_per_node(2) <= 1000
+    assert 1370 <= bytes_per_node(2) <= 1460
     assert 1060 <= bytes_per_node(3) <= 1140
