@@ -30,14 +30,16 @@ __device__ __forceinline__ void bern4(double x, double& Bp, double& Bm, double& 
   }
   const double e1 = expm1(x);   // e^x - 1
   const double e2 = expm1(-x);  // e^-x - 1
-  Bp = x / e1;
-  Bm = (-x) / e2;
-  double om = -e2;  // 1 - e^-x
-  if (fabs(om) < 1e-300) om = 1e-300;
-  dBp = Bp * (1.0 / x - 1.0 / om);
-  double om2 = -e1;  // 1 - e^x
-  if (fabs(om2) < 1e-300) om2 = 1e-300;
-  dBm = Bm * (1.0 / (-x) - 1.0 / om2);
+  // Off the series branch |x| >= 1e-4, so |e1|, |e2| > 9e-5: the
+  // reference's 1e-300 floor on 1 - e^-x and 1 - e^x never applies, and the
+  // four values share three reciprocals (1/(1 - e^-x) = -1/e2,
+  // 1/(1 - e^x) = -1/e1, 1/(-x) = -1/x) -- the same formulas, rounded at
+  // the last bit differently from one division each.
+  const double r1 = 1.0 / e1, r2 = 1.0 / e2, ix = 1.0 / x;
+  Bp = x * r1;
+  Bm = (-x) * r2;
+  dBp = Bp * (ix + r2);
+  dBm = Bm * (r1 - ix);
 }
 
 // Everything the two endpoint rows need from one edge (low -> high node).
@@ -96,10 +98,11 @@ __device__ __forceinline__ void recomb(double n, double p, double nie, double ta
   const double nph = n * Ns, pph = p * Ns;
   const double excess = nph * pph - nie * nie;
   const double den = taup * (nph + nie) + taun * (pph + nie);
-  double R = excess / den;
-  const double den2 = den * den;
-  double dRdn = (pph * den - excess * taup) / den2;
-  double dRdp = (nph * den - excess * taun) / den2;
+  const double iden = 1.0 / den;   // one reciprocal for R and its derivatives
+  double R = excess * iden;
+  const double iden2 = iden * iden;
+  double dRdn = (pph * den - excess * taup) * iden2;
+  double dRdp = (nph * den - excess * taun) * iden2;
   if (par[TCAD_P_AUGER] != 0.0) {
     const double Cn = par[TCAD_P_CN], Cp = par[TCAD_P_CP];
     const double cc = Cn * nph + Cp * pph;
@@ -107,9 +110,10 @@ __device__ __forceinline__ void recomb(double n, double p, double nie, double ta
     dRdn = dRdn + Cn * excess + cc * pph;
     dRdp = dRdp + Cp * excess + cc * nph;
   }
-  Rs = R / R0;
-  dRsn = dRdn * Ns / R0;
-  dRsp = dRdp * Ns / R0;
+  const double iR0 = 1.0 / R0;
+  Rs = R * iR0;
+  dRsn = dRdn * Ns * iR0;
+  dRsp = dRdp * Ns * iR0;
 }
 
 }  // namespace tcad
