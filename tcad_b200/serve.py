@@ -25,6 +25,7 @@ a request's result is the one it gets alone.
 from __future__ import annotations
 
 import collections
+import copy
 import threading
 import time
 
@@ -256,12 +257,23 @@ class RoundPack(Pack):
         raise NotImplementedError
 
 
+def own_setup(setup):
+    """A copy of a Setup whose contacts and gates are its own objects (the
+    coefficient arrays stay shared, read-only): the bias a session applies
+    lives on its BC objects, so two sessions built from one Setup must not
+    share them."""
+    own = copy.copy(setup)
+    own.bcs = {name: copy.copy(b) for name, b in setup.bcs.items()}
+    return own
+
+
 class Session:
-    """A device resident (or to be resident) in an arena."""
+    """A device resident (or to be resident) in an arena.  It owns its BC
+    objects (own_setup), so requests that share a Setup keep their biases."""
 
     def __init__(self, key, setup):
         self.key = key
-        self.setup = setup
+        self.setup = own_setup(setup)
         self.pl = None
         self.bias_prev = self.bias_cur = None
         self.need_eq = True

@@ -141,3 +141,28 @@ def test_repeated_device_stays_resident():
         assert grew < 8 * setup.N * 2      # guess + bias values, not the coefficients
     finally:
         srv.stop()
+
+
+def test_requests_sharing_a_setup_keep_their_own_bias():
+    """Two requests on different keys built from ONE Setup object (a design
+    served to two clients at once) are solved at their own biases."""
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    from tcad_b200.serve import Request, Server
+    opts = tb.NewtonOptions()
+    q = MOS[0]
+    pa = W.ramp({"gate": 0.9, "drain": 0.6}, 3)
+    pb = W.ramp({"gate": 0.3, "drain": 1.0}, 3)
+    ref = {"a": _alone(lambda: _mosfet(q), pa, [False, False, True], "drain", opts),
+           "b": _alone(lambda: _mosfet(q), pb, [False, False, True], "drain", opts)}
+    setup = _mosfet(q).setup
+    srv = Server(budget={2: 64 << 20}, opts=opts).start()
+    try:
+        ra = srv.submit(Request("a", setup, pa, "drain", [False, False, True],
+                                return_state=True))
+        rb = srv.submit(Request("b", setup, pb, "drain", [False, False, True],
+                                return_state=True))
+        assert srv.wait_idle(120)
+        _check([ra, rb], ref)
+    finally:
+        srv.stop()
