@@ -709,7 +709,8 @@ def run_serve(args):
         p_req += 1
         r = served[f"{kind}-{q}"]
         if r.error is None and r.currents:
-            p_err.extend(abs(x - y) / max(abs(y), 1e-300) for x, y in zip(r.currents, I))
+            p_err.extend(abs(x - y) / max(abs(y), 1e-300)
+                         for x, y, ok_ in zip(r.currents, I, r.converged) if ok_)
         dev._pack = None
     plain_rate = p_pts / p_time if p_time > 0 else None
     return {
