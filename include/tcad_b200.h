@@ -183,6 +183,16 @@ int tcad_state_extrapolate(const tcad_pack_t* pk, double* psi, double* n, double
  * Workspace size in bytes for tcad_block_krylov / tcad_newton_solve. */
 size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart);
 
+/* Launch shape of the node-block-Jacobi BiCGStab (an implementation switch;
+ * the reference has no counterpart: pytcad/linsolve.py:725-985 is one
+ * scipy call).  on = 1 (the default): a single-instance pack whose flat
+ * blocks all fit on the GPU at once is solved in ONE cooperative launch --
+ * one CTA per flat block, bounded grid barriers between the steps, the same
+ * arithmetic in the same order as the launch-per-step kernels, so the
+ * result is bit-identical; on = 0: one launch per step always.  Process-
+ * wide; returns the previous setting. */
+int tcad_set_krylov_fused(int on);
+
 /* Node-block-Jacobi set-up (pytcad/linsolve.py:363-427): inverts every
  * diagonal 3x3 block of J in place and replaces F by the block-scaled
  * right-hand side b^ = D^-1 (-F).  status[inst] gets TCAD_ERR_SINGULAR for a

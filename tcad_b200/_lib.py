@@ -83,6 +83,7 @@ _SIGS = {
     "tcad_edge_currents": (ctypes.c_int, [_p, ctypes.c_int, _p, _p, _p, _p, _p, _p]),
     "tcad_poisson_assemble": (ctypes.c_int, [_p, _p, _p, _p, ctypes.c_int, _p]),
     "tcad_block_workspace_bytes": (ctypes.c_size_t, [_p, ctypes.c_int, ctypes.c_int]),
+    "tcad_set_krylov_fused": (ctypes.c_int, [ctypes.c_int]),
     "tcad_state_extrapolate": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "tcad_block_jacobi_setup": (ctypes.c_int, [_p, _p, _p, _p, _p]),
     "tcad_block_jacobi_setup_rel": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, ctypes.c_double,

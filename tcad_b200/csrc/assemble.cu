@@ -23,13 +23,12 @@ struct NodeVals {
 // Neighbour-block entry offsets: 9 + 5*d + m.
 __device__ __forceinline__ int nb(int d, int m) { return 9 + 5 * d + m; }
 
-// CTAs per SM the coupled assembly is compiled for (register budget)
-#ifndef TCAD_ASM_MIN_CTAS
-#define TCAD_ASM_MIN_CTAS 3
-#endif
-
+// CTAs per SM the coupled assembly is compiled for (register budget):
+// 4 in 2D (64 registers, no spills), 3 in 3D (80 registers; the z-march
+// carries two edges and two node states in registers, and at 64 registers
+// the spills cost more than the fourth CTA gains)
 template <int DIM>
-__global__ void __launch_bounds__(kTileThreads, TCAD_ASM_MIN_CTAS)
+__global__ void __launch_bounds__(kTileThreads, DIM == 2 ? 4 : 3)
 k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
               const double* __restrict__ nn, const double* __restrict__ pp,
               double* __restrict__ F, double* __restrict__ J, int mode,

@@ -9,9 +9,11 @@
 // itself runs without host round trips; blocks of finished instances return
 // immediately, which is the per-instance convergence mask of a packed batch.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -44,15 +46,16 @@ __device__ __forceinline__ void nbr_offsets(const Inst& g, int64_t* off) {
 }
 
 // --------------------------------------------------------------------------
-// partial sums -> per-instance totals (last block finalizes)
+// partial sums -> per-instance totals.  store(): this block's sums into
+// partial[b * 4 + q]; total(): the instance's block partials summed in block
+// order (valid in thread 0).  run(): both, the total taken by the LAST block
+// of the instance to finish (atomic ticket); true in every thread of that
+// block.
 template <int NS>
 struct Reduce {
-  // returns true in every thread of the block that must finalize
-  __device__ static bool run(const tcad_pack_t& pk, int64_t b, int inst, double (&v)[NS],
-                             double* partial, unsigned* ticket, double* tot) {
+  __device__ static void store(int64_t b, double (&v)[NS], double* partial) {
     __shared__ double sm[32];
     __shared__ double st[NS];
-    __shared__ int last;
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
       const double r = block_sum<NT>(v[q], sm);
@@ -61,14 +64,11 @@ struct Reduce {
     if (threadIdx.x == 0) {
 #pragma unroll
       for (int q = 0; q < NS; ++q) partial[b * 4 + q] = st[q];
-      __threadfence();
-      const int64_t nb = pk.flat_off[inst + 1] - pk.flat_off[inst];
-      const unsigned prev = atomicAdd(&ticket[inst], 1u);
-      last = (prev == (unsigned)(nb - 1));
     }
-    __syncthreads();
-    if (!last) return false;
-    __threadfence();
+  }
+  __device__ static void total(const tcad_pack_t& pk, int inst, const double* partial,
+                               double* tot) {
+    __shared__ double sm[32];
     const int64_t b0 = pk.flat_off[inst], b1 = pk.flat_off[inst + 1];
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
@@ -77,10 +77,100 @@ struct Reduce {
       const double r = block_sum<NT>(s, sm);
       if (threadIdx.x == 0) tot[q] = r;
     }
+  }
+  __device__ static bool run(const tcad_pack_t& pk, int64_t b, int inst, double (&v)[NS],
+                             double* partial, unsigned* ticket, double* tot) {
+    __shared__ int last;
+    store(b, v, partial);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const int64_t nb = pk.flat_off[inst + 1] - pk.flat_off[inst];
+      const unsigned prev = atomicAdd(&ticket[inst], 1u);
+      last = (prev == (unsigned)(nb - 1));
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    total(pk, inst, partial, tot);
     if (threadIdx.x == 0) ticket[inst] = 0u;
     return true;
   }
 };
+
+// --------------------------------------------------------------------------
+// BiCGStab scalar updates of one instance from its totals.  Both the
+// launch-per-step kernels (last block of the instance) and the fused
+// persistent kernel (every CTA, on its shared copy) use these.
+__device__ __forceinline__ void fin_init(KState& s, double tot, double rt, int maxit,
+                                         int pre) {
+  s.bb = tot; s.rr = tot; s.r0n2 = tot;
+  s.tol2 = rt * rt * tot;
+  s.rho = tot; s.rho_prev = 1.0; s.alpha = 1.0; s.omega = 1.0;
+  s.beta = 0.0; s.it = 0; s.maxit = maxit; s.restart = 0; s.early = 0;
+  s.status = pre;
+  const bool done = s.status != TCAD_OK || !(tot > 0.0) || !isfinite(tot);
+  if (s.status == TCAD_OK && !isfinite(tot)) s.status = TCAD_ERR_NONFINITE;
+  s.active = done ? 0 : 1;
+}
+
+// alpha = rho / (rh, v)
+__device__ __forceinline__ void fin_v(KState& s, double rv) {
+  s.restart = 0;
+  s.rv = rv;
+  if (rv == 0.0 || !isfinite(rv)) {
+    s.status = TCAD_ERR_BREAKDOWN;
+    s.active = 0;
+  } else {
+    s.alpha = s.rho / rv;
+  }
+}
+
+// (s, s): early exit when s alone meets the tolerance
+__device__ __forceinline__ void fin_s(KState& s, double ss) {
+  s.ss = ss;
+  s.early = ss <= s.tol2 ? 1 : 0;
+}
+
+// omega = (t, s) / (t, t)
+__device__ __forceinline__ void fin_t(KState& s, double ts, double tt) {
+  s.omega = (s.early || !(tt > 0.0)) ? 0.0 : ts / tt;
+}
+
+// rho = (rh, r), convergence on (r, r), restart when the shadow residual is lost
+__device__ __forceinline__ void fin_x(KState& s, double rhr, double rr, double hh) {
+  s.it += 1;
+  s.rr = rr;
+  s.rho_prev = s.rho;
+  s.rho = rhr;
+  if (!isfinite(rr)) {
+    s.status = TCAD_ERR_NONFINITE;
+    s.active = 0;
+  } else if (rr <= s.tol2) {
+    s.active = 0;                     // converged (true residual checked next)
+  } else if (s.it >= s.maxit) {
+    s.status = TCAD_ERR_NOCONV;
+    s.active = 0;
+  } else if (s.omega == 0.0 || fabs(rhr) <= 1e-14 * sqrt(rr * hh)) {
+    s.restart = 1;                    // shadow residual lost: restart from r
+    s.rho = rr;
+    s.r0n2 = rr;
+    s.beta = 0.0;
+  } else {
+    s.beta = (s.rho / s.rho_prev) * (s.alpha / s.omega);
+  }
+}
+
+// true residual norm; re-arm a restart when the recursive residual drifted
+__device__ __forceinline__ void fin_true(KState& s, double rr, int rearm) {
+  s.rr = rr;
+  if (rearm && s.status == TCAD_OK && s.bb > 0.0 && rr > 4.0 * s.tol2 && s.it < s.maxit &&
+      isfinite(rr)) {
+    s.active = 1;
+    s.restart = 1;
+    s.rho = rr;
+    s.r0n2 = rr;
+  }
+}
 
 }  // namespace tcad
 #include "ilu.cuh"
@@ -165,21 +255,24 @@ k_bj_setup(const tcad_pack_t pk, double* __restrict__ J, double* __restrict__ F,
 // y = D x + sum_d A_d x_nbr(d)             (raw J, !SCALED)
 // T is the storage and arithmetic type (double: plain path; float: the
 // mixed-precision inner solves).
-template <int DIM, bool SCALED, class T>
-__device__ __forceinline__ void spmv_node(const T* __restrict__ J, const T* __restrict__ x,
-                                          int64_t k, int64_t NN, const int64_t* off,
-                                          int64_t lo, int64_t hi, T& y0, T& y1, T& y2) {
+// The vector is read through X(m, c) = x[c * NN + m] (spmv_node) or any
+// other functor giving the same values (the fused solve forms neighbour
+// values on the fly); the arithmetic is the same either way.
+template <int DIM, bool SCALED, class T, class XF>
+__device__ __forceinline__ void spmv_node_f(const T* __restrict__ J, const XF& X, int64_t k,
+                                            int64_t NN, const int64_t* off, int64_t lo,
+                                            int64_t hi, T& y0, T& y1, T& y2) {
   T t0 = T(0), t1 = T(0), t2 = T(0);
 #pragma unroll
   for (int d = 0; d < 2 * DIM; ++d) {
     const int64_t m = clampi(k + off[d], lo, hi);
     const int e = 9 + 5 * d;
-    const T xs = x[m], xn = x[NN + m], xp = x[2 * NN + m];
+    const T xs = X(m, 0), xn = X(m, 1), xp = X(m, 2);
     t0 += J[(int64_t)e * NN + k] * xs;
     t1 += J[(int64_t)(e + 1) * NN + k] * xs + J[(int64_t)(e + 2) * NN + k] * xn;
     t2 += J[(int64_t)(e + 3) * NN + k] * xs + J[(int64_t)(e + 4) * NN + k] * xp;
   }
-  const T x0 = x[k], x1 = x[NN + k], x2 = x[2 * NN + k];
+  const T x0 = X(k, 0), x1 = X(k, 1), x2 = X(k, 2);
   T d[9];
 #pragma unroll
   for (int e = 0; e < 9; ++e) d[e] = J[(int64_t)e * NN + k];
@@ -192,6 +285,14 @@ __device__ __forceinline__ void spmv_node(const T* __restrict__ J, const T* __re
     y1 = d[3] * x0 + d[4] * x1 + d[5] * x2 + t1;
     y2 = d[6] * x0 + d[7] * x1 + d[8] * x2 + t2;
   }
+}
+
+template <int DIM, bool SCALED, class T>
+__device__ __forceinline__ void spmv_node(const T* __restrict__ J, const T* __restrict__ x,
+                                          int64_t k, int64_t NN, const int64_t* off,
+                                          int64_t lo, int64_t hi, T& y0, T& y1, T& y2) {
+  spmv_node_f<DIM, SCALED, T>(J, [&](int64_t m, int c) { return x[c * NN + m]; }, k, NN, off,
+                              lo, hi, y0, y1, y2);
 }
 
 template <int DIM, bool SCALED>
@@ -212,7 +313,10 @@ k_spmv(const tcad_pack_t pk, const double* __restrict__ J, const double* __restr
 
 // --------------------------------------------------------------------------
 // BiCGStab on A^ (per instance).  Vectors: r, rh (shadow), p, v, s, t; x.
-// Scalars and dot products are always FP64.
+// Scalars and dot products are always FP64.  Each step's per-block work is a
+// body function (returning the thread's partial dot products), shared by the
+// launch-per-step kernels and the fused persistent kernel, so both run the
+// same arithmetic in the same order.
 template <class T>
 struct BiVecT {
   T *r, *rh, *p, *v, *s, *t;
@@ -220,51 +324,33 @@ struct BiVecT {
 };
 using BiVec = BiVecT<double>;
 
+// x = 0, r = rh = b, p = v = 0; (b, b)
 template <class T>
-__global__ void __launch_bounds__(NT)
-k_bi_init(const tcad_pack_t pk, const T* __restrict__ b, T* __restrict__ x, BiVecT<T> w,
-          KState* ks, double* partial, unsigned* ticket, double rtol, int maxit,
-          const int32_t* __restrict__ pre_status, const double* __restrict__ rtol_inst) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+__device__ __forceinline__ double bi_init_body(const tcad_pack_t& pk, const FlatBlock& fb,
+                                               const T* __restrict__ b, T* __restrict__ x,
+                                               const BiVecT<T>& w) {
   const int64_t NN = pk.n_nodes;
-  double v[1] = {0.0};
+  double v = 0.0;
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t q = c * NN + k;
       const T bv = b[q];
       x[q] = T(0); w.r[q] = bv; w.rh[q] = bv; w.p[q] = T(0); w.v[q] = T(0);
-      v[0] += (double)bv * (double)bv;
+      v += (double)bv * (double)bv;
     }
   }
-  double tot[1];
-  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
-    KState& s = ks[fb.inst];
-    s.bb = tot[0]; s.rr = tot[0]; s.r0n2 = tot[0];
-    const double rt = rtol_inst ? rtol_inst[fb.inst] : rtol;
-    s.tol2 = rt * rt * tot[0];
-    s.rho = tot[0]; s.rho_prev = 1.0; s.alpha = 1.0; s.omega = 1.0;
-    s.beta = 0.0; s.it = 0; s.maxit = maxit; s.restart = 0; s.early = 0;
-    s.status = pre_status ? pre_status[fb.inst] : TCAD_OK;
-    const bool done = s.status != TCAD_OK || !(tot[0] > 0.0) || !isfinite(tot[0]);
-    if (s.status == TCAD_OK && !isfinite(tot[0])) s.status = TCAD_ERR_NONFINITE;
-    s.active = done ? 0 : 1;
-  }
+  return v;
 }
 
 // p = r + beta (p - omega v)   (restart: rh = r, p = r)
-// The vector kernels read through restrict-qualified locals and issue every
+// The vector bodies read through restrict-qualified locals and issue every
 // load of two nodes before any store, so each thread keeps a dozen loads in
 // flight (the struct members alone would force load-store serialisation).
 template <class T>
-__global__ void __launch_bounds__(NT, 4)
-k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __restrict__ blk) {
-  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
-  const FlatBlock fb = flat_block(pk, fbi);
-  const KState s = ks[fb.inst];
-  if (!s.active) return;
+__device__ __forceinline__ void bi_p_body(const tcad_pack_t& pk, const FlatBlock& fb,
+                                          const BiVecT<T>& w, T beta, T omega, int restart) {
   const int64_t NN = pk.n_nodes;
-  const T beta = (T)s.beta, omega = (T)s.omega;
   const T* __restrict__ R = w.r;
   const T* __restrict__ V = w.v;
   T* __restrict__ P = w.p;
@@ -276,10 +362,10 @@ k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __res
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       r[c] = R[c * NN + k0];
-      if (!s.restart) { pv[c] = P[c * NN + k0]; vv[c] = V[c * NN + k0]; }
+      if (!restart) { pv[c] = P[c * NN + k0]; vv[c] = V[c * NN + k0]; }
       if (two) {
         r[3 + c] = R[c * NN + k1];
-        if (!s.restart) { pv[3 + c] = P[c * NN + k1]; vv[3 + c] = V[c * NN + k1]; }
+        if (!restart) { pv[3 + c] = P[c * NN + k1]; vv[3 + c] = V[c * NN + k1]; }
       }
     }
 #pragma unroll
@@ -289,7 +375,7 @@ k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __res
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const int q = 3 * h + c;
-        if (s.restart) {
+        if (restart) {
           RH[c * NN + k] = r[q];
           P[c * NN + k] = r[q];
         } else {
@@ -300,19 +386,15 @@ k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __res
   }
 }
 
-// v = A^ p, alpha = rho / (rh, v)
+// v = A^ ph; (rh, v)
 template <int DIM, class T>
-__global__ void __launch_bounds__(NT)
-k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
-       double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
-  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
-  const FlatBlock fb = flat_block(pk, fbi);
-  if (!ks[fb.inst].active) return;
+__device__ __forceinline__ double bi_v_body(const tcad_pack_t& pk, const FlatBlock& fb,
+                                            const T* __restrict__ J, const BiVecT<T>& w) {
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
   nbr_offsets(g, off);
   const int64_t NN = pk.n_nodes;
-  double v[1] = {0.0};
+  double v = 0.0;
   const T* __restrict__ X = w.ph;
   const T* __restrict__ RH = w.rh;
   T* __restrict__ Vo = w.v;
@@ -321,37 +403,20 @@ k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
     spmv_node<DIM, true, T>(J, X, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
     const T h0 = RH[k], h1 = RH[NN + k], h2 = RH[2 * NN + k];
     Vo[k] = y0; Vo[NN + k] = y1; Vo[2 * NN + k] = y2;
-    v[0] += (double)h0 * y0 + (double)h1 * y1 + (double)h2 * y2;
+    v += (double)h0 * y0 + (double)h1 * y1 + (double)h2 * y2;
   }
-  double tot[1];
-  if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
-    KState& s = ks[fb.inst];
-    s.restart = 0;
-    s.rv = tot[0];
-    if (tot[0] == 0.0 || !isfinite(tot[0])) {
-      s.status = TCAD_ERR_BREAKDOWN;
-      s.active = 0;
-    } else {
-      s.alpha = s.rho / tot[0];
-    }
-  }
+  return v;
 }
 
-// s = r - alpha v, (s, s)
+// s = r - alpha v; (s, s)
 template <class T>
-__global__ void __launch_bounds__(NT, 4)
-k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned* ticket,
-       const int32_t* __restrict__ blk) {
-  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
-  const FlatBlock fb = flat_block(pk, fbi);
-  const KState s0 = ks[fb.inst];
-  if (!s0.active) return;
+__device__ __forceinline__ double bi_s_body(const tcad_pack_t& pk, const FlatBlock& fb,
+                                            const BiVecT<T>& w, T alpha) {
   const int64_t NN = pk.n_nodes;
-  const T alpha = (T)s0.alpha;
   const T* __restrict__ R = w.r;
   const T* __restrict__ V = w.v;
   T* __restrict__ S = w.s;
-  double v[1] = {0.0};
+  double v = 0.0;
   for (int64_t k0 = fb.begin + threadIdx.x; k0 < fb.end; k0 += 2 * NT) {
     const int64_t k1 = k0 + NT;
     const bool two = k1 < fb.end;
@@ -370,31 +435,23 @@ k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned*
       for (int c = 0; c < 3; ++c) {
         const T sv = r[3 * h + c] - alpha * vv[3 * h + c];
         S[c * NN + k] = sv;
-        v[0] += (double)sv * (double)sv;
+        v += (double)sv * (double)sv;
       }
     }
   }
-  double tot[1];
-  if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
-    KState& s = ks[fb.inst];
-    s.ss = tot[0];
-    s.early = tot[0] <= s.tol2 ? 1 : 0;
-  }
+  return v;
 }
 
-// t = A^ s, omega = (t, s) / (t, t)
+// t = A^ sh; (t, s), (t, t)
 template <int DIM, class T>
-__global__ void __launch_bounds__(NT)
-k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
-       double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
-  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
-  const FlatBlock fb = flat_block(pk, fbi);
-  if (!ks[fb.inst].active) return;
+__device__ __forceinline__ void bi_t_body(const tcad_pack_t& pk, const FlatBlock& fb,
+                                          const T* __restrict__ J, const BiVecT<T>& w,
+                                          double (&v)[2]) {
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
   nbr_offsets(g, off);
   const int64_t NN = pk.n_nodes;
-  double v[2] = {0.0, 0.0};
+  v[0] = 0.0; v[1] = 0.0;
   const T* __restrict__ X = w.sh;
   const T* __restrict__ S = w.s;
   T* __restrict__ To = w.t;
@@ -406,32 +463,58 @@ k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
     v[0] += (double)y0 * s0 + (double)y1 * s1 + (double)y2 * s2;
     v[1] += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
   }
-  double tot[2];
-  if (Reduce<2>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
-    KState& s = ks[fb.inst];
-    s.omega = (s.early || !(tot[1] > 0.0)) ? 0.0 : tot[0] / tot[1];
+}
+
+// The s and t steps in one pass (fused solve, no preconditioner): s = r -
+// alpha v at the block's nodes (stored), t = A^ s with the neighbours' s
+// formed from their r and v (neither changes in this step); (s, s), (t, s),
+// (t, t).  Same expressions and accumulation order as bi_s_body followed by
+// bi_t_body.
+template <int DIM>
+__device__ __forceinline__ void bi_st_body(const tcad_pack_t& pk, const FlatBlock& fb,
+                                           const double* __restrict__ J, const BiVec& w,
+                                           double alpha, double (&v)[3]) {
+  const Inst g = load_inst(pk, fb.inst);
+  int64_t off[6];
+  nbr_offsets(g, off);
+  const int64_t NN = pk.n_nodes;
+  v[0] = 0.0; v[1] = 0.0; v[2] = 0.0;
+  const double* R = w.r;
+  const double* V = w.v;
+  double* S = w.s;
+  double* To = w.t;
+  const auto sval = [&](int64_t m, int c) {
+    const double rv = R[c * NN + m], vv = V[c * NN + m];
+    const double sv = rv - alpha * vv;
+    return sv;
+  };
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    const double s0 = sval(k, 0), s1 = sval(k, 1), s2 = sval(k, 2);
+    S[k] = s0; S[NN + k] = s1; S[2 * NN + k] = s2;
+    v[0] += (double)s0 * (double)s0;
+    v[0] += (double)s1 * (double)s1;
+    v[0] += (double)s2 * (double)s2;
+    double y0, y1, y2;
+    spmv_node_f<DIM, true, double>(J, sval, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    To[k] = y0; To[NN + k] = y1; To[2 * NN + k] = y2;
+    v[1] += (double)y0 * s0 + (double)y1 * s1 + (double)y2 * s2;
+    v[2] += (double)y0 * y0 + (double)y1 * y1 + (double)y2 * y2;
   }
 }
 
-// x += alpha p + omega s; r = s - omega t; rho = (rh, r); (r, r)
-// (with a right preconditioner x moves along M^-1 p and M^-1 s)
+// x += alpha ph + omega sh; r = s - omega t; (rh, r), (r, r), (rh, rh)
 template <class T>
-__global__ void __launch_bounds__(NT, 3)
-k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double* partial,
-       unsigned* ticket, const int32_t* __restrict__ blk) {
-  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
-  const FlatBlock fb = flat_block(pk, fbi);
-  const KState s0 = ks[fb.inst];
-  if (!s0.active) return;
+__device__ __forceinline__ void bi_x_body(const tcad_pack_t& pk, const FlatBlock& fb,
+                                          T* __restrict__ x, const BiVecT<T>& w, T alpha,
+                                          T omega, double (&v)[3]) {
   const int64_t NN = pk.n_nodes;
-  const T alpha = (T)s0.alpha, omega = (T)s0.omega;
   const T* __restrict__ PH = w.ph;
   const T* __restrict__ SH = w.sh;
   const T* __restrict__ S = w.s;
   const T* __restrict__ Tt = w.t;
   const T* __restrict__ RH = w.rh;
   T* __restrict__ R = w.r;
-  double v[3] = {0.0, 0.0, 0.0};
+  v[0] = 0.0; v[1] = 0.0; v[2] = 0.0;
   for (int64_t k0 = fb.begin + threadIdx.x; k0 < fb.end; k0 += 2 * NT) {
     const int64_t k1 = k0 + NT;
     const bool two = k1 < fb.end;
@@ -463,30 +546,107 @@ k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double*
       }
     }
   }
-  double tot[3];
-  if (Reduce<3>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
-    KState& s = ks[fb.inst];
-    s.it += 1;
-    s.rr = tot[1];
-    s.rho_prev = s.rho;
-    s.rho = tot[0];
-    if (!isfinite(tot[1])) {
-      s.status = TCAD_ERR_NONFINITE;
-      s.active = 0;
-    } else if (tot[1] <= s.tol2) {
-      s.active = 0;                     // converged (true residual checked by the host)
-    } else if (s.it >= s.maxit) {
-      s.status = TCAD_ERR_NOCONV;
-      s.active = 0;
-    } else if (s.omega == 0.0 || fabs(tot[0]) <= 1e-14 * sqrt(tot[1] * tot[2])) {
-      s.restart = 1;                    // shadow residual lost: restart from r
-      s.rho = tot[1];
-      s.r0n2 = tot[1];
-      s.beta = 0.0;
-    } else {
-      s.beta = (s.rho / s.rho_prev) * (s.alpha / s.omega);
-    }
+}
+
+// r = b - A^ x; (r, r)
+template <int DIM, class T>
+__device__ __forceinline__ double true_resid_body(const tcad_pack_t& pk, const FlatBlock& fb,
+                                                  const T* __restrict__ J,
+                                                  const T* __restrict__ b,
+                                                  const T* __restrict__ x, T* __restrict__ r) {
+  const Inst g = load_inst(pk, fb.inst);
+  int64_t off[6];
+  nbr_offsets(g, off);
+  const int64_t NN = pk.n_nodes;
+  double v = 0.0;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    T y0, y1, y2;
+    spmv_node<DIM, true, T>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
+    const T a0 = b[k] - y0, a1 = b[NN + k] - y1, a2 = b[2 * NN + k] - y2;
+    r[k] = a0; r[NN + k] = a1; r[2 * NN + k] = a2;
+    v += (double)a0 * a0 + (double)a1 * a1 + (double)a2 * a2;
   }
+  return v;
+}
+
+// ---- one launch per step (any pack; blocks of finished instances return)
+template <class T>
+__global__ void __launch_bounds__(NT)
+k_bi_init(const tcad_pack_t pk, const T* __restrict__ b, T* __restrict__ x, BiVecT<T> w,
+          KState* ks, double* partial, unsigned* ticket, double rtol, int maxit,
+          const int32_t* __restrict__ pre_status, const double* __restrict__ rtol_inst) {
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  double v[1] = {bi_init_body<T>(pk, fb, b, x, w)};
+  double tot[1];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
+    fin_init(ks[fb.inst], tot[0], rtol_inst ? rtol_inst[fb.inst] : rtol, maxit,
+             pre_status ? pre_status[fb.inst] : TCAD_OK);
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT, 4)
+k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
+  const KState s = ks[fb.inst];
+  if (!s.active) return;
+  bi_p_body<T>(pk, fb, w, (T)s.beta, (T)s.omega, s.restart);
+}
+
+template <int DIM, class T>
+__global__ void __launch_bounds__(NT)
+k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
+       double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
+  if (!ks[fb.inst].active) return;
+  double v[1] = {bi_v_body<DIM, T>(pk, fb, J, w)};
+  double tot[1];
+  if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
+    fin_v(ks[fb.inst], tot[0]);
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT, 4)
+k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned* ticket,
+       const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
+  const KState s0 = ks[fb.inst];
+  if (!s0.active) return;
+  double v[1] = {bi_s_body<T>(pk, fb, w, (T)s0.alpha)};
+  double tot[1];
+  if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
+    fin_s(ks[fb.inst], tot[0]);
+}
+
+template <int DIM, class T>
+__global__ void __launch_bounds__(NT)
+k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
+       double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
+  if (!ks[fb.inst].active) return;
+  double v[2];
+  bi_t_body<DIM, T>(pk, fb, J, w, v);
+  double tot[2];
+  if (Reduce<2>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
+    fin_t(ks[fb.inst], tot[0], tot[1]);
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT, 3)
+k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double* partial,
+       unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
+  const KState s0 = ks[fb.inst];
+  if (!s0.active) return;
+  double v[3];
+  bi_x_body<T>(pk, fb, x, w, (T)s0.alpha, (T)s0.omega, v);
+  double tot[3];
+  if (Reduce<3>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
+    fin_x(ks[fb.inst], tot[0], tot[1], tot[2]);
 }
 
 // true scaled residual r = b - A^ x, its norm into the state; re-arm a restart
@@ -497,30 +657,154 @@ k_true_resid(const tcad_pack_t pk, const T* __restrict__ J, const T* __restrict_
              const T* __restrict__ x, T* __restrict__ r, KState* ks, double* partial,
              unsigned* ticket, int rearm) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
-  const Inst g = load_inst(pk, fb.inst);
-  int64_t off[6];
-  nbr_offsets(g, off);
-  const int64_t NN = pk.n_nodes;
-  double v[1] = {0.0};
-  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
-    T y0, y1, y2;
-    spmv_node<DIM, true, T>(J, x, k, NN, off, fb.ioff, fb.iend, y0, y1, y2);
-    const T a0 = b[k] - y0, a1 = b[NN + k] - y1, a2 = b[2 * NN + k] - y2;
-    r[k] = a0; r[NN + k] = a1; r[2 * NN + k] = a2;
-    v[0] += (double)a0 * a0 + (double)a1 * a1 + (double)a2 * a2;
-  }
+  double v[1] = {true_resid_body<DIM, T>(pk, fb, J, b, x, r)};
   double tot[1];
-  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
-    KState& s = ks[fb.inst];
-    s.rr = tot[0];
-    if (rearm && s.status == TCAD_OK && s.bb > 0.0 && tot[0] > 4.0 * s.tol2 &&
-        s.it < s.maxit && isfinite(tot[0])) {
-      s.active = 1;
-      s.restart = 1;
-      s.rho = tot[0];
-      s.r0n2 = tot[0];
+  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
+    fin_true(ks[fb.inst], tot[0], rearm);
+}
+
+// ---- the whole solve in one cooperative launch (single-instance packs whose
+// flat blocks all fit on the GPU at once: one CTA per flat block)
+//
+// Grid barrier: thread 0 of each CTA adds one arrival to the monotonic
+// counter bar[0] (acquire-release, so the CTA's writes before the barrier are
+// visible to every CTA after it) and waits until the counter reaches
+// round x nblocks.  Every wait is bounded: past kBarrierNs of device time, or
+// once another CTA has given up (bar[2] != 0), the CTA sets bar[2] and the
+// barrier returns false, and the kernel returns -- the host sees bar[2] and
+// solves again with one launch per step.
+constexpr unsigned long long kBarrierNs = 1000000000ull;   // 1 s
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+               : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks, unsigned& round) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int good = 1;
+    round += 1u;
+    const unsigned target = round * nblocks;
+    const unsigned prev = atom_add_acq_rel(&bar[0], 1u);
+    if (prev + 1u != target) {
+      const unsigned long long t0 = globaltimer_ns();
+      for (unsigned it = 0;; ++it) {
+        if ((int)(ld_acquire(&bar[0]) - target) >= 0) break;
+        if ((it & 255u) == 255u) {
+          if (ld_acquire(&bar[2]) != 0u) { good = 0; break; }
+          if (globaltimer_ns() - t0 > kBarrierNs || it > (1u << 30)) {
+            atomicExch(&bar[2], 1u);
+            good = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
     }
+    __threadfence();
+    ok = good;
   }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Four barriers per iteration: p; v (alpha); s and t in one pass (early,
+// omega); x (rho, beta, convergence).  Block partials alternate between two
+// halves of `partial` by step parity: a CTA reaches the next step's store
+// only after every CTA has passed the barrier that follows its read of the
+// previous totals.
+template <int DIM>
+__global__ void __launch_bounds__(NT, 2)
+k_bicgstab_fused(const tcad_pack_t pk, const double* __restrict__ J,
+                 const double* __restrict__ b, double* __restrict__ x, BiVec w, KState* ks,
+                 double* partial, unsigned* bar, double rtol, int maxit,
+                 const int32_t* __restrict__ pre_status, const double* __restrict__ rtol_inst,
+                 int max_rechecks) {
+  __shared__ KState S;
+  const unsigned G = gridDim.x;
+  const FlatBlock fb = flat_block(pk, blockIdx.x);
+  const int inst = fb.inst;
+  double* const half[2] = {partial, partial + 4 * (int64_t)pk.n_flat};
+  int ph = 0;
+  unsigned round = 0;
+  double tot[3];
+  {
+    double v[1] = {bi_init_body<double>(pk, fb, b, x, w)};
+    Reduce<1>::store(blockIdx.x, v, half[ph]);
+    if (!grid_barrier(bar, G, round)) return;
+    Reduce<1>::total(pk, inst, half[ph], tot);
+    ph ^= 1;
+    if (threadIdx.x == 0)
+      fin_init(S, tot[0], rtol_inst ? rtol_inst[inst] : rtol, maxit,
+               pre_status ? pre_status[inst] : TCAD_OK);
+    __syncthreads();
+  }
+  for (int rechecks = 0;; ++rechecks) {
+    while (S.active) {
+      bi_p_body<double>(pk, fb, w, S.beta, S.omega, S.restart);
+      if (!grid_barrier(bar, G, round)) return;
+      {
+        double v[1] = {bi_v_body<DIM, double>(pk, fb, J, w)};
+        Reduce<1>::store(blockIdx.x, v, half[ph]);
+        if (!grid_barrier(bar, G, round)) return;
+        Reduce<1>::total(pk, inst, half[ph], tot);
+        ph ^= 1;
+        if (threadIdx.x == 0) fin_v(S, tot[0]);
+        __syncthreads();
+      }
+      if (!S.active) break;
+      {
+        double v[3];
+        bi_st_body<DIM>(pk, fb, J, w, S.alpha, v);
+        Reduce<3>::store(blockIdx.x, v, half[ph]);
+        if (!grid_barrier(bar, G, round)) return;
+        Reduce<3>::total(pk, inst, half[ph], tot);
+        ph ^= 1;
+        if (threadIdx.x == 0) {
+          fin_s(S, tot[0]);
+          fin_t(S, tot[1], tot[2]);
+        }
+        __syncthreads();
+      }
+      {
+        double v[3];
+        bi_x_body<double>(pk, fb, x, w, S.alpha, S.omega, v);
+        Reduce<3>::store(blockIdx.x, v, half[ph]);
+        if (!grid_barrier(bar, G, round)) return;
+        Reduce<3>::total(pk, inst, half[ph], tot);
+        ph ^= 1;
+        if (threadIdx.x == 0) fin_x(S, tot[0], tot[1], tot[2]);
+        __syncthreads();
+      }
+    }
+    {
+      double v[1] = {true_resid_body<DIM, double>(pk, fb, J, b, x, w.r)};
+      Reduce<1>::store(blockIdx.x, v, half[ph]);
+      if (!grid_barrier(bar, G, round)) return;
+      Reduce<1>::total(pk, inst, half[ph], tot);
+      ph ^= 1;
+      if (threadIdx.x == 0) fin_true(S, tot[0], rechecks < max_rechecks ? 1 : 0);
+      __syncthreads();
+    }
+    if (!S.active) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) ks[inst] = S;
 }
 
 // --------------------------------------------------------------------------
@@ -824,7 +1108,8 @@ struct Carve {
 struct Work {
   BiVec bi;
   CgVec cg;
-  double* partial;
+  double* partial;  // 2 x 4 x n_flat: block partial sums (the fused solve alternates halves)
+  unsigned* bar;    // fused solve's grid barrier: counter, generation, gave-up flag
   KState* ks;
   unsigned* ticket;
   int32_t* status;
@@ -921,7 +1206,8 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   w.cg.z = w.bi.r + pk->n_nodes;
   w.cg.p = w.bi.r + 2 * pk->n_nodes;
   w.cg.q = w.bi.rh;
-  w.partial = c.take<double>(4 * (size_t)pk->n_flat);
+  w.partial = c.take<double>(8 * (size_t)pk->n_flat);
+  w.bar = c.take<unsigned>(4);
   w.ks = c.take<KState>(pk->n_inst);
   w.ticket = c.take<unsigned>(pk->n_inst);
   w.status = c.take<int32_t>(pk->n_inst);
@@ -956,6 +1242,64 @@ static void ilu_apply_t(const tcad_pack_t* pk, const double* J, const double* Q,
   note_launch();
 }
 
+// ---- fused (one cooperative launch) BiCGStab: when and how
+static std::atomic<int> g_fused_mode{1};   // 0: one launch per step always
+
+// k_bicgstab_fused<DIM> needs every flat block resident at once
+template <int DIM>
+static bool fused_fits(unsigned nb) {
+  int dev = 0, coop = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+    return false;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return false;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bicgstab_fused<DIM>, NT, 0) !=
+      cudaSuccess)
+    return false;
+  return nb >= 1 && (long long)nb <= (long long)per * sms;
+}
+
+// The whole solve of a single-instance pack in one launch (same arithmetic
+// as the launch-per-step path).  Returns TCAD_OK with hks[0] filled, or 1
+// when the launch was refused or a grid barrier gave up (the caller then
+// solves with one launch per step).
+static int launch_bicgstab_fused(const tcad_pack_t* pk, const double* J, const double* b,
+                                 double* x, double rtol, int maxiter, const BiVec& bi,
+                                 const Work& w, const int32_t* pre_status,
+                                 std::vector<KState>& hks, cudaStream_t s,
+                                 const double* rtol_inst) {
+  TCAD_CUDA_CHECK(cudaMemsetAsync(w.bar, 0, 4 * sizeof(unsigned), s));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)pk->n_flat);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const int rechecks = 8;
+  cudaError_t e =
+      pk->dim == 2
+          ? cudaLaunchKernelEx(&cfg, k_bicgstab_fused<2>, *pk, J, b, x, bi, w.ks, w.partial,
+                               w.bar, rtol, maxiter, pre_status, rtol_inst, rechecks)
+          : cudaLaunchKernelEx(&cfg, k_bicgstab_fused<3>, *pk, J, b, x, bi, w.ks, w.partial,
+                               w.bar, rtol, maxiter, pre_status, rtol_inst, rechecks);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 1;
+  }
+  note_launch();
+  hks.resize(1);
+  unsigned hbar[4] = {0u, 0u, 0u, 0u};
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState), cudaMemcpyDeviceToHost, s));
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(hbar, w.bar, sizeof(hbar), cudaMemcpyDeviceToHost, s));
+  TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+  return hbar[2] != 0u ? 1 : TCAD_OK;
+}
+
 template <class T>
 static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x, double rtol,
                              int maxiter, const BiVecT<T>& bi, const Work& w,
@@ -966,6 +1310,13 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
                              const WorkIlu* ilc = nullptr) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
+  if constexpr (std::is_same<T, double>::value) {
+    if (g_fused_mode.load() && ni == 1 && Qilu == nullptr &&
+        (pk->dim == 2 ? fused_fits<2>(nb) : fused_fits<3>(nb)) &&
+        launch_bicgstab_fused(pk, J, b, x, rtol, maxiter, bi, w, pre_status, hks, s,
+                              rtol_inst) == TCAD_OK)
+      return TCAD_OK;
+  }
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
   k_bi_init<<<nb, NT, 0, s>>>(*pk, b, x, bi, w.ks, w.partial, w.ticket, rtol, maxiter,
                               pre_status, rtol_inst);
@@ -1204,6 +1555,10 @@ static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, do
 }  // namespace tcad
 
 using namespace tcad;
+
+extern "C" int tcad_set_krylov_fused(int on) {
+  return g_fused_mode.exchange(on ? 1 : 0);
+}
 
 extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart) {
   if (!pk) return 0;

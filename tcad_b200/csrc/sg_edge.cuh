@@ -19,7 +19,17 @@ __device__ __forceinline__ void bern_series(double x, double& B, double& dB) {
 }
 
 // B(x), B(-x), B'(x), B'(-x) with B(x) = x / expm1(x) and
-// B'(x) = B(x) (1/x - 1/(1 - e^-x)); the two expm1 values serve all four.
+// B'(x) = B(x) (1/x - 1/(1 - e^-x)), from ONE expm1 and ONE reciprocal.
+//
+// With a = |x|, e = expm1(a) > 0 and r = 1/e:
+//   S  = B(a)   = a r                    (the small side, in (0, 1))
+//   L  = B(-a)  = a e^a / (e^a - 1) = S + a
+//   dS = B'(a)  = S (1/a - (1 + r))     = r (1 - a (1 + r))
+//   dL = B'(-a) = L (r - 1/a)           = (1 + r) (S - 1)
+// (L = a (1 + r), so L / a = 1 + r and S / a = r).  Every sum adds terms
+// of one sign except the ones that are also differences of nearly equal
+// terms in the reference's own formula near the series threshold, so the
+// values agree with B(x) = x / expm1(x) evaluated at +-x to rounding.
 __device__ __forceinline__ void bern4(double x, double& Bp, double& Bm, double& dBp,
                                       double& dBm) {
   x = clip700(x);
@@ -28,18 +38,19 @@ __device__ __forceinline__ void bern4(double x, double& Bp, double& Bm, double& 
     bern_series(-x, Bm, dBm);
     return;
   }
-  const double e1 = expm1(x);   // e^x - 1
-  const double e2 = expm1(-x);  // e^-x - 1
-  // Off the series branch |x| >= 1e-4, so |e1|, |e2| > 9e-5: the
-  // reference's 1e-300 floor on 1 - e^-x and 1 - e^x never applies, and the
-  // four values share three reciprocals (1/(1 - e^-x) = -1/e2,
-  // 1/(1 - e^x) = -1/e1, 1/(-x) = -1/x) -- the same formulas, rounded at
-  // the last bit differently from one division each.
-  const double r1 = 1.0 / e1, r2 = 1.0 / e2, ix = 1.0 / x;
-  Bp = x * r1;
-  Bm = (-x) * r2;
-  dBp = Bp * (ix + r2);
-  dBm = Bm * (r1 - ix);
+  const double a = fabs(x);
+  const double e = expm1(a);
+  const double r = 1.0 / e;
+  const double r1 = 1.0 + r;
+  const double S = a * r;
+  const double L = S + a;
+  const double dS = r * (1.0 - a * r1);
+  const double dL = r1 * (S - 1.0);
+  const bool pos = x > 0.0;
+  Bp = pos ? S : L;
+  Bm = pos ? L : S;
+  dBp = pos ? dS : dL;
+  dBm = pos ? dL : dS;
 }
 
 // Everything the two endpoint rows need from one edge (low -> high node).

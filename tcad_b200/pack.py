@@ -363,6 +363,10 @@ class Pack:
     """Device-memory image of a list of Setups of one dimension, packed back
     to back."""
 
+    # measure the 3D assembly tile depth at the first coupled solve
+    # (tcad_b200.tune); results do not depend on it
+    autotune = True
+
     def __init__(self, setups, device="cuda"):
         import torch
         self._init_common(setups, device)
@@ -676,8 +680,30 @@ class Pack:
         o.polish_eta = float(getattr(opts, "polish_eta", 1e-10))
         return o
 
+    def set_tile_z(self, tile_z):
+        """Re-tile the 3D assembly `tile_z` planes deep (the tile list and
+        the workspace's tile-list room follow)."""
+        if self.dim != 3:
+            return
+        tiles = [instance_tiles(s, 3, tile_z) for s in self.setups]
+        tl = np.concatenate([np.concatenate([np.full((t.shape[0], 1), i, np.int32), t], axis=1)
+                             for i, t in enumerate(tiles)]).ravel().astype(np.int32)
+        self.t["tile"] = self._up(tl, self.torch.int32)
+        self.n_tiles = tl.size // 4
+        P = self.P
+        P.tile = self.t["tile"].data_ptr()
+        P.n_tiles = self.n_tiles
+        P.tile_z = self.tile_z = int(tile_z)
+        wb = int(self.lib.tcad_block_workspace_bytes(self.pref, 0, 0))
+        if wb > self.work.numel():
+            self.work = self.torch.empty(wb, dtype=self.torch.uint8, device=self.device)
+
     def newton(self, opts, active=None):
         ni = len(self.setups)
+        if self.autotune and self.dim == 3 and not getattr(self, "_tuned", False):
+            from . import tune
+            tune.tune_tile_z(self)
+            self._tuned = True
         if active is None:
             self.active.fill_(1)
         else:

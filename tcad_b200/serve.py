@@ -231,6 +231,8 @@ class RoundPack(Pack):
     per-instance tables are built for the set, the node arrays are the
     arena's (n_nodes = arena capacity)."""
 
+    autotune = False     # resident devices keep their placement's tiles
+
     def __init__(self, arena, sessions):
         sessions = sorted(sessions, key=lambda s: s.pl.off)
         self.sessions = sessions
