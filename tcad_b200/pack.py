@@ -237,19 +237,21 @@ def instance_par(s):
 
 
 def choose_tile_z(setups, dim, sm_count=148, ctas_per_sm=3, waves=4.0):
-    """Z depth of the 3D assembly tiles: the deepest of 16, 8, 4, 2 planes
-    whose tile count still fills `waves` waves of the GPU's CTA slots (a
-    deeper tile re-evaluates fewer z-edges at its first plane; a shallower
-    one keeps every SM busy on small meshes)."""
+    """Starting z depth of the 3D assembly tiles (tcad_b200.tune measures the
+    best one at a pack's first coupled solve): the deeper of 4 and 2 planes
+    whose tile count still fills `waves` waves of the GPU's CTA slots, else 1.
+    A deeper tile re-evaluates fewer z-edges at its first plane, but deep
+    tiles leave a long last wave: measured, 1-2 planes are best on a 1M-node
+    mesh and 4 on an 8M-node one; 8 and 16 are slower on both."""
     if dim != 3:
         return 1
     slots = sm_count * ctas_per_sm * waves
-    for tz in (16, 8, 4, 2):
+    for tz in (4, 2):
         n = sum(-(-s.nax[0] // _lib.TILE_X) * -(-s.nax[1] // _lib.TILE_Y) * -(-s.nax[2] // tz)
                 for s in setups)
         if n >= slots:
             return tz
-    return 2
+    return 1
 
 
 def instance_tiles(s, dim, tile_z=1):
