@@ -314,6 +314,9 @@ typedef struct tcad_newton_opts {
   double scale_floor;    /* density_scaling: floor of s (dens_floor when <= 0) */
   double polish_eta;     /* forcing 1: Krylov tolerance of the polishing steps (<= 0: the
                             forcing rule's) */
+  double polish_scale_floor; /* density_scaling: floor of s in the polishing steps (<= 0:
+                                scale_floor); a floor far below the densities lets the
+                                polish resolve sub-floor minority densities */
 } tcad_newton_opts_t;
 
 /* Per-instance result of a Newton solve (host memory). */

@@ -62,7 +62,7 @@ class NewtonOpts(ctypes.Structure):
                 ("precision", ctypes.c_int32),
                 ("density_scaling", ctypes.c_int32), ("precond", ctypes.c_int32),
                 ("eta_min", ctypes.c_double), ("scale_floor", ctypes.c_double),
-                ("polish_eta", ctypes.c_double)]
+                ("polish_eta", ctypes.c_double), ("polish_scale_floor", ctypes.c_double)]
 
 
 class NewtonResult(ctypes.Structure):

@@ -190,8 +190,10 @@ template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_bj_setup(const tcad_pack_t pk, double* __restrict__ J, double* __restrict__ F,
            int32_t* __restrict__ status, const double* __restrict__ nn,
-           const double* __restrict__ pp, double floor_, const int32_t* __restrict__ blk) {
+           const double* __restrict__ pp, double floor_, const int32_t* __restrict__ blk,
+           const double* __restrict__ floor_inst = nullptr) {
   const FlatBlock fb = flat_block(pk, blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x);
+  if (floor_inst) floor_ = floor_inst[fb.inst];   // per-instance floor of this step
   const int64_t NN = pk.n_nodes;
   const bool rel = nn != nullptr;
   int64_t off[6];
@@ -813,9 +815,11 @@ __global__ void __launch_bounds__(NT)
 k_newton_update(const tcad_pack_t pk, double* __restrict__ psi, double* __restrict__ nn,
                 double* __restrict__ pp, const double* __restrict__ du, double max_dpsi,
                 double floor_, const uint8_t* __restrict__ active,
-                unsigned long long* __restrict__ err, int relative, int dry, double sfloor) {
+                unsigned long long* __restrict__ err, int relative, int dry, double sfloor,
+                const double* __restrict__ sfloor_inst = nullptr) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   if (active && !active[fb.inst]) return;
+  if (sfloor_inst) sfloor = sfloor_inst[fb.inst];  // the floor the step was scaled with
   __shared__ double sm[32];
   const int64_t NN = pk.n_nodes;
   double e = 0.0;
@@ -1115,6 +1119,7 @@ struct Work {
   int32_t* status;
   unsigned long long* err;
   double* eta;
+  double* sfl;   // per-instance density floor of the relative unknowns this step
   int32_t* blk;  // compact list of the flat blocks still iterating (Krylov)
   int32_t* fl;   // flat blocks / tiles of the instances a Newton step still
   int32_t* tl;   //   solves (assembly and block-Jacobi set-up)
@@ -1213,6 +1218,7 @@ static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   w.status = c.take<int32_t>(pk->n_inst);
   w.err = c.take<unsigned long long>(pk->n_inst);
   w.eta = c.take<double>(pk->n_inst);
+  w.sfl = c.take<double>(pk->n_inst);
   w.blk = c.take<int32_t>(pk->n_flat);
   w.fl = c.take<int32_t>(pk->n_flat);
   w.tl = c.take<int32_t>(pk->n_tiles);
@@ -1764,6 +1770,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   std::vector<int32_t> last_kit(ni, 0);
   std::vector<double> heta(ni, opts->forcing ? std::max(opts->eta_max, opts->rtol) : opts->rtol);
   const double sfloor = opts->scale_floor > 0.0 ? opts->scale_floor : opts->dens_floor;
+  std::vector<double> hsfl(ni, sfloor);
   const double eta_lo = std::max(opts->rtol, opts->eta_min);
   // Per-step launch lists: once the instances still iterating cover under
   // 3/4 of the pack, the assembly and the block-Jacobi set-up cover only
@@ -1815,15 +1822,22 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
     int rc = sg_assemble_tiles(pk, psi, n, p, F, J, TCAD_MODE_ELIMINATE, tl, ntl, s);
     if (rc != TCAD_OK) return rc;
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int32_t) * ni, s));
+    // density floor of each instance's relative unknowns: the polishing
+    // steps use their own (far below the densities), the others sfloor
+    for (int i = 0; i < ni; ++i)
+      hsfl[i] = (polish_left[i] > 0 && opts->polish_scale_floor > 0.0)
+                    ? opts->polish_scale_floor : sfloor;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(w.sfl, hsfl.data(), sizeof(double) * ni,
+                                    cudaMemcpyHostToDevice, s));
     if (!fl || nfl > 0) {
       const bool rel = opts->density_scaling != 0;
       const double* sn_ = rel ? n : nullptr;
       const double* sp_ = rel ? p : nullptr;
       const unsigned g = fl ? (unsigned)nfl : nb;
       if (pk->dim == 2)
-        k_bj_setup<2><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, sfloor, fl);
+        k_bj_setup<2><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, sfloor, fl, w.sfl);
       else
-        k_bj_setup<3><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, sfloor, fl);
+        k_bj_setup<3><<<g, NT, 0, s>>>(*pk, J, F, w.status, sn_, sp_, sfloor, fl, w.sfl);
     }
     note_launch();
     TCAD_LAUNCH_CHECK();
@@ -1865,7 +1879,8 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       // stays in FP64 for the rest of the call.
       TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp32.data(), ni, cudaMemcpyHostToDevice, s));
       k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
-                                        active, w.err, opts->density_scaling, 1, sfloor);
+                                        active, w.err, opts->density_scaling, 1, sfloor,
+                                        w.sfl);
       note_launch();
       TCAD_LAUNCH_CHECK();
       TCAD_CUDA_CHECK(cudaMemcpyAsync(herr.data(), w.err, sizeof(unsigned long long) * ni,
@@ -1904,7 +1919,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
         TCAD_CUDA_CHECK(cudaMemcpyAsync(active, grp32.data(), ni, cudaMemcpyHostToDevice, s));
         k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi,
                                           opts->dens_floor, active, w.err,
-                                          opts->density_scaling, 0, sfloor);
+                                          opts->density_scaling, 0, sfloor, w.sfl);
         note_launch();
         TCAD_LAUNCH_CHECK();
       }
@@ -1966,7 +1981,8 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
       // their du is overwritten by the next pass)
       TCAD_CUDA_CHECK(cudaMemcpyAsync(active, apply.data(), ni, cudaMemcpyHostToDevice, s));
       k_newton_update<<<nb, NT, 0, s>>>(*pk, psi, n, p, du, opts->max_dpsi, opts->dens_floor,
-                                        active, w.err, opts->density_scaling, 0, sfloor);
+                                        active, w.err, opts->density_scaling, 0, sfloor,
+                                        w.sfl);
       note_launch();
       TCAD_LAUNCH_CHECK();
       if (!any_retry) break;

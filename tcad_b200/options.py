@@ -85,6 +85,13 @@ class NewtonOptions:
     # are small differences of large drift and diffusion fluxes, so the
     # state after the last step must be accurate well beyond the update test.
     polish_eta: float = 1e-10
+    # GPU-only: density floor of the relative Krylov unknowns in the
+    # polishing steps.  The update test and the forcing steps scale n and p by
+    # max(density, 1e-10), which leaves minority densities below the floor
+    # loosely converged (a forward-biased p-i-n's anode current at 1e-13 A
+    # moved by 2e-6 when re-solved floor-free); the polish scales by the
+    # density itself, so it converges them too.
+    polish_scale_floor: float = 1e-30
     # GPU-only: inexact-Newton forcing.  "adaptive" solves step k to
     # eta_k = clamp(0.1 * update_{k-1}, linsolve_rtol, eta_max) (quadratic
     # convergence is kept; the converged state is the same); "fixed" solves
