@@ -86,12 +86,12 @@ class NewtonOptions:
     # state after the last step must be accurate well beyond the update test.
     polish_eta: float = 1e-10
     # GPU-only: density floor of the relative Krylov unknowns in the
-    # polishing steps.  The update test and the forcing steps scale n and p by
-    # max(density, 1e-10), which leaves minority densities below the floor
-    # loosely converged (a forward-biased p-i-n's anode current at 1e-13 A
-    # moved by 2e-6 when re-solved floor-free); the polish scales by the
-    # density itself, so it converges them too.
-    polish_scale_floor: float = 1e-30
+    # polishing steps (0: krylov_scale_floor).  Measured, a floor far below
+    # the densities (1e-30) is not more accurate: it moved one anode current
+    # of the 8.4M-node p-i-n (1.2e-13 A) onto the plain path's, but put the
+    # 600-node p-i-n's 0.5 V current 1.4e-6 from the exact-Newton oracle,
+    # which the default meets.  Off by default.
+    polish_scale_floor: float = 0.0
     # GPU-only: inexact-Newton forcing.  "adaptive" solves step k to
     # eta_k = clamp(0.1 * update_{k-1}, linsolve_rtol, eta_max) (quadratic
     # convergence is kept; the converged state is the same); "fixed" solves

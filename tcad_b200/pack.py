@@ -680,7 +680,7 @@ class Pack:
         # solve fails, 3D packs keep node-block Jacobi
         o.precond = {"ilu": 1, "auto": 2, "schur": 2}.get(pc, 0)
         o.polish_eta = float(getattr(opts, "polish_eta", 1e-10))
-        o.polish_scale_floor = float(getattr(opts, "polish_scale_floor", 1e-30))
+        o.polish_scale_floor = float(getattr(opts, "polish_scale_floor", 0.0))
         return o
 
     def set_tile_z(self, tile_z):
