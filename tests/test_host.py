@@ -84,6 +84,43 @@ def test_library_exports_every_header_symbol():
     assert lib.tcad_pack_sizeof() == ctypes.sizeof(_lib.TcadPack)
 
 
+def _header_struct_fields(tag):
+    """Field names of `typedef struct <tag> { ... }` in the header, in order
+    (array fields by their name)."""
+    src = open(os.path.join(ROOT, "include", "tcad_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    body = re.search(r"typedef struct " + tag + r"\s*\{(.*?)\}", src, flags=re.S).group(1)
+    names = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if decl:
+            names.append(re.search(r"(\w+)\s*(\[\d+\])?$", decl).group(1))
+    return names
+
+
+@pytest.mark.parametrize("tag,cls", [("tcad_pack", "TcadPack"),
+                                     ("tcad_newton_opts", "NewtonOpts"),
+                                     ("tcad_newton_result", "NewtonResult")])
+def test_ctypes_structs_mirror_the_header(tag, cls):
+    """The ctypes mirrors list the header's fields in the header's order (a
+    field added on one side only would shift every later one)."""
+    from tcad_b200 import _lib
+    assert [f[0] for f in getattr(_lib, cls)._fields_] == _header_struct_fields(tag)
+
+
+def test_tile_depth_prior():
+    """The starting 3D tile depth: the deeper of 4 and 2 planes that fills 4
+    waves of 3 CTAs on 148 SMs, else 1 (2D: 1)."""
+    from types import SimpleNamespace as NS
+    from tcad_b200.pack import choose_tile_z
+    mesh = lambda *nax: NS(nax=nax)  # noqa: E731
+    assert choose_tile_z([mesh(160, 96, 64)], 3) == 2        # 960 tiles at 4, 1,920 at 2
+    assert choose_tile_z([mesh(256, 256, 128)], 3) == 4      # 8,192 tiles at 4
+    assert choose_tile_z([mesh(40, 24, 20)], 3) == 1
+    assert choose_tile_z([mesh(160, 96, 64)] * 2, 3) == 4    # a pack of two: 1,920 at 4
+    assert choose_tile_z([mesh(512, 256)], 2) == 1
+
+
 def test_product_does_not_import_oracle():
     for dirpath, _, files in os.walk(os.path.join(ROOT, "tcad_b200")):
         for f in files:
