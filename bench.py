@@ -8,10 +8,14 @@ faces; Id-Vg sweep Vg = 0..1.0 V in 21 steps at Vd = 0.05 V and at 0.7 V,
 each sweep warm-started from equilibrium.  Synthetic device (no dataset).
 
 One step = one bias point (warm-started Newton + terminal current).  A point
-counts only when Newton converged (update < 1e-8 plus the polishing step).
+counts only when Newton converged (update < 1e-8 plus the polishing step)
+and its current is within 1e-6 of the reference current: the plain FP64
+path's state at that point, solved on untimed to the oracle fixtures'
+setting (update test 1e-12, Krylov at 1e-10 in relative unknowns).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload trigate3d|diode2d] [--small]
+                  [--workload trigate3d|diode2d|pin3d|mosfet2d_batch|serve]
+                  [--method fp64|mixed|plain] [--small] [--kernels]
 
 N > 1: one process per GPU under torchrun, each an independent replica of the
 sweep (the path does not shard: replicas only); value = all ranks' points /
