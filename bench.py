@@ -304,6 +304,18 @@ def timed_points(torch, runner, steps, e2e, ref_currents=None):
     return lat, lat_e2e, conv, h2d, d2h
 
 
+def reduce_over_ranks(dist, device, t_dev, t_e2e, ok_pts):
+    """Whole-job figures of independent replicas: the slowest rank's device
+    and end-to-end times, and the points all ranks counted.  Every rank calls
+    it once, at the same place (two all-reduces, MAX then SUM)."""
+    import torch
+    tt = torch.tensor([t_dev, t_e2e], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    cc = torch.tensor([ok_pts], device=device, dtype=torch.float64)
+    dist.all_reduce(cc, op=dist.ReduceOp.SUM)
+    return float(tt[0]), float(tt[1]), int(cc.item())
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -363,12 +375,7 @@ def run_ours(args):
         plain_counts = ([r["iters"] for r in pts_chosen], [r["krylov_iters"] for r in pts_chosen])
 
     if world > 1:
-        tt = torch.tensor([t_dev, t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = float(tt[0]), float(tt[1])
-        cc = torch.tensor([ok_pts], device="cuda", dtype=torch.float64)
-        dist.all_reduce(cc, op=dist.ReduceOp.SUM)
-        ok_all = int(cc.item())
+        t_dev, t_e2e, ok_all = reduce_over_ranks(dist, "cuda", t_dev, t_e2e, ok_pts)
     else:
         ok_all = ok_pts
 
