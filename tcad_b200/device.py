@@ -213,6 +213,24 @@ class _Device:
                           f"{res['relres']:.1e})")
         return self
 
+    def save_state(self):
+        """A copy of the solution state (the GPU psi/n/p and the sweep history
+        the predictor uses), for restore_state."""
+        pk = self.pack
+        return dict(psi=pk.psi.clone(), n=pk.n.clone(), p=pk.p.clone(),
+                    have=self._have_state, prev=self._bias_prev, cur=self._bias_cur)
+
+    def restore_state(self, st):
+        """Put back a state taken by save_state (e.g. the last converged one
+        after a failed solve, which leaves its diverged iterate behind)."""
+        pk = self.pack
+        pk.psi.copy_(st["psi"])
+        pk.n.copy_(st["n"])
+        pk.p.copy_(st["p"])
+        self._have_state = st["have"]
+        self._bias_prev, self._bias_cur = st["prev"], st["cur"]
+        self._host.clear()
+
     def terminal_current(self, name):
         """Total current into a contact from the raw continuity residual at its
         nodes: A/cm (2D) or A (3D) (pytcad/device2d.py:2194-2227,
