@@ -317,6 +317,22 @@ typedef struct tcad_newton_opts {
   double polish_scale_floor; /* density_scaling: floor of s in the polishing steps (<= 0:
                                 scale_floor); a floor far below the densities lets the
                                 polish resolve sub-floor minority densities */
+  /* One time step of the theta scheme (pytcad/transient2d.py:104-135,
+   * transient3d.py): dt > 0 adds, at every non-contact node, the storage
+   * term to the continuity rows after each assembly --
+   *   F_n <- theta F_n + (1 - theta) fn_old - dV/dt (n - n_old)
+   *   F_p <- theta F_p + (1 - theta) fp_old + dV/dt (p - p_old)
+   * with the n and p rows of J scaled by theta and their diagonal entries
+   * moved by -dV/dt and +dV/dt.  dt is in the device's scaled time
+   * (seconds * R0 / Ns); the arrays are [n_nodes], device memory; fn_old and
+   * fp_old (raw continuity residuals at the previous time) are read only
+   * when theta != 1.  dt = 0: a steady solve. */
+  double dt;
+  double theta;
+  const double* n_old;
+  const double* p_old;
+  const double* fn_old;
+  const double* fp_old;
 } tcad_newton_opts_t;
 
 /* Per-instance result of a Newton solve (host memory). */

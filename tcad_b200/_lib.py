@@ -62,7 +62,9 @@ class NewtonOpts(ctypes.Structure):
                 ("precision", ctypes.c_int32),
                 ("density_scaling", ctypes.c_int32), ("precond", ctypes.c_int32),
                 ("eta_min", ctypes.c_double), ("scale_floor", ctypes.c_double),
-                ("polish_eta", ctypes.c_double), ("polish_scale_floor", ctypes.c_double)]
+                ("polish_eta", ctypes.c_double), ("polish_scale_floor", ctypes.c_double),
+                ("dt", ctypes.c_double), ("theta", ctypes.c_double),
+                ("n_old", _p), ("p_old", _p), ("fn_old", _p), ("fp_old", _p)]
 
 
 class NewtonResult(ctypes.Structure):

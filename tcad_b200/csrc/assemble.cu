@@ -471,6 +471,74 @@ k_poisson_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Theta-scheme storage term of one time step (pytcad/transient2d.py:104-135):
+// at every non-contact node, on the assembled continuity rows,
+//   F_n <- theta F_n + (1 - theta) fn_old - dV/dt (n - n_old)
+//   F_p <- theta F_p + (1 - theta) fp_old + dV/dt (p - p_old)
+// the n and p rows of J (diagonal-block rows 1 and 2, neighbour entries
+// m = 1..4) scaled by theta, then J[n,n] += -dV/dt, J[p,p] += dV/dt.  The
+// Poisson row and the contact rows are left as assembled.  Same operation
+// order as the reference (this unit rounds step by step, -fmad=false).
+template <int DIM>
+__global__ void __launch_bounds__(kFlatThreads)
+k_storage(const tcad_pack_t pk, const double* __restrict__ nn, const double* __restrict__ pp,
+          const double* __restrict__ n_old, const double* __restrict__ p_old,
+          const double* __restrict__ fn_old, const double* __restrict__ fp_old, double dt,
+          double theta, double* __restrict__ F, double* __restrict__ J,
+          const int32_t* __restrict__ blk) {
+  const FlatBlock fb = flat_block(pk, blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x);
+  const Inst g = load_inst(pk, fb.inst);
+  const int64_t sxy = (int64_t)g.nx * g.ny;
+  const int64_t ax0 = pk.axis_off[3 * fb.inst], ay0 = pk.axis_off[3 * fb.inst + 1];
+  const int64_t az0 = pk.axis_off[3 * fb.inst + 2];
+  const int64_t NN = pk.n_nodes;
+  constexpr int NE = DIM == 2 ? TCAD_NE2 : TCAD_NE3;
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += kFlatThreads) {
+    if (pk.bcflag[k] & TCAD_BC_CONTACT) continue;
+    const int64_t loc = k - fb.ioff;
+    const int i = (int)(loc % g.nx), j = (int)((loc / g.nx) % g.ny);
+    const int kz = DIM == 3 ? (int)(loc / sxy) : 0;
+    const double dvx = pk.dv[0][ax0 + i], dvy = pk.dv[1][ay0 + j];
+    const double dvz = DIM == 3 ? pk.dv[2][az0 + kz] : 1.0;
+    const double dV = DIM == 2 ? dvy * dvx : (dvz * dvy) * dvx;
+    double f1 = F[NN + k], f2 = F[2 * NN + k];
+    if (theta != 1.0) {
+      f1 = theta * f1 + (1.0 - theta) * fn_old[k];
+      f2 = theta * f2 + (1.0 - theta) * fp_old[k];
+#pragma unroll
+      for (int e = 3; e < 9; ++e) J[(int64_t)e * NN + k] = theta * J[(int64_t)e * NN + k];
+#pragma unroll
+      for (int e = 9; e < NE; ++e)
+        if ((e - 9) % 5 != 0) J[(int64_t)e * NN + k] = theta * J[(int64_t)e * NN + k];
+    }
+    const double c = dV / dt;
+    F[NN + k] = f1 - c * (nn[k] - n_old[k]);
+    F[2 * NN + k] = f2 + c * (pp[k] - p_old[k]);
+    J[(int64_t)4 * NN + k] = J[(int64_t)4 * NN + k] + (-c);
+    J[(int64_t)8 * NN + k] = J[(int64_t)8 * NN + k] + c;
+  }
+}
+
+int storage_terms(const tcad_pack_t* pk, const double* n, const double* p,
+                  const double* n_old, const double* p_old, const double* fn_old,
+                  const double* fp_old, double dt, double theta, double* F, double* J,
+                  const int32_t* blk, int64_t n_list, cudaStream_t s) {
+  if (!pack_ok(pk) || !(dt > 0.0) || !n_old || !p_old) return TCAD_ERR_ARG;
+  if (theta != 1.0 && (!fn_old || !fp_old)) return TCAD_ERR_ARG;
+  const unsigned nb = (unsigned)(blk ? n_list : pk->n_flat);
+  if (nb == 0) return TCAD_OK;
+  if (pk->dim == 2)
+    k_storage<2><<<nb, kFlatThreads, 0, s>>>(*pk, n, p, n_old, p_old, fn_old, fp_old, dt, theta,
+                                             F, J, blk);
+  else
+    k_storage<3><<<nb, kFlatThreads, 0, s>>>(*pk, n, p, n_old, p_old, fn_old, fp_old, dt, theta,
+                                             F, J, blk);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
 int sg_assemble_tiles(const tcad_pack_t* pk, const double* psi, const double* n,
                       const double* p, double* F, double* J, int mode, const int32_t* tiles,
                       int64_t n_list, cudaStream_t s) {

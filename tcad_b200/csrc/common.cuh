@@ -108,4 +108,11 @@ int sg_assemble_tiles(const tcad_pack_t* pk, const double* psi, const double* n,
                       const double* p, double* F, double* J, int mode, const int32_t* tiles,
                       int64_t n_list, cudaStream_t s);
 
+// Theta-scheme storage term of a time step on the assembled rows, over a list
+// of flat blocks (nullptr: all n_flat).
+int storage_terms(const tcad_pack_t* pk, const double* n, const double* p,
+                  const double* n_old, const double* p_old, const double* fn_old,
+                  const double* fp_old, double dt, double theta, double* F, double* J,
+                  const int32_t* blk, int64_t n_list, cudaStream_t s);
+
 }  // namespace tcad

@@ -1821,6 +1821,11 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
     }
     int rc = sg_assemble_tiles(pk, psi, n, p, F, J, TCAD_MODE_ELIMINATE, tl, ntl, s);
     if (rc != TCAD_OK) return rc;
+    if (opts->dt > 0.0) {  // one step of the theta scheme: storage term
+      rc = storage_terms(pk, n, p, opts->n_old, opts->p_old, opts->fn_old, opts->fp_old,
+                         opts->dt, opts->theta, F, J, fl, nfl, s);
+      if (rc != TCAD_OK) return rc;
+    }
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int32_t) * ni, s));
     // density floor of each instance's relative unknowns: the polishing
     // steps use their own (far below the densities), the others sfloor

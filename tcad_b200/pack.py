@@ -701,7 +701,10 @@ class Pack:
         if wb > self.work.numel():
             self.work = self.torch.empty(wb, dtype=self.torch.uint8, device=self.device)
 
-    def newton(self, opts, active=None):
+    def newton(self, opts, active=None, transient=None):
+        """Coupled Newton on every (active) instance; `transient` = {dt (scaled
+        time), theta, n_old, p_old[, fn_old, fp_old]} (device tensors) makes
+        it one step of the theta scheme (tcad_newton_opts_t.dt)."""
         ni = len(self.setups)
         if self.autotune and self.dim == 3 and not getattr(self, "_tuned", False):
             from . import tune
@@ -712,6 +715,14 @@ class Pack:
         else:
             self.active.copy_(self.torch.as_tensor(np.asarray(active, np.uint8)))
         o = self.newton_opts(opts)
+        if transient is not None:
+            o.dt = float(transient["dt"])
+            o.theta = float(transient.get("theta", 1.0))
+            o.n_old = transient["n_old"].data_ptr()
+            o.p_old = transient["p_old"].data_ptr()
+            for f in ("fn_old", "fp_old"):
+                t = transient.get(f)
+                setattr(o, f, t.data_ptr() if t is not None else None)
         res = (_lib.NewtonResult * ni)()
         rc = self.lib.tcad_newton_solve(
             self.pref, _lib.ptr(self.psi), _lib.ptr(self.n), _lib.ptr(self.p),

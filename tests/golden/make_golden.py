@@ -305,6 +305,42 @@ def diode_c1(pt, out, nx=201, ny=101, vmax=0.70):
     np.savez_compressed(out, **_dump_dev(dev, 2, extra))
 
 
+def transient_small(pt, out, nx=41, ny=11):
+    """pytcad.transient2d.solve_transient on the 41x11 diode of diode_small:
+    from equilibrium, the anode stepped to 0.3 V at t = 0, 20 fixed steps of
+    10 ps (growth 1), backward Euler and Crank-Nicolson (theta 0.5); the
+    per-step terminal currents of both contacts and the final states."""
+    from pytcad.device2d import Device2D
+    from pytcad.mesh2d import Mesh2D
+    from pytcad.device import Models, NewtonOptions
+    from pytcad.materials import Semiconductor
+    from pytcad.transient import StepWaveform
+    from pytcad.transient2d import solve_transient
+    x = diode_x(nx)
+    y = np.linspace(0.0, 1.0e-4, ny)
+    dop = np.where(np.meshgrid(x, y)[0] < 1.0e-4, -1e17, 1e18)
+    mat = Semiconductor(tau_n0=1e-7, tau_p0=1e-7, tau_Nref=1e300)
+    mdl = Models(doping_mobility=False, srh=True, auger=False, bgn=False)
+    opts = NewtonOptions(linsolve="direct", tol_update=SWEEP_TOL)
+    dt0, t_end = 1e-11, 2e-10
+    extra = dict(dt0=dt0, t_end=t_end, v_step=0.3, tol_update=SWEEP_TOL, mat_tau=1e-7)
+    dev = None
+    for tag, theta in (("be", 1.0), ("cn", 0.5)):
+        dev = Device2D(Mesh2D(x, y), dop, material=mat, models=mdl)
+        dev.add_contact("anode", i=np.zeros(ny, int), j=np.arange(ny))
+        dev.add_contact("cathode", i=np.full(ny, nx - 1), j=np.arange(ny))
+        dev.solve_equilibrium(opts)
+        r = solve_transient(dev, {"anode": StepWaveform(0.0, 0.3, 0.0)}, t_end, dt0,
+                            theta=theta, opts=opts, growth=1.0)
+        extra[tag + "_t"] = np.array(r.times)
+        extra[tag + "_Ia"] = np.array(r.terminal_current["anode"])
+        extra[tag + "_Ic"] = np.array(r.terminal_current["cathode"])
+        extra[tag + "_psi"] = dev.psi.ravel().copy()
+        extra[tag + "_n"] = dev.n.ravel().copy()
+        extra[tag + "_p"] = dev.p.ravel().copy()
+    np.savez_compressed(out, **_dump_dev(dev, 2, extra))
+
+
 def diode_x(nx, L=2.0e-4, xj=1.0e-4, ratio=1.05):
     """nx nodes on [0, L], cell widths a symmetric geometric series growing by
     `ratio` away from xj on both sides (nx odd puts a node at xj)."""
@@ -407,6 +443,7 @@ def main():
     jobs = [("elem", elem), ("asm2d", asm2d), ("asm3d", asm3d),
             ("mosfet_small", mosfet_small), ("trigate_small", trigate_small),
             ("diode_small", lambda pt, out: diode_c1(pt, out, nx=41, ny=11)),
+            ("transient_small", transient_small),
             ("diode_c1", diode_c1)]
     for name, fn in jobs:
         if a.only and name not in a.only.split(","):
