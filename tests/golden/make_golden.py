@@ -341,6 +341,45 @@ def transient_small(pt, out, nx=41, ny=11):
     np.savez_compressed(out, **_dump_dev(dev, 2, extra))
 
 
+def transient3d_small(pt, out, nx=21, ny=5, nz=4):
+    """pytcad.transient3d.solve_transient on a small 3D diode (x graded as the
+    2D diode's, 1 um x 0.4 um x 0.3 um, N_A 1e17 | N_D 1e18, constant
+    lifetimes): the anode stepped to 0.3 V at t = 0, 40 fixed steps of
+    0.5 ps (at 10 ps the reference's own Newton fails and halves the step),
+    backward Euler and Crank-Nicolson."""
+    from pytcad.device3d import Device3D
+    from pytcad.mesh3d import Mesh3D
+    from pytcad.device import Models, NewtonOptions
+    from pytcad.materials import Semiconductor
+    from pytcad.transient import StepWaveform
+    from pytcad.transient3d import solve_transient
+    x = diode_x(nx)
+    y = np.linspace(0.0, 0.4e-4, ny)
+    z = np.linspace(0.0, 0.3e-4, nz)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    dop = np.where(X < 1.0e-4, -1e17, 1e18)
+    mat = Semiconductor(tau_n0=1e-7, tau_p0=1e-7, tau_Nref=1e300)
+    mdl = Models(doping_mobility=False, srh=True, auger=False, bgn=False)
+    opts = NewtonOptions(linsolve="direct", tol_update=SWEEP_TOL)
+    dt0, t_end = 5e-13, 2e-11
+    extra = dict(dt0=dt0, t_end=t_end, v_step=0.3, tol_update=SWEEP_TOL, mat_tau=1e-7)
+    dev = None
+    J, K = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
+    for tag, theta in (("be", 1.0), ("cn", 0.5)):
+        dev = Device3D(Mesh3D(x, y, z), dop, material=mat, models=mdl)
+        dev.add_contact("anode", np.zeros(J.size, int), J.ravel(), K.ravel())
+        dev.add_contact("cathode", np.full(J.size, nx - 1), J.ravel(), K.ravel())
+        dev.solve_equilibrium(opts)
+        r = solve_transient(dev, {"anode": StepWaveform(0.0, 0.3, 0.0)}, t_end, dt0,
+                            theta=theta, opts=opts, growth=1.0)
+        assert len(r.times) == 41, "the reference's Newton cut a step"
+        extra[tag + "_t"] = np.array(r.times)
+        extra[tag + "_Ia"] = np.array(r.terminal_current["anode"])
+        extra[tag + "_Ic"] = np.array(r.terminal_current["cathode"])
+        extra[tag + "_psi"] = dev.psi.ravel().copy()
+    np.savez_compressed(out, **_dump_dev(dev, 3, extra))
+
+
 def diode_x(nx, L=2.0e-4, xj=1.0e-4, ratio=1.05):
     """nx nodes on [0, L], cell widths a symmetric geometric series growing by
     `ratio` away from xj on both sides (nx odd puts a node at xj)."""
@@ -444,6 +483,7 @@ def main():
             ("mosfet_small", mosfet_small), ("trigate_small", trigate_small),
             ("diode_small", lambda pt, out: diode_c1(pt, out, nx=41, ny=11)),
             ("transient_small", transient_small),
+            ("transient3d_small", transient3d_small),
             ("diode_c1", diode_c1)]
     for name, fn in jobs:
         if a.only and name not in a.only.split(","):

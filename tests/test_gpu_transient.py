@@ -1,8 +1,10 @@
 """The theta-scheme time stepping (tcad_b200.transient, storage term in the
 GPU Newton) against the reference's own solve_transient run
-(pytcad/transient2d.py, fixture transient_small): the 41x11 diode stepped to
-0.3 V, 20 fixed steps of 10 ps, backward Euler and Crank-Nicolson, Newton
-to the fixture's update tolerance (1e-12).  Every step's terminal currents
+(pytcad/transient2d.py, fixture transient_small: the 41x11 diode stepped to
+0.3 V, 20 fixed steps of 10 ps; pytcad/transient3d.py, fixture
+transient3d_small: a 21x5x4 diode, 40 steps of 0.5 ps), backward Euler and
+Crank-Nicolson, Newton to the fixture's update tolerance (1e-12).  Every
+step's terminal currents
 within 1e-6 of max(|I|, 1e-7 x the run's peak current): the step response
 falls five decades (0.28 A/cm to 1.6 nA/cm), and in its tail the two
 contacts' currents differ by ~1e-13 A/cm, where the sub-floor minority
@@ -17,11 +19,12 @@ import fixtures as fx
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("name", ["transient_small", "transient3d_small"])
 @pytest.mark.parametrize("tag,theta", [("be", 1.0), ("cn", 0.5)])
-def test_transient_matches_reference(tag, theta):
+def test_transient_matches_reference(name, tag, theta):
     import tcad_b200 as tb
     from tcad_b200.transient import StepWaveform, solve_transient
-    g = fx.load("transient_small")
+    g = fx.load(name)
     opts = tb.NewtonOptions(tol_update=float(g["tol_update"]))   # the fixture's own setting
     dev = fx.gpu_device(g, material=dict(tau_n0=1e-7, tau_p0=1e-7, tau_Nref=1e300))
     dev.solve_equilibrium()
