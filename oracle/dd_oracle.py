@@ -13,7 +13,8 @@ Reference files (paths relative to the reference's ``pytcad/``):
   442-518, mesh2d.py:15-27, contacts.py:21-38, dirichlet.py:270-300,
   linsolve.py:363-427,941-985, device2d.py:168-453,676-759,844-942,
   1308-1373,1402-2227, device3d.py:190-258,320-408,437-724,774-947,
-  952-1020,1311-1454,1485-2306, moscap.py:60-90.
+  952-1020,1311-1454,1485-2306, moscap.py:60-90, transient2d.py:94-330,
+  transient3d.py:108-380.
 """
 from __future__ import annotations
 
@@ -616,6 +617,138 @@ class OracleDevice:
         self.last_converged = converged
         self.psi, self.n, self.p = psi, n, p
         return self
+
+    # -- transient: theta scheme (transient2d.py:94-330, transient3d.py:108-380)
+    def _free_nodes(self):
+        mask = np.zeros(self.N, dtype=bool)
+        for k, _ in self.contacts.values():
+            mask[np.asarray(k)] = True
+        return np.arange(self.N)[~mask]
+
+    def _step_residual_jacobian(self, psi, n, p, volts, n_old, p_old, Fn_old, Fp_old,
+                                dt_s, theta, k_free):
+        """transient2d.py:104-135: the storage term on the non-contact
+        continuity rows, theta-weighted with the previous time's residual."""
+        F_new, J_new, _, _ = self.residual_jacobian(psi, n, p, volts)
+        F = F_new.copy()
+        idx_n = 3 * k_free + 1
+        idx_p = 3 * k_free + 2
+        dVi = self.dV.ravel()[k_free]
+        nf, pf = np.asarray(n).ravel()[k_free], np.asarray(p).ravel()[k_free]
+        n0f, p0f = np.asarray(n_old).ravel()[k_free], np.asarray(p_old).ravel()[k_free]
+        if theta != 1.0:
+            F[idx_n] = theta * F[idx_n] + (1.0 - theta) * Fn_old.ravel()[k_free]
+            F[idx_p] = theta * F[idx_p] + (1.0 - theta) * Fp_old.ravel()[k_free]
+            row_scale = np.ones(F.shape[0])
+            row_scale[idx_n] = theta
+            row_scale[idx_p] = theta
+            J = sp.diags(row_scale) @ J_new
+        else:
+            J = J_new
+        F[idx_n] -= dVi / dt_s * (nf - n0f)
+        F[idx_p] += dVi / dt_s * (pf - p0f)
+        rows = np.concatenate([idx_n, idx_p])
+        vals = np.concatenate([-dVi / dt_s, dVi / dt_s])
+        J = J + sp.csr_matrix((vals, (rows, rows)), shape=J.shape)
+        return F, J
+
+    def _transient_newton(self, psi0, n0, p0, volts, Fn_old, Fp_old, dt_s, theta, k_free,
+                          max_iter, tol, max_dpsi):
+        """transient2d.py:138-183: Newton with exact (direct) steps and a
+        backtracking line search on 0.5 |F|^2, densities clipped to
+        [0.1, 10] x per step, stopped on the update test."""
+        sh = self.shape
+        psi, n, p = psi0.copy(), n0.copy(), p0.copy()
+        args = (volts, n0, p0, Fn_old, Fp_old, dt_s, theta, k_free)
+        for it in range(max_iter):
+            F, J = self._step_residual_jacobian(psi, n, p, *args)
+            du = spsolve(J.tocsc(), -F)
+            dpsi = np.clip(du[0::3].reshape(sh), -max_dpsi, max_dpsi)
+            dn = du[1::3].reshape(sh)
+            dp = du[2::3].reshape(sh)
+            base = 0.5 * float(np.dot(F, F))
+            lam = 1.0
+            for _ in range(40):
+                psi_t = psi + lam * dpsi
+                n_t = np.clip(n + lam * dn, 0.1 * n, 10.0 * n)
+                p_t = np.clip(p + lam * dp, 0.1 * p, 10.0 * p)
+                Ft, _ = self._step_residual_jacobian(psi_t, n_t, p_t, *args)
+                merit = 0.5 * float(np.dot(Ft, Ft))
+                if np.isfinite(merit) and merit <= base * (1.0 - 1e-4 * lam):
+                    break
+                lam *= 0.5
+            else:
+                lam = 0.0
+            n_prev, p_prev = n, p
+            psi = psi + lam * dpsi
+            n = np.clip(n + lam * dn, 0.1 * n, 10.0 * n)
+            p = np.clip(p + lam * dp, 0.1 * p, 10.0 * p)
+            rel_n = (np.abs(n - n_prev) / np.maximum(n_prev, 1e-10)).max()
+            rel_p = (np.abs(p - p_prev) / np.maximum(p_prev, 1e-10)).max()
+            err = max(float(np.abs(dpsi).max()), float(rel_n), float(rel_p))
+            if err < tol:
+                return psi, n, p, True, it + 1
+        return psi, n, p, False, max_iter
+
+    def _current_at(self, psi, n, p, name):
+        k, _ = self.contacts[name]
+        cur = {nm: V for nm, (kk, V) in self.contacts.items()}
+        *_, F_n, F_p = self.residual_jacobian(psi, n, p, cur)
+        scale = self.J0 * self.LD if self.dim == 2 else self.J0 * self.LD ** 2
+        return float((F_n.ravel()[k] + F_p.ravel()[k]).sum()) * scale
+
+    def solve_transient(self, waveforms, t_end, dt0, theta=1.0, max_iter=100, tol=1e-8,
+                        max_dpsi=5.0, dt_min=None, dt_max=None, growth=1.5, shrink=0.5):
+        """transient2d.py:186-330 / transient3d.py:234-380 from the current
+        state: waveforms {contact: object with .value(t), function of t, or
+        volts}.  Returns
+        {"times", "currents": {contact: [...]}} and leaves the final state."""
+        def wv(w, t):   # a waveform object, a function of t, or a constant
+            return w.value(t) if hasattr(w, "value") else (w(t) if callable(w) else float(w))
+        names = list(self.contacts)
+
+        def volts_at(t):
+            return {nm: (wv(waveforms[nm], t) if nm in waveforms else self.contacts[nm][1])
+                    for nm in names}
+
+        k_free = self._free_nodes()
+        t0 = self.Ns / self.R0
+        dt_s = dt0 / t0
+        dt_min_s = (dt_min if dt_min is not None else dt0 / 1024.0) / t0
+        dt_max_s = (dt_max if dt_max is not None else dt0 * 64.0) / t0
+        t = 0.0
+        psi, n, p = self.psi.copy(), self.n.copy(), self.p.copy()
+        times = [t]
+        currents = {nm: [self._current_at(psi, n, p, nm)] for nm in names}
+        while t < t_end - 1e-15:
+            step_dt_s = dt_s
+            t_new = t + step_dt_s * t0
+            if t_new > t_end:
+                t_new = t_end
+                step_dt_s = (t_new - t) / t0
+            volts = volts_at(t_new)
+            Fn_old = Fp_old = None
+            if theta != 1.0:
+                *_, Fn_old, Fp_old = self.residual_jacobian(psi, n, p, volts_at(t))
+            for nm, V in volts.items():
+                self.contacts[nm][1] = float(V)
+            psi_n, n_n, p_n, ok, iters = self._transient_newton(
+                psi, n, p, volts, Fn_old, Fp_old, step_dt_s, theta, k_free, max_iter, tol,
+                max_dpsi)
+            if ok:
+                t = t_new
+                psi, n, p = psi_n, n_n, p_n
+                times.append(t)
+                for nm in names:
+                    currents[nm].append(self._current_at(psi, n, p, nm))
+                dt_s = min(step_dt_s * growth, dt_max_s) \
+                    if iters <= max(3, max_iter // 4) else step_dt_s
+            else:
+                dt_s = step_dt_s * shrink
+                if dt_s < dt_min_s:
+                    raise RuntimeError(f"oracle transient stalled at t={t:.3e}s")
+        self.psi, self.n, self.p = psi, n, p
+        return {"times": np.array(times), "currents": {k: np.array(v) for k, v in currents.items()}}
 
     def terminal_current(self, name):
         """device2d.py:2194-2227 (A/cm) / device3d.py:2274-2306 (A)."""

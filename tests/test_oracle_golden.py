@@ -117,3 +117,24 @@ def test_diode_c1_equilibrium():
                                             tau_Nref=1e300))
     dev.solve_equilibrium()
     assert np.abs(dev.psi.ravel() - g["psi_eq"]).max() * dev.VT < 1e-9
+
+
+@pytest.mark.parametrize("name", ["transient_small", "transient3d_small"])
+@pytest.mark.parametrize("tag,theta", [("be", 1.0), ("cn", 0.5)])
+def test_transient_matches_reference(name, tag, theta):
+    """The oracle's theta-scheme time stepping against the reference's own
+    solve_transient run (transient2d.py / transient3d.py)."""
+    g = fx.load(name)
+    dev = fx.oracle_device(g, material=dict(tau_n0=1e-7, tau_p0=1e-7, tau_Nref=1e300))
+    tol = float(g["tol_update"])
+    dev.solve_equilibrium(tol=tol)
+    v = float(g["v_step"])
+    r = dev.solve_transient({"anode": (lambda t: v if t >= 0.0 else 0.0)},
+                            float(g["t_end"]), float(g["dt0"]), theta=theta, tol=tol,
+                            growth=1.0)
+    assert np.array_equal(r["times"], g[tag + "_t"])
+    for c, key in (("anode", "_Ia"), ("cathode", "_Ic")):
+        I, Iref = r["currents"][c], g[tag + key]
+        err = np.abs(I - Iref) / np.maximum(np.abs(Iref), 1e-7 * np.abs(Iref).max())
+        assert err.max() < 1e-9, (c, float(err.max()), int(err.argmax()))
+    assert np.abs(dev.psi.ravel() - g[tag + "_psi"]).max() * dev.VT < 1e-12
