@@ -153,6 +153,19 @@ int tcad_edge_currents(const tcad_pack_t* pk, int axis, const double* psi,
 int tcad_poisson_assemble(const tcad_pack_t* pk, const double* psi, double* F,
                           double* J, int mode, void* stream);
 
+/* Elementwise SG device functions, compiled in the assembly's unit with the
+ * assembly's rounding, for elementwise parity checks.
+ * tcad_eval_bernoulli: out[4*count] = B(x), B(-x), B'(x), B'(-x) blocks of
+ * count each -- pytcad/kernels.py:88-109 bernoulli / dbernoulli.
+ * tcad_eval_recombination: out[3*count] = Rs, dRs/dn, dRs/dp blocks with
+ * the per-instance parameters par[TCAD_NPAR] (Ns, R0, Cn, Cp, SRH, AUGER) --
+ * pytcad/materials.py:474-518 recombination, scaled as
+ * pytcad/device2d.py:1482-1508 (Ns = R0 = 1 gives the physical rates). */
+int tcad_eval_bernoulli(const double* x, int64_t count, double* out, void* stream);
+int tcad_eval_recombination(const double* n, const double* p, const double* nie,
+                            const double* tau_n, const double* tau_p, int64_t count,
+                            const double* par, double* out, void* stream);
+
 /* ---- boundary conditions -------------------------------------------------
  * Contact targets at the current bias (contacts.ohmic_values,
  * pytcad/contacts.py:21-38, with psi0 = V/VT + ln(n0/nie)): for each listed

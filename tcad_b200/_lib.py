@@ -84,6 +84,9 @@ _SIGS = {
                                             ctypes.c_int64, _p, _p]),
     "tcad_edge_currents": (ctypes.c_int, [_p, ctypes.c_int, _p, _p, _p, _p, _p, _p]),
     "tcad_poisson_assemble": (ctypes.c_int, [_p, _p, _p, _p, ctypes.c_int, _p]),
+    "tcad_eval_bernoulli": (ctypes.c_int, [_p, ctypes.c_int64, _p, _p]),
+    "tcad_eval_recombination": (ctypes.c_int, [_p, _p, _p, _p, _p, ctypes.c_int64, _p, _p,
+                                               _p]),
     "tcad_block_workspace_bytes": (ctypes.c_size_t, [_p, ctypes.c_int, ctypes.c_int]),
     "tcad_set_krylov_fused": (ctypes.c_int, [ctypes.c_int]),
     "tcad_state_extrapolate": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),

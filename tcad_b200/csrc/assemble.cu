@@ -520,6 +520,36 @@ k_storage(const tcad_pack_t pk, const double* __restrict__ nn, const double* __r
   }
 }
 
+// ---------------------------------------------------------------------------
+// Elementwise evaluation of the SG device functions, compiled exactly as the
+// assembly uses them (same unit, same -fmad=false rounding): the hook the
+// elementwise parity tests read through.
+__global__ void k_eval_bernoulli(const double* __restrict__ x, int64_t count,
+                                 double* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  double Bp, Bm, dBp, dBm;
+  bern4(x[t], Bp, Bm, dBp, dBm);
+  out[t] = Bp;
+  out[count + t] = Bm;
+  out[2 * count + t] = dBp;
+  out[3 * count + t] = dBm;
+}
+
+__global__ void k_eval_recombination(const double* __restrict__ n, const double* __restrict__ p,
+                                     const double* __restrict__ nie,
+                                     const double* __restrict__ taun,
+                                     const double* __restrict__ taup, int64_t count,
+                                     const double* __restrict__ par, double* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  double Rs, dRsn, dRsp;
+  recomb(n[t], p[t], nie[t], taun[t], taup[t], par, Rs, dRsn, dRsp);
+  out[t] = Rs;
+  out[count + t] = dRsn;
+  out[2 * count + t] = dRsp;
+}
+
 int storage_terms(const tcad_pack_t* pk, const double* n, const double* p,
                   const double* n_old, const double* p_old, const double* fn_old,
                   const double* fp_old, double dt, double theta, double* F, double* J,
@@ -609,6 +639,29 @@ extern "C" int tcad_poisson_assemble(const tcad_pack_t* pk, const double* psi, d
     k_poisson_assemble<2><<<nb_, kFlatThreads, 0, s>>>(*pk, psi, F, J, mode);
   else
     k_poisson_assemble<3><<<nb_, kFlatThreads, 0, s>>>(*pk, psi, F, J, mode);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_eval_bernoulli(const double* x, int64_t count, double* out, void* stream) {
+  if (count < 0 || (count > 0 && (!x || !out))) return TCAD_ERR_ARG;
+  if (count == 0) return TCAD_OK;
+  k_eval_bernoulli<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(x, count,
+                                                                                     out);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
+extern "C" int tcad_eval_recombination(const double* n, const double* p, const double* nie,
+                                       const double* tau_n, const double* tau_p, int64_t count,
+                                       const double* par, double* out, void* stream) {
+  if (count < 0 || !par || (count > 0 && (!n || !p || !nie || !tau_n || !tau_p || !out)))
+    return TCAD_ERR_ARG;
+  if (count == 0) return TCAD_OK;
+  k_eval_recombination<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      n, p, nie, tau_n, tau_p, count, par, out);
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;

@@ -18,27 +18,43 @@ __device__ __forceinline__ void bern_series(double x, double& B, double& dB) {
   dB = (-0.5 + x / 6.0) - (x * x * x) / 180.0;
 }
 
-// B(x), B(-x), B'(x), B'(-x) with B(x) = x / expm1(x) and
-// B'(x) = B(x) (1/x - 1/(1 - e^-x)), from ONE expm1 and ONE reciprocal.
+// B(x), B(-x), B'(x), B'(-x).  Three argument bands:
 //
-// With a = |x|, e = expm1(a) > 0 and r = 1/e:
-//   S  = B(a)   = a r                    (the small side, in (0, 1))
-//   L  = B(-a)  = a e^a / (e^a - 1) = S + a
-//   dS = B'(a)  = S (1/a - (1 + r))     = r (1 - a (1 + r))
-//   dL = B'(-a) = L (r - 1/a)           = (1 + r) (S - 1)
-// (L = a (1 + r), so L / a = 1 + r and S / a = r).  Every sum adds terms
-// of one sign except the ones that are also differences of nearly equal
-// terms in the reference's own formula near the series threshold, so the
-// values agree with B(x) = x / expm1(x) evaluated at +-x to rounding.
+//   |x| < 1e-4          the reference's series (kernels.py:92-96, 105-109);
+//   1e-4 <= |x| < 1e-2  the reference's own formulas at +x and at -x
+//                       (kernels.py:88-109): B = x / expm1(x) and
+//                       B' = B (1/x - 1/(1 - e^-x)), two expm1 and the same
+//                       divisions.  Here 1/x - 1/(1 - e^-x) cancels (about
+//                       4 digits at 1e-4), so the reference's derivative
+//                       carries that cancellation's rounding; reproducing
+//                       its steps reproduces its values elementwise.
+//   |x| >= 1e-2         ONE expm1 and ONE reciprocal serve all four values.
+//                       With a = |x|, e = expm1(a) > 0 and r = 1/e:
+//                         S  = B(a)   = a r
+//                         L  = B(-a)  = a e^a / (e^a - 1) = S + a
+//                         dS = B'(a)  = S (1/a - (1 + r)) = r (1 - a (1 + r))
+//                         dL = B'(-a) = L (r - 1/a)       = (1 + r) (S - 1)
+//                       (L / a = 1 + r and S / a = r).  In this band the
+//                       values agree with the reference's formulas to a few
+//                       ulp (derivatives within 1e-13 relative; measured
+//                       over 4e5 arguments against kernels.py).
 __device__ __forceinline__ void bern4(double x, double& Bp, double& Bm, double& dBp,
                                       double& dBm) {
   x = clip700(x);
-  if (fabs(x) < 1e-4) {
+  const double a = fabs(x);
+  if (a < 1e-4) {
     bern_series(x, Bp, dBp);
     bern_series(-x, Bm, dBm);
     return;
   }
-  const double a = fabs(x);
+  if (a < 1e-2) {
+    const double ep = expm1(x), em = expm1(-x);
+    Bp = x / ep;
+    Bm = (-x) / em;
+    dBp = Bp * (1.0 / x - 1.0 / (-em));
+    dBm = Bm * (1.0 / (-x) - 1.0 / (-ep));
+    return;
+  }
   const double e = expm1(a);
   const double r = 1.0 / e;
   const double r1 = 1.0 + r;
@@ -97,7 +113,9 @@ __device__ __forceinline__ void sg_edge(double psi_lo, double psi_hi, double n_l
 }
 
 // SRH + Auger recombination, scaled (materials.py:474-518 with the
-// device's R0/Ns scaling, pytcad/device2d.py:1482-1508).
+// device's R0/Ns scaling, pytcad/device2d.py:1482-1508), with the
+// reference's divisions: R = excess / den, dR/dn = (p den - excess tau_p) /
+// den^2, Rs = R / R0, dRs/dn = dR/dn Ns / R0.
 __device__ __forceinline__ void recomb(double n, double p, double nie, double taun,
                                        double taup, const double* par, double& Rs,
                                        double& dRsn, double& dRsp) {
@@ -109,11 +127,10 @@ __device__ __forceinline__ void recomb(double n, double p, double nie, double ta
   const double nph = n * Ns, pph = p * Ns;
   const double excess = nph * pph - nie * nie;
   const double den = taup * (nph + nie) + taun * (pph + nie);
-  const double iden = 1.0 / den;   // one reciprocal for R and its derivatives
-  double R = excess * iden;
-  const double iden2 = iden * iden;
-  double dRdn = (pph * den - excess * taup) * iden2;
-  double dRdp = (nph * den - excess * taun) * iden2;
+  double R = excess / den;
+  const double den2 = den * den;
+  double dRdn = (pph * den - excess * taup) / den2;
+  double dRdp = (nph * den - excess * taun) / den2;
   if (par[TCAD_P_AUGER] != 0.0) {
     const double Cn = par[TCAD_P_CN], Cp = par[TCAD_P_CP];
     const double cc = Cn * nph + Cp * pph;
@@ -121,10 +138,9 @@ __device__ __forceinline__ void recomb(double n, double p, double nie, double ta
     dRdn = dRdn + Cn * excess + cc * pph;
     dRdp = dRdp + Cp * excess + cc * nph;
   }
-  const double iR0 = 1.0 / R0;
-  Rs = R * iR0;
-  dRsn = dRdn * Ns * iR0;
-  dRsp = dRdp * Ns * iR0;
+  Rs = R / R0;
+  dRsn = dRdn * Ns / R0;
+  dRsp = dRdp * Ns / R0;
 }
 
 }  // namespace tcad

@@ -88,6 +88,41 @@ def rownorm_err(A, B):
     return float((num / den).max())
 
 
+def elem_err(A, B, floor_rel=0.0):
+    """Elementwise max |A_ij - B_ij| / |B_ij| over B's non-zero entries that
+    are at least floor_rel x their row's largest |entry|.  A floor excludes
+    entries formed where a sum of terms may cancel; the coupled Jacobian's
+    duplicate sums add terms of one sign, so its default is 0 (every
+    entry).  Entries of A outside B's pattern must be zero.  Returns
+    (max error, entries compared)."""
+    A = A.tocsr().copy()
+    B = B.tocsr().copy()
+    for M in (A, B):
+        M.sum_duplicates()
+        M.sort_indices()
+    n = B.shape[1]
+
+    def keys(M):
+        r = np.repeat(np.arange(M.shape[0], dtype=np.int64), np.diff(M.indptr))
+        return r * n + M.indices.astype(np.int64), r
+
+    ka, _ = keys(A)
+    kb, rb = keys(B)
+    pos = np.searchsorted(ka, kb)
+    pos_c = np.minimum(pos, max(ka.size - 1, 0))
+    hit = (pos < ka.size) & (ka[pos_c] == kb) if ka.size else np.zeros(kb.size, bool)
+    av = np.where(hit, A.data[pos_c] if ka.size else 0.0, 0.0)
+    extra = np.ones(ka.size, bool)
+    extra[pos_c[hit]] = False
+    assert not np.any(A.data[extra] != 0.0), "entries outside the reference pattern"
+    absb = np.abs(B.data)
+    rowmax = np.zeros(B.shape[0])
+    np.maximum.at(rowmax, rb, absb)
+    sel = (absb >= floor_rel * rowmax[rb]) & (absb > 0)
+    err = np.abs(av - B.data)[sel] / absb[sel]
+    return (float(err.max()) if err.size else 0.0), int(sel.sum())
+
+
 def vec_err(a, b, scale=None):
     """max |a-b| / max(|b|, scale) -- scale guards entries that cancel."""
     a = np.asarray(a, dtype=float)
@@ -153,3 +188,15 @@ def oracle_from_device(dev):
         else:
             ora.gates[name] = [b.nodes.copy(), b.kappa, b.Vfb, b.Vg, b.w.copy()]
     return ora
+
+
+def field_errs(psi, n, p, psi_ref, n_ref, p_ref):
+    """(max |dpsi|, max |d phi_n|, max |d phi_p|) in scaled units (x VT for
+    volts): phi_n = psi - ln(n / nie), phi_p = psi + ln(p / nie), so the
+    n_ie of the device cancels out of the differences."""
+    psi, n, p = (np.asarray(a, float).ravel() for a in (psi, n, p))
+    psi_ref, n_ref, p_ref = (np.asarray(a, float).ravel() for a in (psi_ref, n_ref, p_ref))
+    dpsi = psi - psi_ref
+    return (float(np.abs(dpsi).max()),
+            float(np.abs(dpsi - (np.log(n) - np.log(n_ref))).max()),
+            float(np.abs(dpsi + (np.log(p) - np.log(p_ref))).max()))

@@ -1,6 +1,8 @@
 """GPU parity: the sm_100a kernels against the reference's own outputs (golden
 fixtures) and the oracle.  Tolerances (the drop-in contract): assembled
-residual / Jacobian entries within 1e-12 relative (normwise per row),
+residual / Jacobian entries within 1e-12 relative (the Jacobian both
+normwise per row and entry by entry; the residual per row, where the
+converging terms cancel),
 converged psi within 1e-9 V, terminal currents within 1e-6 relative."""
 import numpy as np
 import pytest
@@ -33,6 +35,9 @@ def test_coupled_assembly(name):
     F_n, F_p = out[-2], out[-1]
     Jref = fx.csr(g)
     assert fx.rownorm_err(J, Jref) < TOL_ASM
+    # and entry by entry, not only normwise per row
+    e_elem, n_cmp = fx.elem_err(J, Jref)
+    assert n_cmp == np.count_nonzero(Jref.data) and e_elem < TOL_ASM, (e_elem, n_cmp)
     x = np.stack([g["st_psi"], g["st_n"], g["st_p"]], axis=1).ravel()
     assert _rownorm_vec(F, Jref, x, g["F"]) < TOL_ASM
     assert np.array_equal(np.sort(dev._dirichlet_rows), np.sort(g["fixed"]))
