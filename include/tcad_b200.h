@@ -280,8 +280,10 @@ int tcad_csr_krylov(int64_t n, const int32_t* indptr, const int32_t* indices,
  * n_nodes <= TCAD_STATIC_MAX_NODES (32768) and n_inst <= TCAD_STATIC_MAX_INST
  * (32); larger packs get TCAD_ERR_ARG.  The first call on each device looks up
  * the array's device address (cudaGetSymbolAddress) with that device current;
- * make it before any stream capture.  Calls share the array: each call clears
- * what must start at zero, and calls whose work overlaps on the GPU race. */
+ * make it before any stream capture.  The looked-up address belongs to the
+ * device's context: after cudaDeviceReset, reload the library before calling
+ * this entry point again.  Calls share the array: each call clears what must
+ * start at zero, and calls whose work overlaps on the GPU race. */
 #define TCAD_STATIC_MAX_NODES 32768
 #define TCAD_STATIC_MAX_INST 32
 #define TCAD_STATIC_SCRATCH_BYTES (5u << 20)

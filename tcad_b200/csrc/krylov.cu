@@ -2125,18 +2125,23 @@ namespace tcad {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[TCAD_STATIC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
-static void* g_noalloc_addr[kMaxDevices] = {nullptr};
+// Per-device address of the array, looked up once per device.  Host threads
+// that race on the first call store the same value; the atomics make that
+// well defined.  The address belongs to the device's context: after a
+// cudaDeviceReset the library must be reloaded before this entry point is
+// used again.
+static std::atomic<void*> g_noalloc_addr[kMaxDevices];
 
 static int noalloc_scratch(void** out) {
   int dev = -1;
   TCAD_CUDA_CHECK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return TCAD_ERR_ARG;
-  if (g_noalloc_addr[dev] == nullptr) {
-    void* p = nullptr;
+  void* p = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (p == nullptr) {
     TCAD_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_addr[dev] = p;
+    g_noalloc_addr[dev].store(p, std::memory_order_release);
   }
-  *out = g_noalloc_addr[dev];
+  *out = p;
   return TCAD_OK;
 }
 
