@@ -80,3 +80,40 @@ def test_gate_bias_upload_matches_setup():
         want = d.setup.gate_arrays()[2]
         assert np.array_equal(pk.t["gate_v"].cpu().numpy(), want)
         assert pk.last_h2d_bytes < 8 * d.N / 4
+
+
+def test_batch_matches_oracle():
+    """Eight instances of the seeded 512-MOSFET batch (the smallest and
+    largest meshes, the extreme dopings, the shortest gate, the highest
+    bias) solved in ONE pack through the same 4-step ramp from equilibrium
+    as the oracle's exact-Newton run (tests/golden/mosfet_batch_oracle.npz,
+    made by tests/golden/make_oracle_sweeps.py): every instance's drain
+    current within 1e-6, psi within 1e-9 V and the quasi-Fermi levels within
+    1e-8 V at the fixture's sampled nodes."""
+    import fixtures as fx
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    from tcad_b200.batch import DeviceBatch
+    g = fx.load("mosfet_batch_oracle")
+    params = W.mosfet_batch_params(512)
+    sel = [params[int(i)] for i in g["inst"]]
+    batch = DeviceBatch([_build(q) for q in sel])
+    opts = tb.NewtonOptions()
+    batch.solve_equilibrium(opts)
+    steps = int(g["ramp"])
+    ramps = [W.ramp({"gate": q["Vg"], "drain": q["Vd"]}, steps) for q in sel]
+    for s in range(steps):
+        res = batch.solve_bias([r[s] for r in ramps], opts)
+    assert all(r["converged"] for r in res)
+    I = batch.terminal_currents("drain")
+    rel = np.abs(I - g["I_drain"]) / np.abs(g["I_drain"])
+    assert rel.max() < 1e-6, rel
+    for a in range(len(sel)):
+        idx = g["idx"][a]
+        idx = idx[idx >= 0]
+        st = [t.ravel()[idx] for t in batch.state(a)]
+        ref = g["fields"][a][:, :idx.size]
+        e_psi, e_n, e_p = fx.field_errs(*st, *ref)
+        VT = batch.devices[a].VT
+        assert e_psi * VT < 1e-9, (a, e_psi * VT)
+        assert max(e_n, e_p) * VT < 1e-8, (a, e_n * VT, e_p * VT)
