@@ -7,10 +7,14 @@ peak 1e20 cm^-3 (sigma 10 nm), 40 nm gate, 1 nm oxide Robin gates on three
 faces; Id-Vg sweep Vg = 0..1.0 V in 21 steps at Vd = 0.05 V and at 0.7 V,
 each sweep warm-started from equilibrium.  Synthetic device (no dataset).
 
-One step = one bias point (warm-started Newton + terminal current).  A point
-counts only when Newton converged (update < 1e-8 plus the polishing step)
-and its current is within 1e-6 of the reference current: the plain FP64
-path's state at that point, solved on untimed to the oracle fixtures'
+One step = one Vg on BOTH Vd branches: two warm-started bias points, solved
+as one packed 2-instance batch by the chosen path (the plain path solves the
+two branch devices one after another), + the terminal currents.  The warm-up
+steps walk the start of the schedule, then the schedule restarts, so K timed
+steps cover Vg = 0 .. 0.05 (K-1) V on both branches, equilibrium included.
+A point counts only when Newton converged (update < 1e-8 plus the polishing
+step) and its current is within 1e-6 of the reference current: the plain
+FP64 path's state at that point, solved on untimed to the oracle fixtures'
 setting (update test 1e-12, Krylov at 1e-10 in relative unknowns).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -46,6 +50,10 @@ UNIT = "bias_pts/s"
 #     an/ap/dl x 3 axes) + bcflag byte + 42 doubles out (F 3, J 39) = 465 B
 BYTES_SPMV = {2: (29 + 3 + 3) * 8, 3: (39 + 3 + 3) * 8}
 BYTES_ASM = {2: (13 + 32) * 8 + 1, 3: (16 + 42) * 8 + 1}
+#  one BiCGStab iteration in the solver (node-block layout, FP64), bytes per
+#  node of the five kernels: k_bi_p 96 (r, v, p in; p out), k_bi_v and k_bi_t
+#  one SpMV each (J + x in, y out), k_bi_s 72, k_bi_x 168
+BYTES_ITER = {d: 96 + 2 * BYTES_SPMV[d] + 72 + 168 for d in (2, 3)}
 
 # Newton iterations / BiCGStab iterations per bias point of the plain FP64
 # path on this workload, from its own bench runs; used only to scale the
@@ -190,117 +198,155 @@ class Clocks:
 
 # ---------------------------------------------------------------------------
 def build_workload(name, small, dev_cls_2d, dev_cls_3d):
+    """(lanes, steps, description, contact).  A lane is one device marching
+    through its own bias points; a step gives every lane its next point:
+    steps[q] = ([volts of lane 0, lane 1, ...], starts_from_equilibrium)."""
     from tcad_b200 import workloads as W
     if name == "pin3d":
         dims = (64, 32, 16) if small else (256, 256, 128)
-        dev = W.pin3d(dev_cls_3d, *dims)
-        sched = [({"anode": v}, i == 0) for i, v in enumerate(W.PIN_SWEEP)]
+        lanes = [W.pin3d(dev_cls_3d, *dims)]
+        steps = [([{"anode": v}], i == 0) for i, v in enumerate(W.PIN_SWEEP)]
         desc = (f"pin3d {dims[0]}x{dims[1]}x{dims[2]} ({int(np.prod(dims)):,} nodes) p+ 1e19 / "
                 "i 1e14 / n+ 1e19, 20 nm erfc transitions, SRH + Auger, forward 0..0.9 V "
                 "step 0.1")
-        return dev, sched, desc, "anode"
+        return lanes, steps, desc, "anode"
     if name == "diode2d":
         nx, ny = (41, 11) if small else (201, 101)
-        dev = W.diode2d(dev_cls_2d, nx, ny)
-        sched = [({"anode": v}, i == 0) for i, v in enumerate(W.DIODE_SWEEP)]
+        lanes = [W.diode2d(dev_cls_2d, nx, ny)]
+        steps = [([{"anode": v}], i == 0) for i, v in enumerate(W.DIODE_SWEEP)]
         desc = f"diode2d {nx}x{ny} ({nx * ny} nodes) 0..0.7 V step 0.05"
-        contact = "anode"
-    else:
-        dims = (40, 24, 16) if small else (160, 96, 64)
-        dev = W.trigate3d(dev_cls_3d, *dims)
-        sched = [(W.trigate_bias(vd, vg), first) for vd, vg, first in W.trigate_schedule()]
-        desc = (f"trigate3d {dims[0]}x{dims[1]}x{dims[2]} ({np.prod(dims):,} nodes) "
-                "Id-Vg Vg 0..1.0 V step 0.05 at Vd 0.05 V and 0.7 V")
-        contact = "drain"
-    return dev, sched, desc, contact
+        return lanes, steps, desc, "anode"
+    dims = (40, 24, 16) if small else (160, 96, 64)
+    lanes = [W.trigate3d(dev_cls_3d, *dims) for _ in W.TRIGATE_VD]
+    steps = [([W.trigate_bias(vd, vg) for vd in W.TRIGATE_VD], q == 0)
+             for q, vg in enumerate(W.TRIGATE_VG)]
+    desc = (f"trigate3d {dims[0]}x{dims[1]}x{dims[2]} ({np.prod(dims):,} nodes) Id-Vg "
+            "Vg 0..1.0 V step 0.05 at Vd 0.05 V and 0.7 V; one step = one Vg on both "
+            "Vd branches (2 bias points)")
+    return lanes, steps, desc, "drain"
 
 
-class PointRunner:
-    """One device marching through the bias schedule with one Newton method."""
+class SweepRunner:
+    """The workload's lanes marching through the bias schedule with one Newton
+    method.  batched: all lanes in ONE packed DeviceBatch (every launch covers
+    both Vd branches, per-instance Newton/Krylov masks); otherwise the lanes'
+    devices are solved one after another, as the reference would."""
 
-    def __init__(self, args, method, dev_classes):
+    def __init__(self, args, method, dev_classes, batched):
         import tcad_b200 as tb
+        from tcad_b200.batch import DeviceBatch
         self.args = args
-        self.dev, self.sched, self.desc, self.contact = build_workload(
+        self.lanes, self.steps, self.desc, self.contact = build_workload(
             args.workload, args.small, *dev_classes)
         self.opts = tb.NewtonOptions(verbose=bool(args.verbose), **METHODS[method])
         self.method = method
+        self.batch = DeviceBatch(self.lanes) if batched and len(self.lanes) > 1 else None
         self.q = 0
         self.log = []
+        self.N = sum(d.N for d in self.lanes)
 
-    def point(self):
-        """Solve the next bias point; returns (current, converged, h2d, d2h)."""
-        dev = self.dev
-        volts, first = self.sched[self.q % len(self.sched)]
+    def restart(self):
+        """Back to the first step (the next step starts from equilibrium)."""
+        self.q = 0
+
+    def step(self):
+        """Solve every lane's next point; returns (currents, converged flags,
+        h2d bytes, d2h bytes)."""
+        volts, first = self.steps[self.q % len(self.steps)]
         self.q += 1
-        if first:
-            dev.solve_equilibrium(self.opts)
-        dev.solve_bias(volts, self.opts)
-        I = dev.terminal_current(self.contact)
-        h2d = dev.pack.last_h2d_bytes   # contact targets + gate-node bias values
-        self.log.append(dict(dev.last_newton, first=first, I=I))
-        if self.args.verbose:
-            r = dev.last_newton
-            sys.stderr.write(f"  [{self.method}] point {self.q:3d} {volts} first={first} "
-                             f"conv={r['converged']} newton={r['iters']} krylov="
-                             f"{r['krylov_iters']} relres={r['relres']:.1e} I={I:.9e}\n")
-            sys.stderr.flush()
-        return I, dev.last_converged, h2d, 8
+        if self.batch is not None:
+            b = self.batch
+            if first:
+                b.solve_equilibrium(self.opts)
+            res = b.solve_bias(volts, self.opts)
+            I = list(b.terminal_currents(self.contact))
+            conv = [r["converged"] for r in res]
+            h2d = b.pack.last_h2d_bytes
+        else:
+            I, conv, res, h2d = [], [], [], 0
+            for dev, v in zip(self.lanes, volts):
+                if first:
+                    dev.solve_equilibrium(self.opts)
+                dev.solve_bias(v, self.opts)
+                I.append(dev.terminal_current(self.contact))
+                conv.append(bool(dev.last_converged))
+                res.append(dev.last_newton)
+                h2d += dev.pack.last_h2d_bytes   # contact targets + gate-node values
+        for lane, (r, i, v) in enumerate(zip(res, I, volts)):
+            self.log.append(dict(r, first=first, I=i, lane=lane))
+            if self.args.verbose:
+                sys.stderr.write(f"  [{self.method}] step {self.q:3d} lane {lane} {v} "
+                                 f"first={first} conv={r['converged']} newton={r['iters']} "
+                                 f"krylov={r['krylov_iters']} relres={r['relres']:.1e} "
+                                 f"I={i:.9e}\n")
+                sys.stderr.flush()
+        return I, conv, h2d, 8 * len(I)
 
-    def reference_current(self):
-        """The current of the tightly converged solution at the last point:
-        the device's state solved on, untimed, with relative Krylov unknowns
-        at 1e-10 every step and the update test at 1e-12 (plus the polishing
+    def read_fields(self):
+        """Host read of every lane's potential field (the e2e result copy);
+        returns the bytes read."""
+        if self.batch is not None:
+            _ = self.batch.pack.psi.cpu()
+        else:
+            for dev in self.lanes:
+                _ = dev.psi
+        return 8 * self.N
+
+    def reference_currents(self):
+        """The currents of the tightly converged solutions at the last step:
+        each lane's state solved on, untimed, with relative Krylov unknowns at
+        1e-10 every step and the update test at 1e-12 (plus the polishing
         step) -- the fixtures' oracle-quality setting: at the stock 1e-8 the
         update test saturates at the 1e-10 density floor, so sub-floor
         minority densities, and the currents that depend on them, are only
-        loosely converged.  The state is put back afterwards, so the runner's
-        own march is unchanged."""
+        loosely converged.  States are put back afterwards, so the runner's
+        own march is unchanged.  (Sequential lanes only.)"""
         import tcad_b200 as tb
-        dev = self.dev
-        volts, _ = self.sched[(self.q - 1) % len(self.sched)]
-        keep = [t.clone() for t in (dev.pack.psi, dev.pack.n, dev.pack.p)]
-        attrs = {k: getattr(dev, k) for k in ("_bias_prev", "_bias_cur", "last_newton",
-                                              "last_converged")}
+        volts, _ = self.steps[(self.q - 1) % len(self.steps)]
         ref = tb.NewtonOptions(precision="fp64", forcing="adaptive",
                                krylov_unknowns="relative", predictor="none",
                                eta_max=1e-10, eta_min=1e-10, tol_update=1e-12)
-        dev.solve_bias(volts, ref)
-        I = dev.terminal_current(self.contact) if dev.last_converged else float("nan")
-        for t, k in zip((dev.pack.psi, dev.pack.n, dev.pack.p), keep):
-            t.copy_(k)
-        for k, v in attrs.items():
-            setattr(dev, k, v)
-        dev._host.clear()
-        return I
+        out = []
+        for dev, v in zip(self.lanes, volts):
+            keep = [t.clone() for t in (dev.pack.psi, dev.pack.n, dev.pack.p)]
+            attrs = {k: getattr(dev, k) for k in ("_bias_prev", "_bias_cur", "last_newton",
+                                                  "last_converged")}
+            dev.solve_bias(v, ref)
+            out.append(dev.terminal_current(self.contact) if dev.last_converged
+                       else float("nan"))
+            for t, k in zip((dev.pack.psi, dev.pack.n, dev.pack.p), keep):
+                t.copy_(k)
+            for k, val in attrs.items():
+                setattr(dev, k, val)
+            dev._host.clear()
+        return out
 
     def release(self):
-        self.dev = None
+        self.lanes = self.batch = None
 
 
-def timed_points(torch, runner, steps, e2e, ref_currents=None):
-    """Per-point device latency (CUDA events on the launching stream) and, with
-    e2e, the latency including the host read of the potential field.  With
+def timed_steps(torch, runner, steps, e2e, ref_currents=None):
+    """Per-step device latency (CUDA events on the launching stream) and, with
+    e2e, the latency including the host read of the potential fields.  With
     ref_currents (a list), each point's tightly converged reference current
     is appended to it, untimed."""
     lat, lat_e2e, conv, h2d, d2h = [], [], 0, 0, 0
     for _ in range(steps):
         a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         a.record()
-        I, ok, hb, db = runner.point()
+        I, ok, hb, db = runner.step()
         b.record()
         if e2e:
-            _ = runner.dev.psi
-            db += 8 * runner.dev.N
+            db += runner.read_fields()
         c.record()
         torch.cuda.synchronize()
         lat.append(a.elapsed_time(b))
         lat_e2e.append(a.elapsed_time(c))
-        conv += int(ok)
+        conv += int(sum(ok))
         h2d += hb
         d2h += db
         if ref_currents is not None:
-            ref_currents.append(runner.reference_current())
+            ref_currents.extend(runner.reference_currents())
     return lat, lat_e2e, conv, h2d, d2h
 
 
@@ -330,42 +376,49 @@ def run_ours(args):
     from tcad_b200 import _lib
     lib = _lib.load()
     classes = (tb.Device2D, tb.Device3D)
-    chosen = PointRunner(args, args.method, classes)
-    dev = chosen.dev
+    chosen = SweepRunner(args, args.method, classes, batched=True)
+    dev = chosen.lanes[0]
     dim, N = dev.dim, dev.N
+    ppstep = len(chosen.lanes)          # bias points per step
 
     for _ in range(args.warmup):
-        chosen.point()
+        chosen.step()
+    chosen.restart()                    # the timed steps walk the schedule from its start
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     L0 = lib.tcad_launch_count()
+    n_warm_log = len(chosen.log)
     with Clocks(local) as clk:
         t_wall = time.perf_counter()
-        lat, lat_e2e, conv, h2d_tot, d2h_tot = timed_points(torch, chosen, args.steps, True)
+        lat, lat_e2e, conv, h2d_tot, d2h_tot = timed_steps(torch, chosen, args.steps, True)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t_wall
     launches = lib.tcad_launch_count() - L0
     t_dev = sum(lat) / 1e3
     t_e2e = sum(lat_e2e) / 1e3
-    pts_chosen = chosen.log[args.warmup:]
+    pts_chosen = chosen.log[n_warm_log:]
 
-    # the plain FP64 path on the same points: its throughput, and the
-    # reference currents for the chosen path's 1e-6 check
+    # the plain FP64 path on the same points, its lanes one after another:
+    # its throughput, and the reference currents for the chosen path's 1e-6
+    # check
     plain_lat = None
     if args.method != "plain":
-        plain = PointRunner(args, "plain", classes)
+        plain = SweepRunner(args, "plain", classes, batched=False)
         for _ in range(args.warmup):
-            plain.point()
+            plain.step()
+        plain.restart()
+        n0 = len(plain.log)
         I_ref = []
-        plain_lat, _, plain_conv, _, _ = timed_points(torch, plain, args.steps, False, I_ref)
-        pts_plain = plain.log[args.warmup:]
+        plain_lat, _, plain_conv, _, _ = timed_steps(torch, plain, args.steps, False, I_ref)
+        pts_plain = plain.log[n0:]
         rel = lambda a, b: abs(a - b) / max(abs(b), 1e-300)  # noqa: E731
         errs = [rel(c["I"], p["I"]) for c, p in zip(pts_chosen, pts_plain)]
         errs_ref = [rel(c["I"], r) for c, r in zip(pts_chosen, I_ref)]
         errs_plain_ref = [rel(p["I"], r) for p, r in zip(pts_plain, I_ref)]
         plain_counts = ([r["iters"] for r in pts_plain], [r["krylov_iters"] for r in pts_plain])
         ok_pts = sum(1 for c, e in zip(pts_chosen, errs_ref) if c["converged"] and e <= 1e-6)
+        plain.release()
         del plain
     else:
         errs = [0.0] * len(pts_chosen)
@@ -381,7 +434,8 @@ def run_ours(args):
 
     # ---- live roofline of the dominant kernel (block SpMV on the last J) and
     # of the assembly, CUDA events on the launching stream
-    pk = dev.pack
+    pk = chosen.batch.pack if chosen.batch is not None else dev.pack
+    NN = pk.N                            # nodes of the timed pack (every lane)
     sp = _lib.stream_ptr()
     y = torch.empty_like(pk.du)
     x = torch.randn(3 * pk.N, dtype=torch.float64, device=pk.device)
@@ -408,9 +462,23 @@ def run_ours(args):
     t_asm = time_kernel(lambda: lib.tcad_sg_assemble(pk.pref, _lib.ptr(pk.psi), _lib.ptr(pk.n),
                                                      _lib.ptr(pk.p), _lib.ptr(Fa), _lib.ptr(Ja),
                                                      _lib.MODE_ELIMINATE, sp), 20)
+    # one whole BiCGStab iteration inside the solver (five fused kernels),
+    # timed as a fixed-count solve that cannot converge
+    ni = pk.P.n_inst
+    kit, kst, krr = (ctypes.c_int32 * ni)(), (ctypes.c_int32 * ni)(), (ctypes.c_double * ni)()
+    xk = torch.zeros_like(pk.du)
+    KIT = 200
+
+    def krylov_fixed():
+        lib.tcad_block_krylov(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(xk), 0, 1e-300,
+                              KIT, 0, _lib.ptr(pk.work), pk.work.numel(), kit, kst, krr, sp)
+    t_kry = time_kernel(krylov_fixed, 2)
+    it_done = max(int(kit[i]) for i in range(ni))
+    t_iter = t_kry / max(it_done, 1)
     peak, peak_kind = load_peaks()
-    ach_spmv = BYTES_SPMV[dim] * N / t_spmv / 1e9
-    ach_asm = BYTES_ASM[dim] * N / t_asm / 1e9
+    ach_spmv = BYTES_SPMV[dim] * NN / t_spmv / 1e9
+    ach_asm = BYTES_ASM[dim] * NN / t_asm / 1e9
+    ach_iter = BYTES_ITER[dim] * NN / t_iter / 1e9
 
     res = {}
     if rank == 0:
@@ -431,7 +499,7 @@ def run_ours(args):
                              f"{8 * _lib.NE[dim] * N / 1e6:.0f} MB)"},
             "p50_ms": statistics.median(lat), "p99_ms": float(np.percentile(lat, 99)),
             "converged_points": conv, "points_within_1e-6_of_reference": ok_pts,
-            "points": args.steps * world,
+            "points": args.steps * world * ppstep, "points_per_step": ppstep,
             "current_reference": "each timed point's plain FP64 state solved on, untimed, "
                                  "to the oracle fixtures' setting (relative unknowns at "
                                  "1e-10, update test 1e-12, polishing step)",
@@ -450,15 +518,21 @@ def run_ours(args):
                          "bound": "hbm", "achieved": ach_spmv, "peak": peak,
                          "unit": "GB/s", "frac": ach_spmv / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                         "bytes_per_launch": BYTES_SPMV[dim] * N,
+                         "bytes_per_launch": BYTES_SPMV[dim] * NN,
                          "launch_ms": t_spmv * 1e3,
                          "traffic": load_traffic(f"spmv{dim}d_{args.workload}")},
             "roofline_assembly": {"kernel": "k_sg_assemble", "bound": "hbm",
                                   "achieved": ach_asm, "peak": peak, "unit": "GB/s",
                                   "frac": ach_asm / peak,
-                                  "bytes_per_launch": BYTES_ASM[dim] * N,
+                                  "bytes_per_launch": BYTES_ASM[dim] * NN,
                                   "launch_ms": t_asm * 1e3,
                                   "traffic": load_traffic(f"assemble{dim}d_{args.workload}")},
+            "roofline_bicgstab_iteration": {
+                "kernel": "k_bi_p + k_bi_v + k_bi_s + k_bi_t + k_bi_x (one iteration in "
+                          "the solver)", "bound": "hbm", "achieved": ach_iter, "peak": peak,
+                "unit": "GB/s", "frac": ach_iter / peak,
+                "bytes_per_iteration": BYTES_ITER[dim] * NN, "iteration_ms": t_iter * 1e3,
+                "iterations_timed": it_done},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "wall_s": wall,
@@ -471,7 +545,9 @@ def run_ours(args):
                 "converged_points": plain_conv}
             res["chosen_over_plain"] = value / res["plain_fp64_gpu"]["value"]
         if world == 1 and not args.no_cpu_baseline:
-            res["cpu_baseline"] = cpu_baseline(dev, args, *plain_counts)
+            st0 = chosen.batch.state(0) if chosen.batch is not None else \
+                (dev.psi, dev.n, dev.p)
+            res["cpu_baseline"] = cpu_baseline(dev, st0, *plain_counts)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -840,13 +916,14 @@ def cpu_costs(ora, psi, n, p, krylov_iters=10):
     return t_asm, t_bj, t_it
 
 
-def cpu_baseline(dev, args, newton_iters, krylov_iters):
-    """Oracle on the host cores, one full-mesh sample scaled to a bias point
-    with the GPU run's own Newton and Krylov iteration counts."""
+def cpu_baseline(dev, state, newton_iters, krylov_iters):
+    """Oracle on the host cores, one full-mesh sample at `state` (psi, n, p)
+    scaled to a bias point with the GPU run's own Newton and Krylov
+    iteration counts."""
     try:
         os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
         ora = oracle_from(dev)
-        t_asm, t_bj, t_it = cpu_costs(ora, dev.psi, dev.n, dev.p)
+        t_asm, t_bj, t_it = cpu_costs(ora, *state)
         per_point = [nw * (t_asm + t_bj) + kr * t_it
                      for nw, kr in zip(newton_iters, krylov_iters)]
         sec = float(np.mean(per_point))
@@ -891,13 +968,13 @@ def reference_worker(workload, small, steps, warmup, wid):
     over warmup + steps bounded samples; returns (seconds per bias point of
     each timed step, sample description, workload description)."""
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
-    dev, sched, desc, contact = build_workload(workload, small, HostDevice, HostDevice)
-    ora = oracle_from(dev)
+    lanes, steps_sched, desc, contact = build_workload(workload, small, HostDevice, HostDevice)
+    ora = oracle_from(lanes[0])
     lat = []
     if workload == "diode2d":
         # full solves: every step is one real warm-started bias point
         ora.solve_equilibrium()
-        pts = [v for v, _ in sched]
+        pts = [v[0] for v, _ in steps_sched]
         for q in range(warmup + steps):
             t0 = time.perf_counter()
             ora.solve_bias(pts[(q + wid) % len(pts)])
@@ -938,6 +1015,14 @@ def reference_processes(workload, small):
     return max(1, min(cores, int(0.7 * avail // per)))
 
 
+def workload_extrapolated(workload):
+    """True where the reference arm's rate is a measured per-iteration cost
+    scaled to a bias point (every 3D workload: a full CPU bias point of a
+    million-node device takes hours), False where each step is a full
+    measured bias point (the 2D diode)."""
+    return workload != "diode2d"
+
+
 def run_reference(args):
     """The oracle's CPU implementation on the host cores (rank 0 only): one
     process per core, each an independent stream of bias points (the
@@ -963,6 +1048,7 @@ def run_reference(args):
             "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic device",
             "config": {"workload": desc, "method": "oracle CPU port (numpy/scipy)"},
+            "extrapolated": workload_extrapolated(args.workload),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port",
                              "sample": sample + f"; {nproc} processes x 1 thread",
                              "per_process_sec_per_point": float(np.mean(
@@ -979,8 +1065,9 @@ def run_kernels(args):
     import tcad_b200 as tb
     from tcad_b200 import _lib
     lib = _lib.load()
-    dev, sched, desc, contact = build_workload(args.workload, args.small, tb.Device2D,
-                                               tb.Device3D)
+    lanes, _, desc, contact = build_workload(args.workload, args.small, tb.Device2D,
+                                             tb.Device3D)
+    dev = lanes[0]
     pk = dev.pack
     s = dev.setup
     g = s.bulk_guess()

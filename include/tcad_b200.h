@@ -361,7 +361,8 @@ typedef struct tcad_newton_result {
   int32_t fp64_from;     /* precision 32: Newton iteration from which this instance
                             solved in FP64 after an FP32-solved step was rejected
                             (-1: never; always -1 for precision 64) */
-  int32_t pad;
+  int32_t polish_iters;  /* of iters, the polishing steps taken after the update test
+                            passed (the reference's own Newton count stops before them) */
 } tcad_newton_result_t;
 
 /* Full coupled Newton solve at the contact targets stored in the pack

@@ -71,7 +71,7 @@ class NewtonResult(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int32), ("converged", ctypes.c_int32),
                 ("krylov_iters", ctypes.c_int32), ("status", ctypes.c_int32),
                 ("err", ctypes.c_double), ("relres", ctypes.c_double),
-                ("fp64_from", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("fp64_from", ctypes.c_int32), ("polish_iters", ctypes.c_int32)]
 
 
 # name -> (restype, argtypes)

@@ -1734,7 +1734,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   for (int i = 0; i < ni; ++i) {
     result[i].iters = 0; result[i].converged = 0; result[i].krylov_iters = 0;
     result[i].status = TCAD_OK; result[i].err = INFINITY; result[i].relres = 0.0;
-    result[i].fp64_from = -1; result[i].pad = 0;
+    result[i].fp64_from = -1; result[i].polish_iters = 0;
   }
   std::vector<KState> hks(ni);  // sized up front: a solve may end before any inner launch
   std::vector<unsigned long long> herr(ni);
@@ -2016,6 +2016,7 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
                            std::max(eta_lo, 0.1 * (std::isfinite(e) ? e : 1.0)));
       if (polish_left[i] > 0) {
         // post-convergence polishing step (already counted as converged)
+        ++result[i].polish_iters;
         if (--polish_left[i] == 0) hact[i] = 0;
       } else if (e < opts->tol_update && lin_ok) {
         result[i].converged = 1;
@@ -2053,7 +2054,7 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
   for (int i = 0; i < ni; ++i) {
     result[i].iters = 0; result[i].converged = 0; result[i].krylov_iters = 0;
     result[i].status = TCAD_OK; result[i].err = INFINITY; result[i].relres = 0.0;
-    result[i].fp64_from = -1; result[i].pad = 0;
+    result[i].fp64_from = -1; result[i].polish_iters = 0;
   }
   std::vector<KState> hks;
   std::vector<unsigned long long> herr(ni);

@@ -79,18 +79,23 @@ class NewtonOptions:
     # GPU-only: Newton steps taken after the update test passes.  The test
     # saturates at the 1e-10 density floor, so sub-floor minority densities
     # (and low-bias currents) are converged only to ~1e-5 when it first
-    # passes; one more quadratic step brings them to round-off.
-    polish: int = 1
-    # GPU-only: Krylov tolerance of the polishing steps.  Low-bias currents
-    # are small differences of large drift and diffusion fluxes, so the
-    # state after the last step must be accurate well beyond the update test.
+    # passes; the first step (solved to polish_eta) brings them to round-off.
+    # The second (solved to the forcing tolerance) lands on the FP64 fixed
+    # point of the residual: at low-current points the terminal current is
+    # a difference of contact fluxes ~1e11 times larger (a 20x6x5 p-i-n at
+    # 0.4 V: 4.9e-15 A), so one ulp of the state still moves it by ~1e-4,
+    # while at the fixed point -- the same one the reference's Newton
+    # reaches, since the residual arithmetic is the reference's -- the
+    # currents agree to 1e-16.
+    polish: int = 2
+    # GPU-only: Krylov tolerance of the first polishing step (the second
+    # follows the forcing rule).  Low-bias currents are small differences of
+    # large drift and diffusion fluxes, so the state after it must be
+    # accurate well beyond the update test.
     polish_eta: float = 1e-10
     # GPU-only: density floor of the relative Krylov unknowns in the
-    # polishing steps (0: krylov_scale_floor).  Measured, a floor far below
-    # the densities (1e-30) is not more accurate: it moved one anode current
-    # of the 8.4M-node p-i-n (1.2e-13 A) onto the plain path's, but put the
-    # 600-node p-i-n's 0.5 V current 1.4e-6 from the exact-Newton oracle,
-    # which the default meets.  Off by default.
+    # polishing steps (0: krylov_scale_floor).  Off by default: the two
+    # polishing steps above already reach the FP64 fixed point.
     polish_scale_floor: float = 0.0
     # GPU-only: inexact-Newton forcing.  "adaptive" solves step k to
     # eta_k = clamp(0.1 * update_{k-1}, linsolve_rtol, eta_max) (quadratic

@@ -731,7 +731,8 @@ class Pack:
         _lib.check(rc, "tcad_newton_solve")
         return [dict(iters=r.iters, converged=bool(r.converged),
                      krylov_iters=r.krylov_iters, status=r.status, err=r.err,
-                     relres=r.relres, fp64_from=r.fp64_from) for r in res]
+                     relres=r.relres, fp64_from=r.fp64_from,
+                     polish_iters=r.polish_iters) for r in res]
 
     def equilibrium(self, opts):
         ni = len(self.setups)
@@ -746,4 +747,5 @@ class Pack:
         _lib.check(rc, "tcad_equilibrium_solve")
         return [dict(iters=r.iters, converged=bool(r.converged),
                      krylov_iters=r.krylov_iters, status=r.status, err=r.err,
-                     relres=r.relres, fp64_from=r.fp64_from) for r in res]
+                     relres=r.relres, fp64_from=r.fp64_from,
+                     polish_iters=r.polish_iters) for r in res]

@@ -89,6 +89,20 @@ class TransientResult:
         self.dt_hist = np.asarray(dt_hist)
 
 
+def next_step(step_dt, converged, newton_iters, max_iter, growth, shrink, dt_max, dt_min):
+    """The adaptive step rule of pytcad/transient2d.py:268-290: after an
+    accepted step, grow by `growth` (capped at dt_max) when Newton took at
+    most max(3, max_iter // 4) steps to pass its update test, else keep the
+    step; after a rejected step, shrink by `shrink`.  Returns the next step,
+    or None when a shrunk step falls below dt_min (the run has stalled)."""
+    if converged:
+        if newton_iters <= max(3, max_iter // 4):
+            return min(step_dt * growth, dt_max)
+        return step_dt
+    nxt = step_dt * shrink
+    return None if nxt < dt_min else nxt
+
+
 def solve_transient(device, waveforms, t_end, dt0, theta=1.0, opts=None, dt_min=None,
                     dt_max=None, growth=1.5, shrink=0.5, output_times=None, verbose=False,
                     keep_history=True):
@@ -166,14 +180,16 @@ def solve_transient(device, waveforms, t_end, dt0, theta=1.0, opts=None, dt_min=
             if out_times is not None and out_idx < len(out_times) and \
                     abs(t - out_times[out_idx]) < 1e-15 * max(1.0, t):
                 out_idx += 1
-            if res["iters"] <= max(3, opts.max_iter // 4):
-                dt_s = min(step_dt_s * growth, dt_max_s)
-            else:
-                dt_s = step_dt_s
+            # the reference's step-growth rule counts the Newton steps up to
+            # the update test (transient2d.py _newton_step returns it + 1),
+            # not the polishing steps taken after it
+            dt_s = next_step(step_dt_s, True, res["iters"] - res.get("polish_iters", 0),
+                             opts.max_iter, growth, shrink, dt_max_s, dt_min_s)
         else:
             device.restore_state(old)
-            dt_s = step_dt_s * shrink
-            if dt_s < dt_min_s:
+            dt_s = next_step(step_dt_s, False, 0, opts.max_iter, growth, shrink, dt_max_s,
+                             dt_min_s)
+            if dt_s is None:
                 raise RuntimeError(
                     f"solve_transient stalled at t={t:.3e}s approaching t={t_new:.3e}s: dt "
                     f"shrank below dt_min={dt_min_s * t_scale:.3e}s without Newton convergence")

@@ -10,7 +10,7 @@ functions the reference's parity tests hold its compiled kernels to
 (tests/test_m47_s2_device3d_accel_parity.py,
 tests/test_device3d_poisson_eq_accel_parity.py).
 
-Usage:  python tests/golden/make_golden.py [--ref /root/reference/pytcad]
+Usage:  python tests/golden/make_golden.py --ref <reference>/pytcad
         [--skip-c1]   (the 201x101 diode sweep takes about 1-2 minutes)
 """
 import argparse
@@ -341,6 +341,38 @@ def transient_small(pt, out, nx=41, ny=11):
     np.savez_compressed(out, **_dump_dev(dev, 2, extra))
 
 
+def transient_growth(pt, out, nx=41, ny=11):
+    """pytcad.transient2d.solve_transient with its default adaptive step
+    (growth 1.5 after every step that converges within max(3, max_iter/4)
+    Newton steps, capped at 64 dt0): the 41x11 diode stepped to 0.3 V from
+    dt0 = 1 ps to 0.2 ns, backward Euler.  Stores the time points, the step
+    history and both contacts' currents."""
+    from pytcad.device2d import Device2D
+    from pytcad.mesh2d import Mesh2D
+    from pytcad.device import Models, NewtonOptions
+    from pytcad.materials import Semiconductor
+    from pytcad.transient import StepWaveform
+    from pytcad.transient2d import solve_transient
+    x = diode_x(nx)
+    y = np.linspace(0.0, 1.0e-4, ny)
+    dop = np.where(np.meshgrid(x, y)[0] < 1.0e-4, -1e17, 1e18)
+    mat = Semiconductor(tau_n0=1e-7, tau_p0=1e-7, tau_Nref=1e300)
+    mdl = Models(doping_mobility=False, srh=True, auger=False, bgn=False)
+    opts = NewtonOptions(linsolve="direct", tol_update=SWEEP_TOL)
+    dt0, t_end = 1e-12, 2e-10
+    dev = Device2D(Mesh2D(x, y), dop, material=mat, models=mdl)
+    dev.add_contact("anode", i=np.zeros(ny, int), j=np.arange(ny))
+    dev.add_contact("cathode", i=np.full(ny, nx - 1), j=np.arange(ny))
+    dev.solve_equilibrium(opts)
+    r = solve_transient(dev, {"anode": StepWaveform(0.0, 0.3, 0.0)}, t_end, dt0,
+                        theta=1.0, opts=opts)
+    extra = dict(dt0=dt0, t_end=t_end, v_step=0.3, tol_update=SWEEP_TOL, mat_tau=1e-7,
+                 t=np.array(r.times), dt_hist=np.array(r.dt_hist),
+                 Ia=np.array(r.terminal_current["anode"]),
+                 Ic=np.array(r.terminal_current["cathode"]), psi=dev.psi.ravel().copy())
+    np.savez_compressed(out, **_dump_dev(dev, 2, extra))
+
+
 def transient3d_small(pt, out, nx=21, ny=5, nz=4):
     """pytcad.transient3d.solve_transient on a small 3D diode (x graded as the
     2D diode's, 1 um x 0.4 um x 0.3 um, N_A 1e17 | N_D 1e18, constant
@@ -474,16 +506,20 @@ def mosfet_small(pt, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/pytcad")
+    ap.add_argument("--ref", default=os.environ.get("PYTCAD_REF"),
+                    help="the reference's pytcad project directory (default: $PYTCAD_REF)")
     ap.add_argument("--skip-c1", action="store_true")
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give --ref or set PYTCAD_REF to the reference's pytcad directory")
     pt = _import_reference(a.ref)
     jobs = [("elem", elem), ("asm2d", asm2d), ("asm3d", asm3d),
             ("mosfet_small", mosfet_small), ("trigate_small", trigate_small),
             ("diode_small", lambda pt, out: diode_c1(pt, out, nx=41, ny=11)),
             ("transient_small", transient_small),
             ("transient3d_small", transient3d_small),
+            ("transient_growth", transient_growth),
             ("diode_c1", diode_c1)]
     for name, fn in jobs:
         if a.only and name not in a.only.split(","):
