@@ -206,6 +206,16 @@ size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart
  * wide; returns the previous setting. */
 int tcad_set_krylov_fused(int on);
 
+/* Test hook of the fused solve's failure path (no counterpart in the
+ * reference).  hold = 1: every later fused launch waits at its first grid
+ * barrier for one arrival that never comes, so the barrier's bounded wait
+ * (1 s of device time) runs out, the kernel returns, and the host solves
+ * again with one launch per step.  Process-wide; returns the previous
+ * setting.  tcad_krylov_fused_gave_up counts the fused launches whose
+ * barrier gave up, hook or not. */
+int tcad_set_krylov_fused_test(int hold);
+uint64_t tcad_krylov_fused_gave_up(void);
+
 /* Node-block-Jacobi set-up (pytcad/linsolve.py:363-427): inverts every
  * diagonal 3x3 block of J in place and replaces F by the block-scaled
  * right-hand side b^ = D^-1 (-F).  status[inst] gets TCAD_ERR_SINGULAR for a

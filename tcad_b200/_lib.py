@@ -89,6 +89,8 @@ _SIGS = {
                                                _p]),
     "tcad_block_workspace_bytes": (ctypes.c_size_t, [_p, ctypes.c_int, ctypes.c_int]),
     "tcad_set_krylov_fused": (ctypes.c_int, [ctypes.c_int]),
+    "tcad_set_krylov_fused_test": (ctypes.c_int, [ctypes.c_int]),
+    "tcad_krylov_fused_gave_up": (ctypes.c_uint64, []),
     "tcad_state_extrapolate": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "tcad_block_jacobi_setup": (ctypes.c_int, [_p, _p, _p, _p, _p]),
     "tcad_block_jacobi_setup_rel": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, ctypes.c_double,

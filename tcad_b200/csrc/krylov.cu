@@ -674,7 +674,10 @@ k_true_resid(const tcad_pack_t pk, const T* __restrict__ J, const T* __restrict_
 // round x nblocks.  Every wait is bounded: past kBarrierNs of device time, or
 // once another CTA has given up (bar[2] != 0), the CTA sets bar[2] and the
 // barrier returns false, and the kernel returns -- the host sees bar[2] and
-// solves again with one launch per step.
+// solves again with one launch per step.  bar[3] is added to every round's
+// target: 0 always, except under the give-up test hook
+// (tcad_set_krylov_fused_test), which sets it to 1 so that the first barrier
+// waits for an arrival that never comes and its time limit runs out.
 constexpr unsigned long long kBarrierNs = 1000000000ull;   // 1 s
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -702,7 +705,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks, un
   if (threadIdx.x == 0) {
     int good = 1;
     round += 1u;
-    const unsigned target = round * nblocks;
+    const unsigned target = round * nblocks + ld_acquire(&bar[3]);
     const unsigned prev = atom_add_acq_rel(&bar[0], 1u);
     if (prev + 1u != target) {
       const unsigned long long t0 = globaltimer_ns();
@@ -1250,6 +1253,8 @@ static void ilu_apply_t(const tcad_pack_t* pk, const double* J, const double* Q,
 
 // ---- fused (one cooperative launch) BiCGStab: when and how
 static std::atomic<int> g_fused_mode{1};   // 0: one launch per step always
+static std::atomic<int> g_fused_test_hold{0};        // give-up test hook (bar[3] = 1)
+static std::atomic<uint64_t> g_fused_gave_up{0};     // fused launches that gave up
 
 // k_bicgstab_fused<DIM> needs every flat block resident at once
 template <int DIM>
@@ -1276,6 +1281,11 @@ static int launch_bicgstab_fused(const tcad_pack_t* pk, const double* J, const d
                                  std::vector<KState>& hks, cudaStream_t s,
                                  const double* rtol_inst) {
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.bar, 0, 4 * sizeof(unsigned), s));
+  if (g_fused_test_hold.load()) {
+    static const unsigned kPhantom = 1u;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(w.bar + 3, &kPhantom, sizeof(unsigned),
+                                    cudaMemcpyHostToDevice, s));
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)pk->n_flat);
   cfg.blockDim = dim3(NT);
@@ -1303,7 +1313,11 @@ static int launch_bicgstab_fused(const tcad_pack_t* pk, const double* J, const d
   TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState), cudaMemcpyDeviceToHost, s));
   TCAD_CUDA_CHECK(cudaMemcpyAsync(hbar, w.bar, sizeof(hbar), cudaMemcpyDeviceToHost, s));
   TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
-  return hbar[2] != 0u ? 1 : TCAD_OK;
+  if (hbar[2] != 0u) {
+    g_fused_gave_up.fetch_add(1);
+    return 1;
+  }
+  return TCAD_OK;
 }
 
 template <class T>
@@ -1561,6 +1575,12 @@ static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, do
 }  // namespace tcad
 
 using namespace tcad;
+
+extern "C" int tcad_set_krylov_fused_test(int hold) {
+  return g_fused_test_hold.exchange(hold ? 1 : 0);
+}
+
+extern "C" uint64_t tcad_krylov_fused_gave_up(void) { return g_fused_gave_up.load(); }
 
 extern "C" int tcad_set_krylov_fused(int on) {
   return g_fused_mode.exchange(on ? 1 : 0);

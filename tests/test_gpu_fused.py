@@ -110,3 +110,29 @@ def test_newton_sweep_bit_identical():
     for u, v in zip(a[:3], b[:3]):
         assert bool((u == v).all())
     assert a[3] == b[3]
+
+
+def test_fused_give_up_falls_back_bit_identical():
+    """The fused solve's failure path: with the test hook, the first grid
+    barrier waits for an arrival that never comes until its 1 s limit runs
+    out; the kernel returns, the host sees the flag and solves again with
+    one launch per step.  The answer is the launch-per-step one bit for bit,
+    and the GPU stays usable (the next fused solve succeeds)."""
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    pk = _scaled_system(W.diode2d(tb.Device2D, 201, 101))
+    lib = pk.lib
+    x0, it0, st0, rr0, _ = _krylov(pk, fused=False)
+    g0 = lib.tcad_krylov_fused_gave_up()
+    prev = lib.tcad_set_krylov_fused_test(1)
+    try:
+        x1, it1, st1, rr1, n1 = _krylov(pk, fused=True)
+    finally:
+        lib.tcad_set_krylov_fused_test(prev)
+    assert lib.tcad_krylov_fused_gave_up() == g0 + 1
+    assert n1 > 2                     # the fused launch, then the per-step launches
+    assert (it1, st1) == (it0, st0) and rr1 == rr0
+    assert np.array_equal(x1.cpu().numpy(), x0.cpu().numpy())
+    x2, it2, st2, rr2, n2 = _krylov(pk, fused=True)
+    assert n2 == 1 and lib.tcad_krylov_fused_gave_up() == g0 + 1
+    assert np.array_equal(x2.cpu().numpy(), x0.cpu().numpy())
