@@ -13,7 +13,7 @@ two branch devices one after another), + the terminal currents.  The warm-up
 steps walk the start of the schedule, then the schedule restarts, so K timed
 steps cover Vg = 0 .. 0.05 (K-1) V on both branches, equilibrium included.
 A point counts only when Newton converged (update < 1e-8 plus the polishing
-step) and its current is within 1e-6 of the reference current: the plain
+steps) and its current is within 1e-6 of the reference current: the plain
 FP64 path's state at that point, solved on untimed to the oracle fixtures'
 setting (update test 1e-12, Krylov at 1e-10 in relative unknowns).
 
@@ -76,8 +76,8 @@ METHOD_DESC = {
     "plain": "plain FP64: fused SG assembly, node-block-Jacobi BiCGStab to rtol 1e-10 on "
              "(dpsi, dn, dp) every Newton step, damped Newton",
     "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the block-scaled system in "
-            "relative unknowns (dpsi, dn/n, dp/p) solved to 1e-3 every Newton step, one "
-            "polishing step, secant predictor along the sweep",
+            "relative unknowns (dpsi, dn/n, dp/p) solved to 1e-3 every Newton step, two "
+            "polishing steps (1e-10, then 1e-3), secant predictor along the sweep",
     "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
              "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
              "relative unknowns, adaptive forcing, secant predictor; per-instance FP64 "
@@ -493,7 +493,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 (FP32 inner Krylov)" if args.method == "mixed" else "f64",
             "data": "synthetic device (analytic doping profiles, explicit mesh)",
-            "config": {"workload": chosen.desc, "method": method_desc + " (+1 polishing Newton step)",
+            "config": {"workload": chosen.desc, "method": method_desc,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (J alone is "
                              f"{8 * _lib.NE[dim] * N / 1e6:.0f} MB)"},
@@ -806,11 +806,19 @@ def run_serve(args):
                              "p99_ms": float(np.percentile(lk, 99))}
     h2d = sum(w.h2d_bytes for w in srv.workers.values())
     d2h = sum(w.d2h_bytes for w in srv.workers.values())
-    rounds = {d: {"rounds": w.rounds,
-                  "mean_instances": float(np.mean([n for _, _, n, _ in w.round_log]))
-                  if w.round_log else 0.0,
-                  "max_instances": max([n for _, _, n, _ in w.round_log], default=0)}
-              for d, w in srv.workers.items()}
+    def round_stats(log):
+        if not log:
+            return {"rounds": 0}
+        a = np.array([(t1 - t0, n, nn, it, nf, nodes) for t0, t1, n, nn, it, nf, nodes in log])
+        return {"rounds": len(log), "mean_instances": float(a[:, 1].mean()),
+                "max_instances": int(a[:, 1].max()), "new_devices": int(a[:, 2].sum()),
+                "round_s_p50": float(np.median(a[:, 0])), "round_s_max": float(a[:, 0].max()),
+                "round_s_total": float(a[:, 0].sum()),
+                "newton_iters_max_p50": float(np.median(a[:, 3])),
+                "newton_iters_max": int(a[:, 3].max()),
+                "unconverged_instances": int(a[:, 4].sum()),
+                "mean_round_nodes": float(a[:, 5].mean())}
+    rounds = {d: round_stats(w.round_log) for d, w in srv.workers.items()}
     value = pts_conv / elapsed
 
     # the plain FP64 path: the same requests in arrival order, one after another

@@ -18,5 +18,5 @@ Parity is pinned: ``tests/golden/make_golden.py`` runs the reference itself
 from .dd_oracle import (  # noqa: F401
     SILICON_PARAMS, OracleModels, OracleDevice, bernoulli, dbernoulli,
     recombination, ohmic_values, control_volume_widths, eliminate_csr,
-    build_block_jacobi, solve_linear_iterative, ReusedLU,
+    build_block_jacobi, solve_linear_iterative,
 )

@@ -23,7 +23,7 @@ import warnings
 
 import numpy as np
 import scipy.sparse as sp
-from scipy.sparse.linalg import LinearOperator, bicgstab, gmres, splu, spsolve
+from scipy.sparse.linalg import LinearOperator, bicgstab, gmres, spsolve
 
 # constants.py:10-14, moscap.py:60, kernels.py:29
 Q = 1.602176634e-19
@@ -220,54 +220,6 @@ def solve_linear_iterative(A, b, method="bicgstab", rtol=1e-10, maxiter=500,
                                                 1e-300)
     ok = code == 0 and bool(np.all(np.isfinite(x))) and res <= max(rtol, 1e-6)
     return x, count[0], ok, res
-
-
-class ReusedLU:
-    """Newton-step solves for 3D systems whose direct factorisation takes
-    minutes (tens of thousands of nodes): the system is scaled so that every
-    row and unknown counts -- rows by the inverse node blocks (block-Jacobi,
-    linsolve.py:363-427; the plain diagonal for the scalar Poisson system),
-    columns by the state's densities for the n and p unknowns (no floor, so
-    minority densities many decades below the majority ones are resolved)
-    -- and solved by GMRES preconditioned with the SuperLU factors of an
-    earlier step's scaled matrix, accepted only at a true relative residual
-    of 1e-12 of the scaled system.  When the old factors no longer give that
-    within one restart cycle, the current matrix is factorised (SuperLU) and
-    used directly, with one step of iterative refinement.  The Newton
-    iterates therefore follow exact-solve Newton to 1e-12; only the cost of
-    a step changes.  ``factorisations`` counts the SuperLU calls."""
-
-    def __init__(self):
-        self.lu = None
-        self.factorisations = 0
-
-    def solve(self, A, b, scale=None):
-        A = A.tocsr()
-        n = A.shape[0]
-        if scale is not None and n % 3 == 0:
-            inv = build_block_jacobi(A, 3)
-            if inv is None:
-                return spsolve(A.tocsc(), b)
-            nb = n // 3
-            Dinv = sp.bsr_matrix((inv, np.arange(nb), np.arange(nb + 1)),
-                                 shape=(n, n)).tocsr()
-        else:
-            d = A.diagonal()
-            Dinv = sp.diags(1.0 / np.where(d == 0.0, 1.0, d), format="csr")
-        c = np.ones(n) if scale is None else np.asarray(scale, dtype=float)
-        As = (Dinv @ A @ sp.diags(c, format="csr")).tocsc()
-        bs = Dinv @ b
-        bn = max(float(np.linalg.norm(bs)), 1e-300)
-        if self.lu is not None:
-            M = LinearOperator(As.shape, self.lu.solve)
-            y, _ = gmres(As, bs, M=M, rtol=1e-13, atol=0.0, restart=40, maxiter=1)
-            if np.all(np.isfinite(y)) and float(np.linalg.norm(As @ y - bs)) <= 1e-12 * bn:
-                return c * y
-        self.lu = splu(As, permc_spec="MMD_AT_PLUS_A")
-        self.factorisations += 1
-        y = self.lu.solve(bs)
-        y = y + self.lu.solve(bs - As @ y)
-        return c * y
 
 
 # ---------------------------------------------------------------------------
@@ -472,16 +424,14 @@ class OracleDevice:
         self.fixed_poisson = fixed
         return Ff.reshape(self.shape), J
 
-    def solve_equilibrium(self, max_iter=100, tol=1e-8, max_dpsi=5.0, linsolve="direct"):
-        """device2d.py:1308-1373 / device3d.py:1311-1454 (direct solve, or
-        ``linsolve="lu_reuse"``: ReusedLU)."""
-        lr = ReusedLU() if linsolve == "lu_reuse" else None
+    def solve_equilibrium(self, max_iter=100, tol=1e-8, max_dpsi=5.0):
+        """device2d.py:1308-1373 / device3d.py:1311-1454 (direct solve)."""
         psi = self.bulk_guess()
         self.eq_iters = 0
         for it in range(max_iter):
             F, J = self.residual_jacobian_poisson(psi)
             Jd, rhs = eliminate_csr(J, -F.ravel(), self.fixed_poisson)
-            d = (lr.solve(Jd, rhs) if lr else spsolve(Jd.tocsc(), rhs)).reshape(self.shape)
+            d = spsolve(Jd.tocsc(), rhs).reshape(self.shape)
             d = np.clip(d, -max_dpsi, max_dpsi)
             psi = psi + d
             self.eq_iters = it + 1
@@ -619,9 +569,8 @@ class OracleDevice:
     def solve_bias(self, voltages=None, max_iter=100, tol=1e-8, max_dpsi=5.0,
                    linsolve="direct", rtol=1e-10):
         """device2d.py:1923-2191 / device3d.py:1981-2271, plain path.
-        ``linsolve``: "direct" (SuperLU), "lu_reuse" (ReusedLU, kept on the
-        device between calls as ``self.lu_reuse``) or "bicgstab"/"gmres"
-        with node block-Jacobi and the per-iteration direct fallback of
+        ``linsolve``: "direct" (SuperLU) or "bicgstab"/"gmres" with node
+        block-Jacobi and the per-iteration direct fallback of
         device3d.py:2146-2168."""
         if self.psi is None:
             self.solve_equilibrium()
@@ -643,14 +592,7 @@ class OracleDevice:
             F, J, _, _ = self.residual_jacobian(psi, n, p, cur)
             Jd, rhs = eliminate_csr(J, -F, self.fixed)
             du = None
-            if linsolve == "lu_reuse":
-                if getattr(self, "lu_reuse", None) is None:
-                    self.lu_reuse = ReusedLU()
-                sc = np.ones(3 * self.N)
-                sc[1::3] = n.ravel()
-                sc[2::3] = p.ravel()
-                du = self.lu_reuse.solve(Jd, rhs, scale=sc)
-            elif linsolve != "direct":
+            if linsolve != "direct":
                 x, its, ok, _ = solve_linear_iterative(
                     Jd, rhs, method=linsolve, rtol=rtol)
                 self.krylov_iters.append(its)

@@ -530,7 +530,10 @@ class Worker(threading.Thread):
                 still.append(r)
         self.active = still
         self.rounds += 1
-        self.round_log.append((t0, now, len(sessions), len(new)))
+        self.round_log.append((t0, now, len(sessions), len(new),
+                               max(rr["iters"] for rr in res),
+                               sum(1 for rr in res if not rr["converged"]),
+                               sum(s_.setup.N for s_ in sessions)))
         return True
 
     def run(self):

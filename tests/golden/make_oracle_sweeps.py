@@ -6,6 +6,13 @@ direct path inside a GPU test, so they are solved once here by the oracle
 assembly and to its converged states by tests/test_oracle_golden.py) and
 committed as small .npz files:
 
+* ``trigate_ds.npz`` -- the tri-gate Id-Vg workload (tcad_b200.workloads.
+  trigate3d) down-scaled to 40 x 24 x 16 nodes (15,360; the bench's --small
+  size): equilibrium, then Vg = 0 .. 1.0 V in 0.05 V steps at Vd = 0.05 V and
+  at Vd = 0.7 V, each sweep from equilibrium (pytcad/finfet3d.py:246-263);
+* ``pin_ds.npz`` -- the p-i-n forward sweep (tcad_b200.workloads.pin3d,
+  SRH + Auger, doping mobility) down-scaled to 48 x 24 x 12 nodes: 0 .. 0.9 V
+  in 0.1 V steps;
 * ``mosfet_batch_oracle.npz`` -- eight instances of the seeded 512-MOSFET
   batch (tcad_b200.workloads.mosfet_batch_params, seed 2026): the smallest
   and largest meshes, the extreme body and source/drain dopings, the
@@ -13,13 +20,19 @@ committed as small .npz files:
   same 4-step ramp (tcad_b200.workloads.ramp) as the batched GPU solve,
   Newton steps solved by SuperLU.
 
+The 3D meshes are the largest whose sweeps the oracle's direct solves finish
+in minutes per point on one host core: a SuperLU factorisation of the coupled
+3D system grows from 0.5 s at 3,840 nodes to about a minute at 30k and
+several minutes (9 GB of factors) at the 71,680-node 64 x 40 x 28 mesh,
+where a 42-point sweep of ~6 Newton steps per point would take most of a day.
+
 Every converged state is solved to the update test 1e-12 (a stock
 NewtonOptions value, as for the reference-run sweep fixtures: at 1e-8 the
 update test saturates at the 1e-10 density floor).  Each fixture holds the
 terminal currents and (psi, n, p) at a seeded sample of nodes (the whole
 fields would be several MB).
 
-Usage:  python tests/golden/make_oracle_sweeps.py [mosfets]
+Usage:  python tests/golden/make_oracle_sweeps.py [mosfets] [trigate] [pin]
 """
 import multiprocessing as mp
 import os
@@ -36,7 +49,11 @@ for p in (ROOT, os.path.dirname(HERE)):
 
 TOL = 1e-12
 N_SAMPLE_2D = 512
+N_SAMPLE_3D = 1024
 BATCH_RAMP = 4
+TRIGATE_SHAPE = (40, 24, 16)
+TRIGATE_FIELD_POINTS = (0, 4, 8, 12, 16, 20)   # Vg indices whose fields are stored
+PIN_SHAPE = (48, 24, 12)
 
 
 def _log(msg):
@@ -115,7 +132,73 @@ def job_mosfets():
                         steps=np.array([r["steps"] for r in res]), ramp=BATCH_RAMP)
 
 
-JOBS = {"mosfets": job_mosfets}
+def job_trigate(vd_index):
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    dev = W.trigate3d(tb.Device3D, *TRIGATE_SHAPE)
+    ora = _oracle(dev)
+    idx = sample_nodes(ora.N, N_SAMPLE_3D, 402416)
+    t = time.time()
+    ora.solve_equilibrium()
+    _log(f"trigate equilibrium {time.time() - t:.1f} s ({ora.eq_iters} steps)")
+    psi_eq = ora.psi.ravel()[idx].copy()
+    vd = W.TRIGATE_VD[vd_index]
+    I = {c: [] for c in ("drain", "source", "body")}
+    F, iters = [], []
+    for q, vg in enumerate(W.TRIGATE_VG):
+        t = time.time()
+        ora.solve_bias(W.trigate_bias(vd, vg), tol=TOL)
+        assert ora.last_converged, (vd, vg)
+        for c in I:
+            I[c].append(ora.terminal_current(c))
+        iters.append(ora.newton_iters)
+        if q in TRIGATE_FIELD_POINTS:
+            F.append(np.stack(_fields(ora, idx)))
+        _log(f"trigate Vd={vd} Vg={vg}: {ora.newton_iters} steps, {time.time() - t:.1f} s, "
+             f"Id={I['drain'][-1]:.9e}")
+    return dict(idx=idx, psi_eq=psi_eq, I_drain=np.array(I["drain"]),
+                I_source=np.array(I["source"]), I_body=np.array(I["body"]),
+                fields=np.array(F), iters=np.array(iters))
+
+
+def job_trigate_both():
+    from tcad_b200 import workloads as W
+    with mp.get_context("spawn").Pool(2) as pool:
+        a, b = pool.map(job_trigate, [0, 1])
+    assert np.array_equal(a["idx"], b["idx"])
+    np.savez_compressed(
+        os.path.join(HERE, "trigate_ds.npz"), shape=np.array(TRIGATE_SHAPE), tol=TOL,
+        Vg=np.array(W.TRIGATE_VG), Vd=np.array(W.TRIGATE_VD), idx=a["idx"],
+        psi_eq=a["psi_eq"], field_points=np.array(TRIGATE_FIELD_POINTS),
+        **{k: np.stack([a[k], b[k]]) for k in ("I_drain", "I_source", "I_body", "fields",
+                                               "iters")})
+
+
+def job_pin():
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    dev = W.pin3d(tb.Device3D, *PIN_SHAPE)
+    ora = _oracle(dev)
+    idx = sample_nodes(ora.N, N_SAMPLE_3D, 482412)
+    t = time.time()
+    ora.solve_equilibrium(tol=TOL)
+    _log(f"pin equilibrium {time.time() - t:.1f} s ({ora.eq_iters} steps)")
+    psi_eq = ora.psi.ravel()[idx].copy()
+    I, F, iters = [], [], []
+    for V in W.PIN_SWEEP:
+        t = time.time()
+        ora.solve_bias({"anode": V}, tol=TOL)
+        assert ora.last_converged, V
+        I.append(ora.terminal_current("anode"))
+        iters.append(ora.newton_iters)
+        F.append(np.stack(_fields(ora, idx)))
+        _log(f"pin V={V}: {ora.newton_iters} steps, {time.time() - t:.1f} s, I={I[-1]:.9e}")
+    np.savez_compressed(os.path.join(HERE, "pin_ds.npz"), shape=np.array(PIN_SHAPE), tol=TOL,
+                        idx=idx, psi_eq=psi_eq, V=np.array(W.PIN_SWEEP), I_anode=np.array(I),
+                        fields=np.array(F), iters=np.array(iters))
+
+
+JOBS = {"mosfets": job_mosfets, "trigate": job_trigate_both, "pin": job_pin}
 
 
 if __name__ == "__main__":

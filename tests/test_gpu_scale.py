@@ -8,8 +8,10 @@ not reach.
 
 Two states: the equilibrium the GPU solves, at zero bias; and a perturbed
 state (smooth +-0.3 potential, +-50 % densities) at Vd = 0.7 V, Vg = 0.6 V.
-Bar: the Jacobian within 1e-12 relative entry by entry and per row, the
-residual within 1e-12 per row on its natural scale (|J| |x| + |F|)."""
+Bar: the Jacobian within 1e-12 relative per row and entry by entry (except
+the rare entries where the reference's B'(x) formula amplifies an ulp of
+expm1, tests/fixtures.py TOL_ENTRY_CANCEL), the residual within 1e-12 per
+row on its natural scale (|J| |x| + |F|)."""
 import numpy as np
 import pytest
 
@@ -54,11 +56,99 @@ def test_trigate_full_mesh_assembly():
         Fo, Jo, Fno, Fpo = ora.residual_jacobian(psi, n, p, {k: v for k, v in volts.items()
                                                              if k in ora.contacts})
         assert np.array_equal(np.sort(dev._dirichlet_rows), np.sort(ora.fixed))
-        e_elem, n_cmp = fx.elem_err(J, Jo)
-        assert n_cmp == np.count_nonzero(Jo.data) and e_elem < TOL_ASM, (e_elem, n_cmp)
+        e_elem, n_cmp, frac = fx.elem_err(J, Jo)
+        assert n_cmp == np.count_nonzero(Jo.data)
+        assert e_elem < fx.TOL_ENTRY_CANCEL and frac <= fx.TOL_ENTRY_FRACTION, (e_elem, frac)
         assert fx.rownorm_err(J, Jo) < TOL_ASM
         x = np.stack([psi.ravel(), n.ravel(), p.ravel()], axis=1).ravel()
         assert _rownorm_vec(F, Jo, x, Fo) < TOL_ASM
         for mine, ref in ((F_n.ravel(), Fno.ravel()), (F_p.ravel(), Fpo.ravel())):
             assert fx.vec_err(mine, ref, 1e-12 * np.abs(ref).max()) < 1e-10
         del out, F, J, Fo, Jo
+
+
+def _rel_err(I, ref, floor_frac=1e-9):
+    I, ref = np.asarray(I, float), np.asarray(ref, float)
+    scale = np.maximum(np.abs(ref), floor_frac * np.abs(ref).max())
+    return float((np.abs(I - ref) / np.where(scale == 0, 1.0, scale)).max())
+
+
+def _check_fields(VT, state, ref, what):
+    e_psi, e_n, e_p = fx.field_errs(*state, *ref)
+    assert e_psi * VT < 1e-9, (what, e_psi * VT)
+    assert max(e_n, e_p) * VT < 1e-8, (what, e_n * VT, e_p * VT)
+
+
+@pytest.mark.parametrize("batched", [False, True])
+def test_trigate_downscaled_sweeps_match_oracle(batched):
+    """The tri-gate Id-Vg workload at 40 x 24 x 16 (tests/golden/trigate_ds.npz,
+    the oracle's exact-Newton sweeps, tests/golden/make_oracle_sweeps.py): both
+    Vd branches from equilibrium, 21 points each, with the default (chosen)
+    Newton options; alone, one device per branch, and batched, both branches
+    in ONE 2-instance pack (the bench's headline form).  Drain, source and
+    body currents within 1e-6 (on 1e-9 x the sweep's largest), psi within
+    1e-9 V and the quasi-Fermi levels within 1e-8 V at the sampled nodes."""
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    from tcad_b200.batch import DeviceBatch
+    g = fx.load("trigate_ds")
+    shape = tuple(int(v) for v in g["shape"])
+    idx = g["idx"]
+    fpts = list(g["field_points"])
+    opts = tb.NewtonOptions()
+    lanes = [W.trigate3d(tb.Device3D, *shape) for _ in W.TRIGATE_VD]
+    VT = lanes[0].VT
+    cur = {c: np.zeros((2, len(W.TRIGATE_VG))) for c in ("drain", "source", "body")}
+    if batched:
+        b = DeviceBatch(lanes)
+        b.solve_equilibrium(opts)
+        for a in range(2):
+            assert np.abs(b.state(a)[0].ravel()[idx] - g["psi_eq"]).max() * VT < 1e-9
+        for q, vg in enumerate(W.TRIGATE_VG):
+            res = b.solve_bias([W.trigate_bias(vd, vg) for vd in W.TRIGATE_VD], opts)
+            assert all(r["converged"] for r in res), vg
+            for c in cur:
+                cur[c][:, q] = b.terminal_currents(c)
+            if q in fpts:
+                for a in range(2):
+                    st = [t.ravel()[idx] for t in b.state(a)]
+                    _check_fields(VT, st, g["fields"][a][fpts.index(q)], (a, vg))
+    else:
+        for a, (dev, vd) in enumerate(zip(lanes, W.TRIGATE_VD)):
+            dev.solve_equilibrium(opts)
+            assert np.abs(dev.psi.ravel()[idx] - g["psi_eq"]).max() * VT < 1e-9
+            for q, vg in enumerate(W.TRIGATE_VG):
+                dev.solve_bias(W.trigate_bias(vd, vg), opts)
+                assert dev.last_converged, (vd, vg)
+                for c in cur:
+                    cur[c][a, q] = dev.terminal_current(c)
+                if q in fpts:
+                    st = [t.ravel()[idx] for t in (dev.psi, dev.n, dev.p)]
+                    _check_fields(VT, st, g["fields"][a][fpts.index(q)], (vd, vg))
+    for c in cur:
+        for a in range(2):
+            err = _rel_err(cur[c][a], g["I_" + c][a])
+            assert err < 1e-6, (c, a, err)
+
+
+def test_pin_downscaled_sweep_matches_oracle():
+    """The p-i-n forward sweep (SRH + Auger, doping mobility, erfc junctions)
+    at 48 x 24 x 12 against the oracle's exact-Newton sweep
+    (tests/golden/pin_ds.npz): every point's anode current within 1e-6,
+    psi within 1e-9 V and the quasi-Fermi levels within 1e-8 V at the
+    sampled nodes, default Newton options."""
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    g = fx.load("pin_ds")
+    dev = W.pin3d(tb.Device3D, *(int(v) for v in g["shape"]))
+    idx = g["idx"]
+    dev.solve_equilibrium()
+    assert np.abs(dev.psi.ravel()[idx] - g["psi_eq"]).max() * dev.VT < 1e-9
+    I = []
+    for k, V in enumerate(g["V"]):
+        dev.solve_bias({"anode": float(V)})
+        assert dev.last_converged, V
+        I.append(dev.terminal_current("anode"))
+        st = [t.ravel()[idx] for t in (dev.psi, dev.n, dev.p)]
+        _check_fields(dev.VT, st, g["fields"][k], V)
+    assert _rel_err(I, g["I_anode"]) < 1e-6

@@ -88,7 +88,7 @@ def test_served_results_equal_alone(precision):
             assert r.done.is_set()
         _check(reqs, ref)
         w2 = srv.workers[2]
-        assert w2.rounds >= 3 and max(n for _, _, n, _ in w2.round_log) >= 2
+        assert w2.rounds >= 3 and max(e[2] for e in w2.round_log) >= 2
     finally:
         srv.stop()
 
@@ -111,7 +111,7 @@ def test_admission_waits_for_arena_room():
         assert srv.wait_idle(300)
         _check(reqs, ref)
         w2 = srv.workers[2]
-        assert max(n for _, _, n, _ in w2.round_log) <= 2
+        assert max(e[2] for e in w2.round_log) <= 2
     finally:
         srv.stop()
 
