@@ -66,6 +66,9 @@ extern "C" {
 /* assembly modes */
 #define TCAD_MODE_RAW 0        /* reference _residual_jacobian rows, BC rows stamped */
 #define TCAD_MODE_ELIMINATE 1  /* + symmetric Dirichlet elimination (pytcad/dirichlet.py:270) */
+#define TCAD_MODE_UNSTAMPED 2  /* contact rows left as assembled continuity/Poisson rows: the
+                                  raw current rows the AC sensitivities sum
+                                  (current_rows_for, pytcad/device2d.py:1751-1758) */
 
 /* bcflag bits */
 #define TCAD_BC_CONTACT 1
@@ -266,8 +269,9 @@ int tcad_block_krylov(const tcad_pack_t* pk, const double* J, const double* b,
  * Solve A x = b for one n x n CSR matrix (int32 indices, device memory),
  * x holding the initial guess.  method 0: BiCGStab (maxiter iterations),
  * 1: GMRES(restart) (maxiter restart cycles), both right-preconditioned by
- * node-block-Jacobi when block_size == 3 divides n (point Jacobi otherwise or
- * when a block is singular; *precond_out = 3, 1 or 0), stopping at
+ * node-block-Jacobi when block_size (3, or 6: the real-equivalent form of a
+ * complex 3 x 3 node block) divides n (point Jacobi otherwise or when a
+ * block is singular; *precond_out = 6, 3, 1 or 0), stopping at
  * ||b - A x|| <= max(atol, rtol ||b||) (pytcad/linsolve.py:941-985).
  * *resid_out = true ||b - A x|| / ||b||.  Returns TCAD_ERR_NOCONV when the
  * tolerance was not met (x then holds the last iterate). */

@@ -28,7 +28,7 @@ NE = {2: 29, 3: 39}
 FLAT_NODES = 512
 TILE_X, TILE_Y, TILE_Z_MAX = 32, 8, 16
 NPAR = 8
-MODE_RAW, MODE_ELIMINATE = 0, 1
+MODE_RAW, MODE_ELIMINATE, MODE_UNSTAMPED = 0, 1, 2
 BC_CONTACT, BC_GATE = 1, 2
 
 _p = ctypes.c_void_p

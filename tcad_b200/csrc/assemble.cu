@@ -152,7 +152,7 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
       const uint8_t flag = s_flag[ty + 1][tx + 1];
       double* __restrict__ Jk = J + k;
       auto st = [&](int e, double v) { Jk[(int64_t)e * NN] = v; };
-      if (flag & TCAD_BC_CONTACT) {
+      if ((flag & TCAD_BC_CONTACT) && mode != TCAD_MODE_UNSTAMPED) {
         F[k] = cur.psi - pk.bc_psi0[k];
         F[NN + k] = cur.n - pk.bc_n0[k];
         F[2 * NN + k] = cur.p - pk.bc_p0[k];
@@ -591,6 +591,8 @@ using namespace tcad;
 extern "C" int tcad_sg_assemble(const tcad_pack_t* pk, const double* psi, const double* n,
                                 const double* p, double* F, double* J, int mode,
                                 void* stream) {
+  if (mode != TCAD_MODE_RAW && mode != TCAD_MODE_ELIMINATE && mode != TCAD_MODE_UNSTAMPED)
+    return TCAD_ERR_ARG;
   return sg_assemble_tiles(pk, psi, n, p, F, J, mode, nullptr, 0, (cudaStream_t)stream);
 }
 

@@ -81,7 +81,66 @@ __global__ void k_bj_setup(Sys A, int bs, double* __restrict__ inv, int* __restr
   o[8] = (a[0] * a[4] - a[1] * a[3]) * id;
 }
 
-// z = M^-1 r (bs = 3 blocks, bs = 1 diagonal, bs = 0 identity)
+// 6 x 6 node blocks (the real-equivalent form of a complex 3 x 3 node block:
+// the AC small-signal systems), inverted by Gauss-Jordan elimination with
+// partial pivoting in registers.
+__global__ void k_bj_setup6(Sys A, double* __restrict__ inv, int* __restrict__ flag) {
+  const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nb = A.n / 6;
+  if (b >= nb) return;
+  double a[36], o[36];
+#pragma unroll
+  for (int q = 0; q < 36; ++q) {
+    a[q] = 0.0;
+    o[q] = (q % 7 == 0) ? 1.0 : 0.0;
+  }
+  for (int r = 0; r < 6; ++r) {
+    const int64_t row = b * 6 + r;
+    for (int q = A.ptr[row]; q < A.ptr[row + 1]; ++q) {
+      const int64_t c = A.idx[q] - b * 6;
+      if (c >= 0 && c < 6) a[r * 6 + c] += A.val[q];
+    }
+  }
+  double scale = 0.0;
+#pragma unroll
+  for (int q = 0; q < 36; ++q) scale = fmax(scale, fabs(a[q]));
+  bool ok = isfinite(scale) && scale > 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    int piv = k;
+    double best = fabs(a[k * 6 + k]);
+#pragma unroll
+    for (int r = k + 1; r < 6; ++r)
+      if (fabs(a[r * 6 + k]) > best) { best = fabs(a[r * 6 + k]); piv = r; }
+    if (!(best > 1e-300 * scale)) ok = false;
+    if (piv != k) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        double t = a[k * 6 + c]; a[k * 6 + c] = a[piv * 6 + c]; a[piv * 6 + c] = t;
+        t = o[k * 6 + c]; o[k * 6 + c] = o[piv * 6 + c]; o[piv * 6 + c] = t;
+      }
+    }
+    const double ip = ok ? 1.0 / a[k * 6 + k] : 0.0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) { a[k * 6 + c] *= ip; o[k * 6 + c] *= ip; }
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      if (r == k) continue;
+      const double f = a[r * 6 + k];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        a[r * 6 + c] -= f * a[k * 6 + c];
+        o[r * 6 + c] -= f * o[k * 6 + c];
+      }
+    }
+  }
+  if (!ok) atomicExch(flag, 1);
+  double* out = inv + 36 * b;
+#pragma unroll
+  for (int q = 0; q < 36; ++q) out[q] = ok ? o[q] : 0.0;
+}
+
+// z = M^-1 r (bs = 3 or 6 blocks, bs = 1 diagonal, bs = 0 identity)
 __global__ void k_bj_apply(int64_t n, int bs, const double* __restrict__ inv,
                            const double* __restrict__ r, double* __restrict__ z) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -92,6 +151,19 @@ __global__ void k_bj_apply(int64_t n, int bs, const double* __restrict__ inv,
     z[3 * t] = m[0] * a + m[1] * b + m[2] * c;
     z[3 * t + 1] = m[3] * a + m[4] * b + m[5] * c;
     z[3 * t + 2] = m[6] * a + m[7] * b + m[8] * c;
+  } else if (bs == 6) {
+    if (t >= n / 6) return;
+    const double* m = inv + 36 * t;
+    double v[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) v[c] = r[6 * t + c];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      double acc = 0.0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) acc += m[6 * q + c] * v[c];
+      z[6 * t + q] = acc;
+    }
   } else if (t < n) {
     z[t] = bs == 1 ? inv[t] * r[t] : r[t];
   }
@@ -223,7 +295,8 @@ int spmv(const Ctx& c, const double* x, double* y) {
 
 int prec(const Ctx& c, const double* r, double* z) {
   const int64_t n = c.A.n;
-  k_bj_apply<<<g1(c.bs == 3 ? n / 3 : n), NT, 0, c.s>>>(n, c.bs, c.inv, r, z);
+  k_bj_apply<<<g1(c.bs == 3 ? n / 3 : (c.bs == 6 ? n / 6 : n)), NT, 0, c.s>>>(n, c.bs,
+                                                                               c.inv, r, z);
   note_launch();
   return TCAD_OK;
 }
@@ -249,7 +322,8 @@ int axpy(const Ctx& c, double a, const double* x, double b, double* y, double cc
 extern "C" size_t tcad_csr_workspace_bytes(int64_t n, int method, int restart) {
   const int m = restart > 0 ? restart : 100;
   size_t vec = (size_t)n * sizeof(double);
-  size_t v = 9 * (size_t)n * sizeof(double);        // block inverses (upper bound)
+  size_t v = 9 * (size_t)n * sizeof(double);        // block inverses (upper bound: 3n
+                                                     // for 3 x 3 blocks, 6n for 6 x 6)
   if (method == 0) v += 8 * vec;                     // BiCGStab vectors
   else v += (size_t)(m + 1) * vec + 3 * vec;         // GMRES basis + work
   v += 4096 * 4 * sizeof(double) + 64 * sizeof(double) + 256;
@@ -287,17 +361,20 @@ extern "C" int tcad_csr_krylov(int64_t n, const int32_t* indptr, const int32_t* 
   int* flag = reinterpret_cast<int*>(c.ticket + 16);
   TCAD_CUDA_CHECK(cudaMemsetAsync(c.ticket, 0, 256, s));
   // preconditioner: node blocks, else point Jacobi, else none
-  c.bs = (block_size == 3 && n % 3 == 0) ? 3 : 1;
+  c.bs = ((block_size == 3 || block_size == 6) && n % block_size == 0) ? block_size : 1;
   for (;;) {
     TCAD_CUDA_CHECK(cudaMemsetAsync(flag, 0, sizeof(int), s));
     const int64_t nb = n / c.bs;
-    k_bj_setup<<<g1(nb), NT, 0, s>>>(c.A, c.bs, c.inv, flag);
+    if (c.bs == 6)
+      k_bj_setup6<<<g1(nb), NT, 0, s>>>(c.A, c.inv, flag);
+    else
+      k_bj_setup<<<g1(nb), NT, 0, s>>>(c.A, c.bs, c.inv, flag);
     note_launch();
     int hflag = 0;
     TCAD_CUDA_CHECK(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
     if (!hflag) break;
-    if (c.bs == 3) c.bs = 1;
+    if (c.bs == 3 || c.bs == 6) c.bs = 1;
     else { c.bs = 0; break; }
   }
   if (precond_out) *precond_out = c.bs;

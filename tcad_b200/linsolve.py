@@ -92,4 +92,5 @@ def solve_linear(A, b, *, method="direct", rtol=1e-10, atol=0.0, maxiter=500,
             "unconverged iterate")
     return x, {"method": method, "iterations": int(iters.value), "converged": True,
                "residual": res,
-               "precond": {3: "block_jacobi", 1: "jacobi", 0: "none"}[int(pc.value)]}
+               "precond": {6: "block_jacobi", 3: "block_jacobi", 1: "jacobi",
+                           0: "none"}[int(pc.value)]}

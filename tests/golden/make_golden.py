@@ -504,6 +504,28 @@ def mosfet_small(pt, out):
     np.savez_compressed(out, **_dump_dev(dev, 2, extra))
 
 
+def ac_small(pt, out):
+    """pytcad.ac2d.y_parameters of the small 2D MOSFET of mosfet_small, biased
+    on (drain 0.5 V, gate 0.8 V): the full 4-port complex Y matrix (source,
+    drain, body ohmic ports and the gate port, in device.bcs order) at
+    1 Hz .. 100 GHz, plus the DC state it linearises about."""
+    from pytcad.mosfet import build_mosfet
+    from pytcad.device import NewtonOptions
+    from pytcad.ac2d import y_parameters
+    dev = build_mosfet(Lg=0.1e-4, Lsd=0.1e-4, depth=0.2e-4, Na=1e17,
+                       Nsd_peak=1e20, tox_cm=3e-7, nx=16, ny=10)
+    opts = NewtonOptions(linsolve="direct", tol_update=SWEEP_TOL)
+    dev.solve_equilibrium(opts)
+    bias = {"drain": 0.5, "gate": 0.8}
+    dev.solve_bias(bias, opts)
+    freqs = np.array([1.0, 1e6, 1e9, 1e10, 3e10, 1e11])
+    r = y_parameters(dev, freqs)
+    extra = dict(freqs=freqs, Y=r.Y, ports=np.array(r.port_names), Vd=0.5, Vg=0.8,
+                 tol_update=SWEEP_TOL, psi_dc=dev.psi.ravel().copy(),
+                 n_dc=dev.n.ravel().copy(), p_dc=dev.p.ravel().copy())
+    np.savez_compressed(out, **_dump_dev(dev, 2, extra))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("PYTCAD_REF"),
@@ -520,6 +542,7 @@ def main():
             ("transient_small", transient_small),
             ("transient3d_small", transient3d_small),
             ("transient_growth", transient_growth),
+            ("ac_small", ac_small),
             ("diode_c1", diode_c1)]
     for name, fn in jobs:
         if a.only and name not in a.only.split(","):

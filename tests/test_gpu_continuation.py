@@ -52,3 +52,40 @@ def test_adaptive_sweep_backs_off_and_matches_ordered_solves():
         assert ref.last_converged
         I = ref.terminal_current("anode")
         assert abs(r["I"] - I) <= 1e-6 * abs(I), (r["V"], r["I"], I)
+
+
+def test_arc_length_sweep_lies_on_the_oracle_branch():
+    """Pseudo-arclength continuation (the bordered corrector on the GPU
+    Jacobian) along the 41x11 diode's forward branch 0 -> 0.6 V: every
+    traced (V, I) lies on the oracle's voltage-controlled solution at that
+    V (exact Newton to 1e-12), within 1e-6 relative; the branch has no
+    fold, so V increases monotonically, and the trace reaches v_end."""
+    import numpy as np
+    import fixtures as fx
+    from tcad_b200.continuation import arc_length_sweep
+    dev = _diode()
+    dev.solve_equilibrium()
+    recs = arc_length_sweep(dev, "anode", 0.0, 0.6, 0.05)
+    V = np.array([r["V"] for r in recs])
+    assert V[-1] >= 0.6 and np.all(np.diff(V) > 0)
+    assert len(recs) >= 6
+    ora = fx.oracle_from_device(dev)
+    ora.contacts["anode"][1] = 0.0
+    ora.solve_equilibrium()
+    for r in recs:
+        ora.solve_bias({"anode": r["V"]}, tol=1e-12)
+        Iref = ora.terminal_current("anode")
+        assert abs(r["I"] - Iref) <= 1e-6 * max(abs(Iref), 1e-12), (r["V"], r["I"], Iref)
+
+
+def test_arc_length_sweep_stalls_loudly():
+    """A corrector that cannot converge (one Newton step allowed) halves ds
+    down to ds_min and raises ArcLengthStalled with the traced records."""
+    import pytest as _pt
+    from tcad_b200.continuation import ArcLengthStalled, arc_length_sweep
+    dev = _diode()
+    dev.solve_equilibrium()
+    with _pt.raises(ArcLengthStalled) as ei:
+        arc_length_sweep(dev, "anode", 0.0, 0.6, 0.2, corrector_tol=1e-30,
+                         corrector_max_iter=1, ds_min=0.05)
+    assert len(ei.value.last_records) == 2 and ei.value.last_V > 0.0
