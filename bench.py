@@ -77,7 +77,7 @@ METHOD_DESC = {
              "(dpsi, dn, dp) every Newton step, damped Newton",
     "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the block-scaled system in "
             "relative unknowns (dpsi, dn/n, dp/p) solved to 1e-3 every Newton step, two "
-            "polishing steps (1e-10, then 1e-3), secant predictor along the sweep",
+            "polishing steps (1e-6, then 1e-3), secant predictor along the sweep",
     "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
              "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
              "relative unknowns, adaptive forcing, secant predictor; per-instance FP64 "
@@ -809,7 +809,8 @@ def run_serve(args):
     def round_stats(log):
         if not log:
             return {"rounds": 0}
-        a = np.array([(t1 - t0, n, nn, it, nf, nodes) for t0, t1, n, nn, it, nf, nodes in log])
+        a = np.array([(t1 - t0, n, nn, it, nf, nodes, teq, kit)
+                      for t0, t1, n, nn, it, nf, nodes, teq, kit in log])
         return {"rounds": len(log), "mean_instances": float(a[:, 1].mean()),
                 "max_instances": int(a[:, 1].max()), "new_devices": int(a[:, 2].sum()),
                 "round_s_p50": float(np.median(a[:, 0])), "round_s_max": float(a[:, 0].max()),
@@ -817,7 +818,9 @@ def run_serve(args):
                 "newton_iters_max_p50": float(np.median(a[:, 3])),
                 "newton_iters_max": int(a[:, 3].max()),
                 "unconverged_instances": int(a[:, 4].sum()),
-                "mean_round_nodes": float(a[:, 5].mean())}
+                "mean_round_nodes": float(a[:, 5].mean()),
+                "equilibrium_s_total": float(a[:, 6].sum()),
+                "krylov_iters_max_p50": float(np.median(a[:, 7]))}
     rounds = {d: round_stats(w.round_log) for d, w in srv.workers.items()}
     value = pts_conv / elapsed
 

@@ -457,9 +457,11 @@ class Worker(threading.Thread):
                     self.h2d_bytes += g.numel() * 8
                 s.fresh_guess = False
             RoundPack(self.arena, new).equilibrium(self.opts)
+            self.stream.synchronize()
             for s in new:
                 s.need_eq = False
                 s.bias_prev, s.bias_cur = None, np.zeros(len(s.setup.bcs))
+        t_eq = time.perf_counter() - t0
         sessions = [r._session for r in self.active]
         for r in self.active:
             for name, V in r.points[r.next].items():
@@ -533,7 +535,8 @@ class Worker(threading.Thread):
         self.round_log.append((t0, now, len(sessions), len(new),
                                max(rr["iters"] for rr in res),
                                sum(1 for rr in res if not rr["converged"]),
-                               sum(s_.setup.N for s_ in sessions)))
+                               sum(s_.setup.N for s_ in sessions), t_eq,
+                               max(rr["krylov_iters"] for rr in res)))
         return True
 
     def run(self):
@@ -567,10 +570,14 @@ class Worker(threading.Thread):
             self.active = []
 
 
-# Default cap of the nodes one round solves: large enough that every kernel
-# streams from HBM at full rate, small enough that a round (one bias point
-# of each member) stays short and new requests join often.
-ROUND_NODES = {2: 8_000_000, 3: 4_000_000}
+# Default cap of the nodes one round solves.  A 2D round's time is set by its
+# deepest member's ILU(0) sweeps (one dependent level per anti-diagonal, up to
+# 767 for 512 x 256) far more than by its node count (a 2D block SpMV streams
+# 8M nodes in ~0.3 ms): measured at 200 req/s, rounds of ~160 devices (6.4M
+# nodes) took 7 s at the median.  So a round takes as many devices as the cap
+# allows: 32M nodes (a quarter of a 160 GB 2D arena).  3D rounds (block
+# Jacobi, no sweeps) scale with their nodes and stay at 4M.
+ROUND_NODES = {2: 32_000_000, 3: 4_000_000}
 
 
 class Server:

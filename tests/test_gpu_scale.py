@@ -62,8 +62,13 @@ def test_trigate_full_mesh_assembly():
         assert fx.rownorm_err(J, Jo) < TOL_ASM
         x = np.stack([psi.ravel(), n.ravel(), p.ravel()], axis=1).ravel()
         assert _rownorm_vec(F, Jo, x, Fo) < TOL_ASM
-        for mine, ref in ((F_n.ravel(), Fno.ravel()), (F_p.ravel(), Fpo.ravel())):
-            assert fx.vec_err(mine, ref, 1e-12 * np.abs(ref).max()) < 1e-10
+        # raw continuity residuals (the terminal-current source) per row on
+        # the row's natural scale: at equilibrium they are round-off noise
+        nat = np.asarray(abs(Jo) @ np.abs(x)).ravel()
+        for c, mine, ref in ((1, F_n.ravel(), Fno.ravel()), (2, F_p.ravel(), Fpo.ravel())):
+            scale = nat[c::3] + np.abs(ref)
+            assert float((np.abs(mine - ref) / np.where(scale == 0, 1.0, scale)).max()) \
+                < TOL_ASM, c
         del out, F, J, Fo, Jo
 
 

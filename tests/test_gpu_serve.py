@@ -166,3 +166,36 @@ def test_requests_sharing_a_setup_keep_their_own_bias():
         _check([ra, rb], ref)
     finally:
         srv.stop()
+
+
+def test_served_requests_match_the_oracle():
+    """One request of each kind served together -- a single-bias 2D MOSFET
+    solve (3-step ramp), a warm-started 2D Id-Vg sweep, a small 3D tri-gate
+    solve -- against the oracle's exact-Newton solutions of the same
+    devices and bias points (update test 1e-12): every reported current
+    within 1e-6 and the final psi within 1e-9 V."""
+    import fixtures as fx
+    import tcad_b200 as tb
+    from tcad_b200.serve import Request, Server
+    opts = tb.NewtonOptions()
+    cases = [c for c in _cases() if c[0] in ("mos1", "sweep", "tri")]
+    ref = {}
+    for key, build, pts, rep, contact in cases:
+        dev = build()
+        ora = fx.oracle_from_device(dev)
+        ora.solve_equilibrium(tol=1e-12)
+        I = []
+        for v, r_ in zip(pts, rep):
+            ora.solve_bias(v, tol=1e-12)
+            assert ora.last_converged, (key, v)
+            if r_:
+                I.append(ora.terminal_current(contact))
+        ref[key] = (np.array(I), ora.psi.copy(), dev.VT)
+    srv = Server(budget={2: 64 << 20, 3: 64 << 20}, opts=opts).start()
+    try:
+        reqs = [srv.submit(Request(key, build().setup, pts, contact, rep, return_state=True))
+                for key, build, pts, rep, contact in cases]
+        assert srv.wait_idle(timeout=300)
+    finally:
+        srv.stop()
+    _check(reqs, ref)
