@@ -112,6 +112,8 @@ def parse():
                     help="the timed (chosen) path; the plain FP64 path is always run "
                          "beside it on the same points for the current check")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--asm-stage", type=int, default=0, choices=(0, 1),
+                    help="--kernels: the 3D assembly's plane staging (pack asm_stage)")
     ap.add_argument("--kernels", action="store_true",
                     help="profiling mode: assembly, block-Jacobi set-up and 20 BiCGStab "
                          "iterations on the full-size workload at its bulk-guess state")
@@ -1080,6 +1082,7 @@ def run_kernels(args):
                                              tb.Device3D)
     dev = lanes[0]
     pk = dev.pack
+    pk.set_asm_stage(args.asm_stage)
     s = dev.setup
     g = s.bulk_guess()
     pk.psi.copy_(dev._to_dev(g))

@@ -83,6 +83,11 @@ typedef struct tcad_pack {
   int32_t tile_z;        /* z planes one 3D tile marches (1..TCAD_TILE_Z; the tiles'
                             k0 are multiples of it); 1 in 2D */
   int32_t flat_nodes;    /* nodes per flat block (>= 1; each instance starts a block) */
+  int32_t asm_stage;     /* 3D coupled assembly: 0 loads each plane's edge and node
+                            coefficients where it uses them; 1 stages the next plane's
+                            into shared memory with asynchronous copies while the
+                            current plane computes (same arithmetic, bit-identical) */
+  int32_t reserved;      /* 0 */
   /* per-instance tables (device memory) */
   const int32_t* shape;    /* [3*n_inst] Nx, Ny, Nz (Nz = 1 in 2D) */
   const int64_t* node_off; /* [n_inst+1] first node of each instance, increasing;

@@ -40,7 +40,8 @@ class TcadPack(ctypes.Structure):
         ("dim", ctypes.c_int32), ("n_inst", ctypes.c_int32),
         ("n_nodes", ctypes.c_int64), ("n_flat", ctypes.c_int64),
         ("n_tiles", ctypes.c_int64), ("tile_z", ctypes.c_int32),
-        ("flat_nodes", ctypes.c_int32),
+        ("flat_nodes", ctypes.c_int32), ("asm_stage", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
         ("shape", _p), ("node_off", _p), ("flat_off", _p), ("flat_inst", _p),
         ("axis_off", _p), ("tile", _p), ("par", _p),
         ("h", _p * 3), ("dv", _p * 3),

@@ -23,17 +23,52 @@ struct NodeVals {
 // Neighbour-block entry offsets: 9 + 5*d + m.
 __device__ __forceinline__ int nb(int d, int m) { return 9 + 5 * d + m; }
 
+// ---- asynchronous staging of a z-plane's coefficients (3D, asm_stage = 1)
+// The coefficients one plane of a tile reads -- an, ap, dl of every x- and
+// y-edge touching the tile and of each node's up z-edge, and C, n_ie, tau_n,
+// tau_p of each node -- are copied global -> shared with cp.async (8 bytes
+// per copy, coalesced across the warp, zero-filled where the edge or node
+// does not exist) one plane AHEAD: while plane k computes, plane k+1's
+// copies are in flight, so the compute phase reads shared memory instead of
+// waiting on global loads.  The values are the same, so the arithmetic and
+// its result are bit-identical to the unstaged kernel.
+struct PlaneStage {
+  double ax[3][TY][TX + 1];  // x-edge slot a of row r: edge (i0-1+a, j0+r) -> +x
+  double ay[3][TY + 1][TX];  // y-edge slot b of column c: edge (i0+c, j0-1+b) -> +y
+  double az[3][TY][TX];      // own node's edge -> +z
+  double nd[4][TY][TX];      // own node's C, n_ie, tau_n, tau_p
+};
+constexpr int kStageBytes = 2 * (int)sizeof(PlaneStage);
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid,
+                                          const double* dummy) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d),
+               "l"(valid ? src : dummy), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
 // CTAs per SM the coupled assembly is compiled for (register budget):
 // 4 in 2D (64 registers, no spills), 3 in 3D (80 registers; the z-march
 // carries two edges and two node states in registers, and at 64 registers
 // the spills cost more than the fourth CTA gains)
-template <int DIM>
-__global__ void __launch_bounds__(kTileThreads, DIM == 2 ? 4 : 3)
+template <int DIM, bool STAGED>
+__global__ void __launch_bounds__(kTileThreads, DIM == 2 ? 4 : (STAGED ? 2 : 3))
 k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
               const double* __restrict__ nn, const double* __restrict__ pp,
               double* __restrict__ F, double* __restrict__ J, int mode,
               const int32_t* __restrict__ tiles) {
+  static_assert(DIM == 3 || !STAGED, "plane staging is the 3D z-march's");
   constexpr int NE = DIM == 2 ? TCAD_NE2 : TCAD_NE3;
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  PlaneStage* const stage = reinterpret_cast<PlaneStage*>(s_dyn);
   __shared__ double s_psi[TY + 2][TX + 2], s_n[TY + 2][TX + 2], s_p[TY + 2][TX + 2];
   __shared__ uint8_t s_flag[TY + 2][TX + 2];
   __shared__ Edge s_ex[TY][TX + 1];  // x-edge slot a: nodes (i0-1+a, i0+a)
@@ -69,8 +104,59 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
             pk.dl[2][ql], pk.h[2][az0 + k0 - 1], eD);
   }
 
+  // this thread's share of plane kz's staging copies into buffer st: its own
+  // node's x-, y- and z-edge coefficients and node data, and (threads 0..7 /
+  // 8..39) the tile's west x-edge / south y-edge halo
+  auto issue = [&](int kz, PlaneStage* sb) {
+    const int64_t pl = g.off + (int64_t)kz * sxy;
+    const double* const dmy = pk.C;
+    const bool xv = (i + 1 < g.nx) && (j < g.ny);
+    const bool yv = (j + 1 < g.ny) && (i < g.nx);
+    const bool zv = own && (kz + 1 < g.nz);
+    const int64_t q = pl + (int64_t)j * g.nx + i;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double* const* arr = c == 0 ? pk.an : (c == 1 ? pk.ap : pk.dl);
+      cp_async8(&sb->ax[c][ty][tx + 1], arr[0] + q, xv, dmy);
+      cp_async8(&sb->ay[c][ty + 1][tx], arr[1] + q, yv, dmy);
+      cp_async8(&sb->az[c][ty][tx], arr[2] + q, zv, dmy);
+    }
+    cp_async8(&sb->nd[0][ty][tx], pk.C + q, own, dmy);
+    cp_async8(&sb->nd[1][ty][tx], pk.nie + q, own, dmy);
+    cp_async8(&sb->nd[2][ty][tx], pk.tau_n + q, own, dmy);
+    cp_async8(&sb->nd[3][ty][tx], pk.tau_p + q, own, dmy);
+    if (tid < TY) {                        // west halo: edge (i0-1, j0+tid) -> +x
+      const int r = tid, jj = j0 + r;
+      const bool v = i0 >= 1 && i0 < g.nx && jj < g.ny;
+      const int64_t qh = pl + (int64_t)jj * g.nx + (i0 - 1);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double* const* arr = c == 0 ? pk.an : (c == 1 ? pk.ap : pk.dl);
+        cp_async8(&sb->ax[c][r][0], arr[0] + qh, v, dmy);
+      }
+    } else if (tid < TY + TX) {            // south halo: edge (i0+col, j0-1) -> +y
+      const int col = tid - TY, ii = i0 + col;
+      const bool v = j0 >= 1 && j0 < g.ny && ii < g.nx;
+      const int64_t qh = pl + (int64_t)(j0 - 1) * g.nx + ii;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double* const* arr = c == 0 ? pk.an : (c == 1 ? pk.ap : pk.dl);
+        cp_async8(&sb->ay[c][0][col], arr[1] + qh, v, dmy);
+      }
+    }
+    cp_async_commit();
+  };
+  if constexpr (STAGED) issue(k0, &stage[0]);
+
   for (int kz = k0; kz < kend; ++kz) {
     const int64_t plane = g.off + (int64_t)kz * sxy;
+    PlaneStage* const stg = STAGED ? &stage[(kz - k0) & 1] : nullptr;
+    if constexpr (STAGED) {
+      // the buffer it fills was last read before the previous plane's final
+      // barrier; an empty group keeps the wait count uniform at the last plane
+      if (kz + 1 < kend) issue(kz + 1, &stage[(kz + 1 - k0) & 1]);
+      else cp_async_commit();
+    }
     // ---- stage the plane (tile + 1-node halo, no corners) in shared memory
     s_psi[ty + 1][tx + 1] = cur.psi;
     s_n[ty + 1][tx + 1] = cur.n;
@@ -100,6 +186,7 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
       const int64_t q = plane + sxy + (int64_t)j * g.nx + i;
       nxt = NodeVals{psi[q], nn[q], pp[q]};
     }
+    if constexpr (STAGED) cp_async_wait_one();   // this plane's copies (own thread)
     __syncthreads();
 
     // ---- evaluate every edge touching the tile once
@@ -108,9 +195,15 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
       Edge e;
       if (ilo >= 0 && ilo + 1 < g.nx && jj < g.ny) {
         const int64_t q = plane + (int64_t)jj * g.nx + ilo;
+        double an, ap, dl;
+        if constexpr (STAGED) {
+          an = stg->ax[0][row][a]; ap = stg->ax[1][row][a]; dl = stg->ax[2][row][a];
+        } else {
+          an = pk.an[0][q]; ap = pk.ap[0][q]; dl = pk.dl[0][q];
+        }
         sg_edge(s_psi[row + 1][a], s_psi[row + 1][a + 1], s_n[row + 1][a],
-                s_n[row + 1][a + 1], s_p[row + 1][a], s_p[row + 1][a + 1], pk.an[0][q],
-                pk.ap[0][q], pk.dl[0][q], pk.h[0][ax0 + ilo], e);
+                s_n[row + 1][a + 1], s_p[row + 1][a], s_p[row + 1][a + 1], an, ap, dl,
+                pk.h[0][ax0 + ilo], e);
       } else {
         zero_edge(e);
       }
@@ -121,9 +214,15 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
       Edge e;
       if (jlo >= 0 && jlo + 1 < g.ny && ii < g.nx) {
         const int64_t q = plane + (int64_t)jlo * g.nx + ii;
+        double an, ap, dl;
+        if constexpr (STAGED) {
+          an = stg->ay[0][b][col]; ap = stg->ay[1][b][col]; dl = stg->ay[2][b][col];
+        } else {
+          an = pk.an[1][q]; ap = pk.ap[1][q]; dl = pk.dl[1][q];
+        }
         sg_edge(s_psi[b][col + 1], s_psi[b + 1][col + 1], s_n[b][col + 1],
-                s_n[b + 1][col + 1], s_p[b][col + 1], s_p[b + 1][col + 1], pk.an[1][q],
-                pk.ap[1][q], pk.dl[1][q], pk.h[1][ay0 + jlo], e);
+                s_n[b + 1][col + 1], s_p[b][col + 1], s_p[b + 1][col + 1], an, ap, dl,
+                pk.h[1][ay0 + jlo], e);
       } else {
         zero_edge(e);
       }
@@ -136,8 +235,14 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
     if (DIM == 3) {
       if (own && kz + 1 < g.nz) {
         const int64_t q = plane + (int64_t)j * g.nx + i;
-        sg_edge(cur.psi, nxt.psi, cur.n, nxt.n, cur.p, nxt.p, pk.an[2][q], pk.ap[2][q],
-                pk.dl[2][q], pk.h[2][az0 + kz], eU);
+        double an, ap, dl;
+        if constexpr (STAGED) {
+          an = stg->az[0][ty][tx]; ap = stg->az[1][ty][tx]; dl = stg->az[2][ty][tx];
+        } else {
+          an = pk.an[2][q]; ap = pk.ap[2][q]; dl = pk.dl[2][q];
+        }
+        sg_edge(cur.psi, nxt.psi, cur.n, nxt.n, cur.p, nxt.p, an, ap, dl,
+                pk.h[2][az0 + kz], eU);
       } else {
         zero_edge(eU);
       }
@@ -193,8 +298,15 @@ k_sg_assemble(const tcad_pack_t pk, const double* __restrict__ psi,
           }
         }
         double Rs, dRsn, dRsp;
-        recomb(cur.n, cur.p, pk.nie[k], pk.tau_n[k], pk.tau_p[k], par, Rs, dRsn, dRsp);
-        double F0 = f0 - dV * (cur.n - cur.p - pk.C[k]);
+        double Ck, niek, tnk, tpk;
+        if constexpr (STAGED) {
+          Ck = stg->nd[0][ty][tx]; niek = stg->nd[1][ty][tx];
+          tnk = stg->nd[2][ty][tx]; tpk = stg->nd[3][ty][tx];
+        } else {
+          Ck = pk.C[k]; niek = pk.nie[k]; tnk = pk.tau_n[k]; tpk = pk.tau_p[k];
+        }
+        recomb(cur.n, cur.p, niek, tnk, tpk, par, Rs, dRsn, dRsp);
+        double F0 = f0 - dV * (cur.n - cur.p - Ck);
         double F1 = f1 - Rs * dV;
         double F2 = f2 + Rs * dV;
         // diagonal block, summed in the reference's stamp order per axis
@@ -575,10 +687,17 @@ int sg_assemble_tiles(const tcad_pack_t* pk, const double* psi, const double* n,
   if (!pack_ok(pk) || pk->n_tiles <= 0) return TCAD_ERR_ARG;
   const unsigned nt = (unsigned)(tiles ? n_list : pk->n_tiles);
   if (nt == 0) return TCAD_OK;
-  if (pk->dim == 2)
-    k_sg_assemble<2><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode, tiles);
-  else
-    k_sg_assemble<3><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode, tiles);
+  if (pk->dim == 2) {
+    k_sg_assemble<2, false><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode, tiles);
+  } else if (pk->asm_stage) {
+    TCAD_CUDA_CHECK(cudaFuncSetAttribute(k_sg_assemble<3, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kStageBytes));
+    k_sg_assemble<3, true><<<nt, kTileThreads, kStageBytes, s>>>(*pk, psi, n, p, F, J, mode,
+                                                                tiles);
+  } else {
+    k_sg_assemble<3, false><<<nt, kTileThreads, 0, s>>>(*pk, psi, n, p, F, J, mode, tiles);
+  }
   note_launch();
   TCAD_LAUNCH_CHECK();
   return TCAD_OK;

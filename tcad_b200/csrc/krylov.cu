@@ -876,7 +876,8 @@ __device__ __forceinline__ double pspmv(const double* __restrict__ J,
 __global__ void __launch_bounds__(NT)
 k_cg_init(const tcad_pack_t pk, const double* __restrict__ J, const double* __restrict__ b,
           double* __restrict__ x, CgVec w, KState* ks, double* partial, unsigned* ticket,
-          double rtol, int maxit, const uint8_t* __restrict__ active) {
+          double rtol, int maxit, const uint8_t* __restrict__ active,
+          const double* __restrict__ rtol_inst) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
   const int64_t NN = pk.n_nodes;
   double v[2] = {0.0, 0.0};
@@ -892,7 +893,8 @@ k_cg_init(const tcad_pack_t pk, const double* __restrict__ J, const double* __re
   if (Reduce<2>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     KState& s = ks[fb.inst];
     s.bb = tot[0]; s.rho = tot[0]; s.rr = tot[0];
-    s.tol2 = rtol * rtol * tot[0];
+    const double rt = rtol_inst ? rtol_inst[fb.inst] : rtol;
+    s.tol2 = rt * rt * tot[0];
     s.it = 0; s.maxit = maxit; s.status = TCAD_OK; s.restart = 0; s.early = 0;
     if (!isfinite(tot[0]) || !isfinite(tot[1])) s.status = TCAD_ERR_NONFINITE;
     s.active = (s.status == TCAD_OK && tot[0] > 0.0 && (!active || active[fb.inst])) ? 1 : 0;
@@ -1536,12 +1538,13 @@ static int solve_mixed(const tcad_pack_t* pk, const double* J, const double* b, 
 
 static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, double* x,
                      double rtol, int maxiter, const Work& w, const uint8_t* active,
-                     std::vector<KState>& hks, cudaStream_t s) {
+                     std::vector<KState>& hks, cudaStream_t s,
+                     const double* rtol_inst = nullptr) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
   k_cg_init<<<nb, NT, 0, s>>>(*pk, J, b, x, w.cg, w.ks, w.partial, w.ticket, rtol, maxiter,
-                              active);
+                              active, rtol_inst);
   note_launch();
   TCAD_LAUNCH_CHECK();
   hks.resize(ni);
@@ -2078,11 +2081,19 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
   }
   std::vector<KState> hks;
   std::vector<unsigned long long> herr(ni);
+  // inexact-Newton forcing (opts->forcing): step k's PCG is solved to
+  // eta_k = clamp(0.1 |d_{k-1}|, rtol, eta_max), so the early steps from the
+  // bulk guess stop at eta_max while the last ones, with |d| near the update
+  // test, are solved to rtol; quadratic convergence is kept and the
+  // converged potential is the same discrete solution
+  std::vector<double> heta(ni, opts->forcing ? std::max(opts->eta_max, opts->rtol) : opts->rtol);
   for (int it = 0; it < opts->max_iter; ++it) {
     TCAD_CUDA_CHECK(cudaMemcpyAsync(dact, hact.data(), ni, cudaMemcpyHostToDevice, s));
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(w.eta, heta.data(), sizeof(double) * ni,
+                                    cudaMemcpyHostToDevice, s));
     int rc = tcad_poisson_assemble(pk, psi, F, J, TCAD_MODE_ELIMINATE, stream);
     if (rc != TCAD_OK) return rc;
-    rc = launch_cg(pk, J, F, d, opts->rtol, opts->krylov_maxiter, w, dact, hks, s);
+    rc = launch_cg(pk, J, F, d, opts->rtol, opts->krylov_maxiter, w, dact, hks, s, w.eta);
     if (rc != TCAD_OK) return rc;
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
     k_eq_update<<<nb, NT, 0, s>>>(*pk, psi, d, opts->max_dpsi, dact, w.err);
@@ -2110,6 +2121,9 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
       } else if (!(e == e) || e == INFINITY) {
         hact[i] = 0;
       }
+      if (opts->forcing)
+        heta[i] = std::min(std::max(opts->eta_max, opts->rtol),
+                           std::max(opts->rtol, 0.1 * (std::isfinite(e) ? e : 1.0)));
       any = any || hact[i];
     }
     if (!any) break;

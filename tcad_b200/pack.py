@@ -468,6 +468,7 @@ class Pack:
         P.n_flat = self.n_flat; P.n_tiles = self.n_tiles
         P.tile_z = self.tile_z = tb["tile_z"]
         P.flat_nodes = self.flat_nodes = tb["flat_nodes"]
+        P.asm_stage = self.asm_stage = 0
         for f in ("shape", "node_off", "flat_off", "flat_inst", "axis_off", "tile", "par",
                   "C", "nie", "nie_s", "tau_n", "tau_p", "bcflag") + BC_ARRAYS:
             setattr(P, f, t[f].data_ptr())
@@ -701,6 +702,12 @@ class Pack:
         if wb > self.work.numel():
             self.work = self.torch.empty(wb, dtype=self.torch.uint8, device=self.device)
 
+    def set_asm_stage(self, stage):
+        """3D coupled assembly: 1 stages each next z-plane's coefficients in
+        shared memory with asynchronous copies, 0 loads them in place (the
+        same arithmetic either way)."""
+        self.P.asm_stage = self.asm_stage = int(bool(stage)) if self.dim == 3 else 0
+
     def newton(self, opts, active=None, transient=None):
         """Coupled Newton on every (active) instance; `transient` = {dt (scaled
         time), theta, n_old, p_old[, fn_old, fp_old]} (device tensors) makes
@@ -708,7 +715,7 @@ class Pack:
         ni = len(self.setups)
         if self.autotune and self.dim == 3 and not getattr(self, "_tuned", False):
             from . import tune
-            tune.tune_tile_z(self)
+            tune.tune_assembly(self)
             self._tuned = True
         if active is None:
             self.active.fill_(1)
