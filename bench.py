@@ -98,7 +98,7 @@ def parse():
     ap.add_argument("--rate", type=float, default=200.0, help="serve: mean requests/s")
     ap.add_argument("--budget-gb", type=float, default=160.0,
                     help="serve: HBM budget of the arenas (GB)")
-    ap.add_argument("--drain", type=float, default=30.0,
+    ap.add_argument("--drain", type=float, default=120.0,
                     help="serve: seconds to finish in-flight work after the arrivals end")
     ap.add_argument("--plain-seconds", type=float, default=45.0,
                     help="serve: time cap of the sequential plain FP64 run")

@@ -154,7 +154,7 @@ class _Bordered:
             F = self.residual(u, V)
             narc = float(torch.dot(t_u, u - u_prev)) + t_V * (V - V_prev) - ds
             base = 0.5 * (float(torch.dot(F, F)) + narc * narc)
-            rhs = -F
+            rhs = F.clone()          # the set-up replaces it by D^-1 (-F)
             rc = pk.lib.tcad_block_jacobi_setup(pk.pref, self._lib.ptr(pk.J),
                                                 self._lib.ptr(rhs), self._lib.ptr(st), pk.sp())
             self._lib.check(rc, "tcad_block_jacobi_setup")

@@ -571,13 +571,15 @@ class Worker(threading.Thread):
 
 
 # Default cap of the nodes one round solves.  A 2D round's time is set by its
-# deepest member's ILU(0) sweeps (one dependent level per anti-diagonal, up to
-# 767 for 512 x 256) far more than by its node count (a 2D block SpMV streams
-# 8M nodes in ~0.3 ms): measured at 200 req/s, rounds of ~160 devices (6.4M
-# nodes) took 7 s at the median.  So a round takes as many devices as the cap
-# allows: 32M nodes (a quarter of a 160 GB 2D arena).  3D rounds (block
-# Jacobi, no sweeps) scale with their nodes and stay at 4M.
-ROUND_NODES = {2: 32_000_000, 3: 4_000_000}
+# members' Newton steps under ILU(0) sweeps (one dependent level per
+# anti-diagonal, up to 767 for 512 x 256) and, in a round that admits many
+# devices, by their equilibrium solves.  Measured at 200 req/s: rounds of
+# ~160 devices (6.4M nodes) took 7 s at the median, rounds of ~300-700
+# devices (13M) 29-70 s -- and a single-bias request needs 4 rounds, a sweep
+# 13-43, so long rounds leave every request unfinished in a minute-long
+# window.  8M 2D nodes keeps rounds short; 3D rounds (block Jacobi, no
+# sweeps) scale with their nodes and stay at 4M.
+ROUND_NODES = {2: 8_000_000, 3: 4_000_000}
 
 
 class Server:
