@@ -91,8 +91,9 @@ def test_trigate_downscaled_sweeps_match_oracle(batched):
     Vd branches from equilibrium, 21 points each, with the default (chosen)
     Newton options; alone, one device per branch, and batched, both branches
     in ONE 2-instance pack (the bench's headline form).  Drain, source and
-    body currents within 1e-6 (on 1e-9 x the sweep's largest), psi within
-    1e-9 V and the quasi-Fermi levels within 1e-8 V at the sampled nodes."""
+    body currents within 1e-6 (on 1e-9 x the branch's largest terminal
+    current), psi within 1e-9 V and the quasi-Fermi levels within 1e-8 V at
+    the sampled nodes."""
     import tcad_b200 as tb
     from tcad_b200 import workloads as W
     from tcad_b200.batch import DeviceBatch
@@ -130,9 +131,15 @@ def test_trigate_downscaled_sweeps_match_oracle(batched):
                 if q in fpts:
                     st = [t.ravel()[idx] for t in (dev.psi, dev.n, dev.p)]
                     _check_fields(VT, st, g["fields"][a][fpts.index(q)], (vd, vg))
-    for c in cur:
-        for a in range(2):
-            err = _rel_err(cur[c][a], g["I_" + c][a])
+    for a in range(2):
+        # each contact on its own scale, floored at 1e-9 x the branch's
+        # largest terminal current: the body current (~1e-19 A, fourteen
+        # decades under the drain's) is a residual sum of cancelling fluxes
+        top = max(np.abs(g["I_" + c][a]).max() for c in cur)
+        for c in cur:
+            ref = g["I_" + c][a]
+            scale = np.maximum(np.abs(ref), 1e-9 * top)
+            err = float((np.abs(cur[c][a] - ref) / scale).max())
             assert err < 1e-6, (c, a, err)
 
 
