@@ -72,6 +72,8 @@ METHODS = {
                  predictor="secant"),
     "mixed": dict(precision="mixed", forcing="adaptive", krylov_unknowns="relative",
                   predictor="secant"),
+    "fp32op": dict(precision="fp32_operator", forcing="adaptive", krylov_unknowns="relative",
+                   predictor="secant"),
 }
 METHOD_DESC = {
     "plain": "plain FP64: fused SG assembly, node-block-Jacobi BiCGStab to rtol 1e-10 on "
@@ -79,6 +81,9 @@ METHOD_DESC = {
     "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the block-scaled system in "
             "relative unknowns (dpsi, dn/n, dp/p) solved to 1e-3 every Newton step, two "
             "polishing steps (1e-6, then 1e-3), secant predictor along the sweep",
+    "fp32op": "FP64 inexact Newton as 'fp64', but the BiCGStab of the Newton steps before the "
+              "update test reads an FP32 copy of the block-scaled Jacobian (FP64 vectors, dots "
+              "and polishing steps)",
     "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
              "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
              "relative unknowns, adaptive forcing, secant predictor; per-instance FP64 "
@@ -494,7 +499,8 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (FP32 inner Krylov)" if args.method == "mixed" else "f64",
+            "dtype": {"mixed": "f64 (FP32 inner Krylov)",
+                      "fp32op": "f64 (FP32 operator copy)"}.get(args.method, "f64"),
             "data": "synthetic device (analytic doping profiles, explicit mesh)",
             "config": {"workload": chosen.desc, "method": method_desc,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",

@@ -70,6 +70,9 @@ extern "C" {
                                   raw current rows the AC sensitivities sum
                                   (current_rows_for, pytcad/device2d.py:1751-1758) */
 
+/* tcad_newton_opts_t.precision: FP32 operator copy, FP64 Krylov vectors */
+#define TCAD_PRECISION_J32 33
+
 /* bcflag bits */
 #define TCAD_BC_CONTACT 1
 #define TCAD_BC_GATE 2
@@ -336,7 +339,11 @@ typedef struct tcad_newton_opts {
                             eta_max) */
   int32_t precision;     /* 64: FP64 Krylov; 32: FP32 Krylov on an FP32 copy of the scaled
                             operator inside FP64 iterative refinement (residual, Newton,
-                            convergence test stay FP64) */
+                            convergence test stay FP64); TCAD_PRECISION_J32 (33): FP64
+                            Krylov on an FP32 copy of the scaled operator in the steps
+                            before the update test passes, FP64 operator in the
+                            polishing steps (node-block Jacobi solves; ILU(0) solves
+                            keep FP64) */
   int32_t density_scaling; /* 1: Krylov unknowns are (dpsi, dn/s_n, dp/s_p), s = max(n|p,
                               scale_floor) -- the quantities of the Newton update test */
   int32_t precond;       /* 0: node-block Jacobi; 1: + block ILU(0) right preconditioner on

@@ -260,8 +260,8 @@ k_bj_setup(const tcad_pack_t pk, double* __restrict__ J, double* __restrict__ F,
 // The vector is read through X(m, c) = x[c * NN + m] (spmv_node) or any
 // other functor giving the same values (the fused solve forms neighbour
 // values on the fly); the arithmetic is the same either way.
-template <int DIM, bool SCALED, class T, class XF>
-__device__ __forceinline__ void spmv_node_f(const T* __restrict__ J, const XF& X, int64_t k,
+template <int DIM, bool SCALED, class T, class XF, class TJ>
+__device__ __forceinline__ void spmv_node_f(const TJ* __restrict__ J, const XF& X, int64_t k,
                                             int64_t NN, const int64_t* off, int64_t lo,
                                             int64_t hi, T& y0, T& y1, T& y2) {
   T t0 = T(0), t1 = T(0), t2 = T(0);
@@ -270,14 +270,14 @@ __device__ __forceinline__ void spmv_node_f(const T* __restrict__ J, const XF& X
     const int64_t m = clampi(k + off[d], lo, hi);
     const int e = 9 + 5 * d;
     const T xs = X(m, 0), xn = X(m, 1), xp = X(m, 2);
-    t0 += J[(int64_t)e * NN + k] * xs;
-    t1 += J[(int64_t)(e + 1) * NN + k] * xs + J[(int64_t)(e + 2) * NN + k] * xn;
-    t2 += J[(int64_t)(e + 3) * NN + k] * xs + J[(int64_t)(e + 4) * NN + k] * xp;
+    t0 += T(J[(int64_t)e * NN + k]) * xs;
+    t1 += T(J[(int64_t)(e + 1) * NN + k]) * xs + T(J[(int64_t)(e + 2) * NN + k]) * xn;
+    t2 += T(J[(int64_t)(e + 3) * NN + k]) * xs + T(J[(int64_t)(e + 4) * NN + k]) * xp;
   }
   const T x0 = X(k, 0), x1 = X(k, 1), x2 = X(k, 2);
   T d[9];
 #pragma unroll
-  for (int e = 0; e < 9; ++e) d[e] = J[(int64_t)e * NN + k];
+  for (int e = 0; e < 9; ++e) d[e] = T(J[(int64_t)e * NN + k]);
   if (SCALED) {
     y0 = x0 + (d[0] * t0 + d[1] * t1 + d[2] * t2);
     y1 = x1 + (d[3] * t0 + d[4] * t1 + d[5] * t2);
@@ -289,8 +289,8 @@ __device__ __forceinline__ void spmv_node_f(const T* __restrict__ J, const XF& X
   }
 }
 
-template <int DIM, bool SCALED, class T>
-__device__ __forceinline__ void spmv_node(const T* __restrict__ J, const T* __restrict__ x,
+template <int DIM, bool SCALED, class T, class TJ = T>
+__device__ __forceinline__ void spmv_node(const TJ* __restrict__ J, const T* __restrict__ x,
                                           int64_t k, int64_t NN, const int64_t* off,
                                           int64_t lo, int64_t hi, T& y0, T& y1, T& y2) {
   spmv_node_f<DIM, SCALED, T>(J, [&](int64_t m, int c) { return x[c * NN + m]; }, k, NN, off,
@@ -389,9 +389,9 @@ __device__ __forceinline__ void bi_p_body(const tcad_pack_t& pk, const FlatBlock
 }
 
 // v = A^ ph; (rh, v)
-template <int DIM, class T>
+template <int DIM, class T, class TJ = T>
 __device__ __forceinline__ double bi_v_body(const tcad_pack_t& pk, const FlatBlock& fb,
-                                            const T* __restrict__ J, const BiVecT<T>& w) {
+                                            const TJ* __restrict__ J, const BiVecT<T>& w) {
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
   nbr_offsets(g, off);
@@ -445,9 +445,9 @@ __device__ __forceinline__ double bi_s_body(const tcad_pack_t& pk, const FlatBlo
 }
 
 // t = A^ sh; (t, s), (t, t)
-template <int DIM, class T>
+template <int DIM, class T, class TJ = T>
 __device__ __forceinline__ void bi_t_body(const tcad_pack_t& pk, const FlatBlock& fb,
-                                          const T* __restrict__ J, const BiVecT<T>& w,
+                                          const TJ* __restrict__ J, const BiVecT<T>& w,
                                           double (&v)[2]) {
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
@@ -472,9 +472,9 @@ __device__ __forceinline__ void bi_t_body(const tcad_pack_t& pk, const FlatBlock
 // formed from their r and v (neither changes in this step); (s, s), (t, s),
 // (t, t).  Same expressions and accumulation order as bi_s_body followed by
 // bi_t_body.
-template <int DIM>
+template <int DIM, class TJ = double>
 __device__ __forceinline__ void bi_st_body(const tcad_pack_t& pk, const FlatBlock& fb,
-                                           const double* __restrict__ J, const BiVec& w,
+                                           const TJ* __restrict__ J, const BiVec& w,
                                            double alpha, double (&v)[3]) {
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
@@ -551,9 +551,9 @@ __device__ __forceinline__ void bi_x_body(const tcad_pack_t& pk, const FlatBlock
 }
 
 // r = b - A^ x; (r, r)
-template <int DIM, class T>
+template <int DIM, class T, class TJ = T>
 __device__ __forceinline__ double true_resid_body(const tcad_pack_t& pk, const FlatBlock& fb,
-                                                  const T* __restrict__ J,
+                                                  const TJ* __restrict__ J,
                                                   const T* __restrict__ b,
                                                   const T* __restrict__ x, T* __restrict__ r) {
   const Inst g = load_inst(pk, fb.inst);
@@ -595,14 +595,14 @@ k_bi_p(const tcad_pack_t pk, BiVecT<T> w, const KState* ks, const int32_t* __res
   bi_p_body<T>(pk, fb, w, (T)s.beta, (T)s.omega, s.restart);
 }
 
-template <int DIM, class T>
+template <int DIM, class T, class TJ = T>
 __global__ void __launch_bounds__(NT)
-k_bi_v(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
+k_bi_v(const tcad_pack_t pk, const TJ* __restrict__ J, BiVecT<T> w, KState* ks,
        double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
   const FlatBlock fb = flat_block(pk, fbi);
   if (!ks[fb.inst].active) return;
-  double v[1] = {bi_v_body<DIM, T>(pk, fb, J, w)};
+  double v[1] = {bi_v_body<DIM, T, TJ>(pk, fb, J, w)};
   double tot[1];
   if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
     fin_v(ks[fb.inst], tot[0]);
@@ -622,15 +622,15 @@ k_bi_s(const tcad_pack_t pk, BiVecT<T> w, KState* ks, double* partial, unsigned*
     fin_s(ks[fb.inst], tot[0]);
 }
 
-template <int DIM, class T>
+template <int DIM, class T, class TJ = T>
 __global__ void __launch_bounds__(NT)
-k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
+k_bi_t(const tcad_pack_t pk, const TJ* __restrict__ J, BiVecT<T> w, KState* ks,
        double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
   const FlatBlock fb = flat_block(pk, fbi);
   if (!ks[fb.inst].active) return;
   double v[2];
-  bi_t_body<DIM, T>(pk, fb, J, w, v);
+  bi_t_body<DIM, T, TJ>(pk, fb, J, w, v);
   double tot[2];
   if (Reduce<2>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
     fin_t(ks[fb.inst], tot[0], tot[1]);
@@ -641,16 +641,16 @@ k_bi_t(const tcad_pack_t pk, const T* __restrict__ J, BiVecT<T> w, KState* ks,
 // (bi_st_body); the last block of the instance applies fin_s and fin_t on
 // the block partials summed in block order, exactly the values k_bi_s and
 // k_bi_t would give -- one launch and one reduction fewer per iteration.
-template <int DIM>
+template <int DIM, class TJ = double>
 __global__ void __launch_bounds__(NT)
-k_bi_st(const tcad_pack_t pk, const double* __restrict__ J, BiVec w, KState* ks,
+k_bi_st(const tcad_pack_t pk, const TJ* __restrict__ J, BiVec w, KState* ks,
         double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
   const FlatBlock fb = flat_block(pk, fbi);
   const KState s0 = ks[fb.inst];
   if (!s0.active) return;
   double v[3];
-  bi_st_body<DIM>(pk, fb, J, w, s0.alpha, v);
+  bi_st_body<DIM, TJ>(pk, fb, J, w, s0.alpha, v);
   double tot[3];
   if (Reduce<3>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     fin_s(ks[fb.inst], tot[0]);
@@ -675,13 +675,13 @@ k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double*
 
 // true scaled residual r = b - A^ x, its norm into the state; re-arm a restart
 // when it is not within the tolerance the recursive residual claimed
-template <int DIM, class T>
+template <int DIM, class T, class TJ = T>
 __global__ void __launch_bounds__(NT)
-k_true_resid(const tcad_pack_t pk, const T* __restrict__ J, const T* __restrict__ b,
+k_true_resid(const tcad_pack_t pk, const TJ* __restrict__ J, const T* __restrict__ b,
              const T* __restrict__ x, T* __restrict__ r, KState* ks, double* partial,
              unsigned* ticket, int rearm) {
   const FlatBlock fb = flat_block(pk, blockIdx.x);
-  double v[1] = {true_resid_body<DIM, T>(pk, fb, J, b, x, r)};
+  double v[1] = {true_resid_body<DIM, T, TJ>(pk, fb, J, b, x, r)};
   double tot[1];
   if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
     fin_true(ks[fb.inst], tot[0], rearm);
@@ -1344,8 +1344,8 @@ static int launch_bicgstab_fused(const tcad_pack_t* pk, const double* J, const d
   return TCAD_OK;
 }
 
-template <class T>
-static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x, double rtol,
+template <class T, class TJ = T>
+static int launch_bicgstab_t(const tcad_pack_t* pk, const TJ* J, const T* b, T* x, double rtol,
                              int maxiter, const BiVecT<T>& bi, const Work& w,
                              const int32_t* pre_status, std::vector<KState>& hks,
                              cudaStream_t s, const double* rtol_inst,
@@ -1354,7 +1354,7 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const T* J, const T* b, T* x
                              const WorkIlu* ilc = nullptr) {
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
-  if constexpr (std::is_same<T, double>::value) {
+  if constexpr (std::is_same<T, double>::value && std::is_same<TJ, double>::value) {
     if (g_fused_mode.load() && ni == 1 && Qilu == nullptr &&
         (pk->dim == 2 ? fused_fits<2>(nb) : fused_fits<3>(nb)) &&
         launch_bicgstab_fused(pk, J, b, x, rtol, maxiter, bi, w, pre_status, hks, s,
@@ -1798,8 +1798,9 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   std::vector<unsigned long long> herr(ni);
   std::vector<int32_t> hstat(ni);
   std::vector<int> polish_left(ni, -1);  // -1: not yet converged
-  if (opts->precision != 64 && opts->precision != 32) return TCAD_ERR_ARG;
-  if (opts->precision == 32 && work_bytes < tcad_block_workspace_bytes(pk, 0, 0))
+  if (opts->precision != 64 && opts->precision != 32 && opts->precision != TCAD_PRECISION_J32)
+    return TCAD_ERR_ARG;
+  if (opts->precision != 64 && work_bytes < tcad_block_workspace_bytes(pk, 0, 0))
     return TCAD_ERR_ARG;
   const Work32 w32 = carve32(pk, reinterpret_cast<char*>(work) + ((w.bytes + 255) & ~(size_t)255));
   // ILU(0) right preconditioner (2D): its region follows the FP32 extension.
@@ -2016,8 +2017,24 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
         note_launch();
         TCAD_LAUNCH_CHECK();
       }
-      rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks, s,
-                           w.eta, any_ilu ? &wilu_use : nullptr, nzmax);
+      // precision 33: the Newton steps before the update test passes run the
+      // FP64 BiCGStab on an FP32 copy of the scaled operator (half the
+      // operator bytes); the polishing steps, and any solve with ILU(0),
+      // keep the FP64 operator
+      bool any_polish = false;
+      for (int i = 0; i < ni; ++i) any_polish = any_polish || (solve_set[i] && polish_left[i] > 0);
+      if (opts->precision == TCAD_PRECISION_J32 && !any_ilu && !any_polish) {
+        const int ne = pk->dim == 2 ? TCAD_NE2 : TCAD_NE3;
+        k_to_f32<<<fl ? (unsigned)nfl : nb, NT, 0, s>>>(*pk, ne, J, w32.J32, fl);
+        note_launch();
+        TCAD_LAUNCH_CHECK();
+        rc = launch_bicgstab_t<double, float>(pk, w32.J32, F, du, opts->rtol,
+                                              opts->krylov_maxiter, w.bi, w, w.status, hks, s,
+                                              w.eta);
+      } else {
+        rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks,
+                             s, w.eta, any_ilu ? &wilu_use : nullptr, nzmax);
+      }
       if (rc != TCAD_OK) return rc;
       std::vector<uint8_t> apply(ni, 0), retry(ni, 0);
       bool any_retry = false;

@@ -113,7 +113,10 @@ class NewtonOptions:
     # to 1e-3: once Newton converges quadratically the step's size, not the
     # linear tolerance, decides the next update), linsolve_rtol for "mixed"
     eta_min: float | None = None
-    # GPU-only: "fp64" solves the Newton systems in FP64; "mixed" runs the
+    # GPU-only: "fp64" solves the Newton systems in FP64; "fp32_operator"
+    # runs the FP64 BiCGStab of the Newton steps before the update test on an
+    # FP32 copy of the block-scaled Jacobian (half the operator's bytes; the
+    # polishing steps keep FP64); "mixed" runs the
     # Krylov iterations in FP32 on an FP32 copy of the block-scaled Jacobian
     # inside FP64 iterative refinement -- residual, Newton update and the
     # convergence test stay FP64, so the converged state is the FP64 one.
@@ -147,5 +150,6 @@ class NewtonOptions:
             raise ValueError(f"unknown linsolve {self.linsolve!r}")
         if self.predictor not in ("none", "secant"):
             raise ValueError(f"NewtonOptions.predictor={self.predictor!r}: 'none' or 'secant'")
-        if self.precision not in ("fp64", "mixed"):
-            raise ValueError(f"NewtonOptions.precision={self.precision!r}: 'fp64' or 'mixed'")
+        if self.precision not in ("fp64", "mixed", "fp32_operator"):
+            raise ValueError(f"NewtonOptions.precision={self.precision!r}: 'fp64', 'mixed' "
+                             "or 'fp32_operator'")

@@ -668,11 +668,12 @@ class Pack:
         o.polish = 0 if equilibrium else int(getattr(opts, "polish", 0))
         o.forcing = 1 if getattr(opts, "forcing", "fixed") == "adaptive" else 0
         o.eta_max = float(getattr(opts, "eta_max", 1e-3))
-        o.precision = 32 if getattr(opts, "precision", "fp64") == "mixed" and not equilibrium else 64
+        prec = getattr(opts, "precision", "fp64")
+        o.precision = {"mixed": 32, "fp32_operator": 33}.get(prec, 64) if not equilibrium else 64
         o.density_scaling = 1 if getattr(opts, "krylov_unknowns", "relative") == "relative" else 0
         em = getattr(opts, "eta_min", None)
         if em is None:
-            em = o.eta_max if o.precision == 64 else opts.linsolve_rtol
+            em = o.eta_max if o.precision in (64, 33) else opts.linsolve_rtol
         o.eta_min = float(em)
         o.scale_floor = float(getattr(opts, "krylov_scale_floor", 1e-10))
         pc = getattr(opts, "precond", "auto")
