@@ -51,10 +51,9 @@ UNIT = "bias_pts/s"
 BYTES_SPMV = {2: (29 + 3 + 3) * 8, 3: (39 + 3 + 3) * 8}
 BYTES_ASM = {2: (13 + 32) * 8 + 1, 3: (16 + 42) * 8 + 1}
 #  one BiCGStab iteration in the solver (node-block layout, FP64), bytes per
-#  node of its four kernels: k_bi_p 96 (r, v, p in; p out); k_bi_v one SpMV
-#  (J + x in, y out); k_bi_st the other SpMV with s formed on the fly (J, r,
-#  v in; s, t out: J + 48 + 48 bytes); k_bi_x 168
-BYTES_ITER = {d: 96 + BYTES_SPMV[d] + (BYTES_SPMV[d] - 48 + 96) + 168 for d in (2, 3)}
+#  node of the five kernels: k_bi_p 96 (r, v, p in; p out), k_bi_v and k_bi_t
+#  one SpMV each (J + x in, y out), k_bi_s 72, k_bi_x 168
+BYTES_ITER = {d: 96 + 2 * BYTES_SPMV[d] + 72 + 168 for d in (2, 3)}
 
 # Newton iterations / BiCGStab iterations per bias point of the plain FP64
 # path on this workload, from its own bench runs; used only to scale the
@@ -537,8 +536,8 @@ def run_ours(args):
                                   "launch_ms": t_asm * 1e3,
                                   "traffic": load_traffic(f"assemble{dim}d_{args.workload}")},
             "roofline_bicgstab_iteration": {
-                "kernel": "k_bi_p + k_bi_v + k_bi_st + k_bi_x (one iteration in the "
-                          "solver)", "bound": "hbm", "achieved": ach_iter, "peak": peak,
+                "kernel": "k_bi_p + k_bi_v + k_bi_s + k_bi_t + k_bi_x (one iteration in "
+                          "the solver)", "bound": "hbm", "achieved": ach_iter, "peak": peak,
                 "unit": "GB/s", "frac": ach_iter / peak,
                 "bytes_per_iteration": BYTES_ITER[dim] * NN, "iteration_ms": t_iter * 1e3,
                 "iterations_timed": it_done},

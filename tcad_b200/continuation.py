@@ -108,10 +108,12 @@ class _Bordered:
     then the reference's damping: psi clipped to +-max_dpsi, n and p to
     [0.1, 10] x, Armijo backtracking on the 2-norm of the full bordered
     residual, and convergence on the undamped update (|dpsi|, |dn/n|,
-    |dp/p|, |dV|) < tol.  After convergence, NewtonOptions.polish more steps
-    take the state to the FP64 fixed point, as the bias-controlled Newton
-    does: near zero bias the current is a small difference of large fluxes
-    and the state at the 1e-8 update test leaves it ~3e-2 off."""
+    |dp/p|, |dV|) < tol.  The converged point is then finished by the
+    bias-controlled Newton at its V (update test, then NewtonOptions.polish
+    steps in relative Krylov unknowns), which takes the state to the FP64
+    fixed point at that bias: near zero bias the current is a small
+    difference of large contact fluxes, and the state at the 1e-8 update
+    test of the bordered system leaves it ~3e-2 off."""
 
     def __init__(self, device, contact, opts, rtol=1e-10, maxiter=4000):
         import torch
@@ -146,6 +148,20 @@ class _Bordered:
         pk.assemble(self._lib.MODE_RAW)
         return pk.F.clone()
 
+    def finish(self, u, V):
+        """Newton at fixed bias V from the corrector's converged u (its update
+        test passes at once; the polishing steps follow); the finished state."""
+        pk = self.pk
+        self.put(u)
+        self.dev._apply_voltages({self.contact: V})
+        pk.set_bias()
+        pk.stamp_contacts()
+        res = pk.newton(self.opts)[0]
+        if not res["converged"]:
+            self.put(u)
+        self.dev._host.clear()
+        return self.state()
+
     def correct(self, u_pred, V_pred, u_prev, V_prev, t_u, t_V, ds, tol, max_iter):
         torch, pk, N = self.torch, self.pk, self.N
         opts = self.opts
@@ -153,8 +169,7 @@ class _Bordered:
         a = torch.empty_like(u)
         b = torch.empty_like(u)
         st = torch.zeros(1, dtype=torch.int32, device=pk.device)
-        polish_left = None                    # steps still to take after convergence
-        for it in range(max_iter + int(getattr(opts, "polish", 0))):
+        for it in range(max_iter):
             F = self.residual(u, V)
             narc = float(torch.dot(t_u, u - u_prev)) + t_V * (V - V_prev) - ds
             base = 0.5 * (float(torch.dot(F, F)) + narc * narc)
@@ -200,18 +215,8 @@ class _Bordered:
             err = max(float(dpsi.abs().max()), rel_n, rel_p, abs(dV))
             u = torch.cat([psi + lam * dpsi, n_new, p_new])
             V = V + lam * dV
-            if polish_left is None and err < tol:
-                polish_left = int(getattr(opts, "polish", 0))
-                n_conv = it + 1
-            elif polish_left is not None:
-                polish_left -= 1
-            if polish_left is not None and polish_left <= 0:
-                self.put(u)
-                self.dev._apply_voltages({self.contact: V})
-                self.pk.set_bias()
-                return u, V, True, n_conv
-            if polish_left is None and it + 1 >= max_iter:
-                break
+            if err < tol:
+                return self.finish(u, V), V, True, it + 1
         return u, V, False, max_iter
 
 

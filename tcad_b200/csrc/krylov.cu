@@ -636,28 +636,6 @@ k_bi_t(const tcad_pack_t pk, const TJ* __restrict__ J, BiVecT<T> w, KState* ks,
     fin_t(ks[fb.inst], tot[0], tot[1]);
 }
 
-// The s and t steps in one launch (FP64, no right preconditioner): s formed
-// at the block's nodes and, for the neighbours t needs, from their r and v
-// (bi_st_body); the last block of the instance applies fin_s and fin_t on
-// the block partials summed in block order, exactly the values k_bi_s and
-// k_bi_t would give -- one launch and one reduction fewer per iteration.
-template <int DIM, class TJ = double>
-__global__ void __launch_bounds__(NT)
-k_bi_st(const tcad_pack_t pk, const TJ* __restrict__ J, BiVec w, KState* ks,
-        double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
-  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
-  const FlatBlock fb = flat_block(pk, fbi);
-  const KState s0 = ks[fb.inst];
-  if (!s0.active) return;
-  double v[3];
-  bi_st_body<DIM, TJ>(pk, fb, J, w, s0.alpha, v);
-  double tot[3];
-  if (Reduce<3>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
-    fin_s(ks[fb.inst], tot[0]);
-    fin_t(ks[fb.inst], tot[1], tot[2]);
-  }
-}
-
 template <class T>
 __global__ void __launch_bounds__(NT, 3)
 k_bi_x(const tcad_pack_t pk, T* __restrict__ x, BiVecT<T> w, KState* ks, double* partial,
@@ -1398,18 +1376,12 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const TJ* J, const T* b, T* 
       else
         k_bi_v<3><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
       note_launch();
-      bool st_done = false;
-      if constexpr (std::is_same<T, double>::value) {
-        if (!Qilu) {   // s and t in one launch (bit-identical to the two below)
-          if (pk->dim == 2)
-            k_bi_st<2><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
-          else
-            k_bi_st<3><<<ng, NT, 0, s>>>(*pk, J, bi, w.ks, w.partial, w.ticket, dlist);
-          note_launch();
-          st_done = true;
-        }
-      }
-      if (!st_done) {
+      // (The s and t steps stay two launches here: k_bi_st, which forms the
+      // neighbours' s from their r and v, measured 120 us against 20 + 80 us
+      // for k_bi_s + k_bi_t on the 983k-node tri-gate -- two loads per
+      // neighbour value instead of one; the single-launch solve of small
+      // packs, which is latency-bound, keeps the fused form.)
+      {
         k_bi_s<<<ng, NT, 0, s>>>(*pk, bi, w.ks, w.partial, w.ticket, dlist);
         note_launch();
         if (Qilu) {  // sh = M^-1 s
