@@ -103,7 +103,7 @@ class _Bordered:
     with F assembled on the GPU with its contact rows stamped (RAW mode),
     so dF/dV is -1/VT on the swept contact's potential rows.  Each step is
     solved by block elimination with two GPU Krylov solves of the block-
-    scaled Jacobian, J a = -F and J b = -dF/dV:
+    scaled Jacobian in relative unknowns, J a = -F and J b = -dF/dV:
         dV = (-N_arc - t_u . a) / (t_V + t_u . b),   du = a + dV b;
     then the reference's damping: psi clipped to +-max_dpsi, n and p to
     [0.1, 10] x, Armijo backtracking on the 2-norm of the full bordered
@@ -127,6 +127,7 @@ class _Bordered:
         nodes = torch.as_tensor(np.asarray(device.bcs[contact].nodes), device=self.pk.device)
         self.cv[nodes] = -1.0 / device.VT            # dF/dV on the contact's psi rows
         self.rtol, self.maxiter = rtol, maxiter
+        self.floor = float(getattr(opts, "krylov_scale_floor", 1e-10))
 
     def state(self):
         pk = self.pk
@@ -173,17 +174,27 @@ class _Bordered:
             F = self.residual(u, V)
             narc = float(torch.dot(t_u, u - u_prev)) + t_V * (V - V_prev) - ds
             base = 0.5 * (float(torch.dot(F, F)) + narc * narc)
-            rhs = F.clone()          # the set-up replaces it by D^-1 (-F)
-            rc = pk.lib.tcad_block_jacobi_setup(pk.pref, self._lib.ptr(pk.J),
-                                                self._lib.ptr(rhs), self._lib.ptr(st), pk.sp())
-            self._lib.check(rc, "tcad_block_jacobi_setup")
+            # relative Krylov unknowns (dpsi, dn / s_n, dp / s_p), s = max(density,
+            # floor), as in the bias-controlled Newton: in absolute unknowns the
+            # solves leave sub-floor minority densities unresolved, and a step
+            # that does not move them passes the update test with them off
+            rhs = F.clone()          # the set-up replaces it by S^-1 D^-1 (-F)
+            rc = pk.lib.tcad_block_jacobi_setup_rel(
+                pk.pref, self._lib.ptr(pk.J), self._lib.ptr(rhs), self._lib.ptr(st),
+                self._lib.ptr(pk.n), self._lib.ptr(pk.p), self.floor, pk.sp())
+            self._lib.check(rc, "tcad_block_jacobi_setup_rel")
             if int(st.item()) != 0:
                 return u, V, False, it + 1
-            # the contact rows' diagonal blocks are identities, so the scaled
-            # -dF/dV is -dF/dV itself
+            # the contact rows' diagonal blocks are identities and their unknowns
+            # potentials, so the scaled -dF/dV is -dF/dV itself
             if not (_block_solve(pk, rhs, a, self.rtol, self.maxiter)
                     and _block_solve(pk, -self.cv, b, self.rtol, self.maxiter)):
                 return u, V, False, it + 1
+            sn = torch.clamp(u[N:2 * N], min=self.floor)
+            sp_ = torch.clamp(u[2 * N:], min=self.floor)
+            for y in (a, b):
+                y[N:2 * N] *= sn
+                y[2 * N:] *= sp_
             den = t_V + float(torch.dot(t_u, b))
             if den == 0.0 or not np.isfinite(den):
                 return u, V, False, it + 1
