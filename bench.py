@@ -73,6 +73,8 @@ METHODS = {
                   predictor="secant"),
     "fp32op": dict(precision="fp32_operator", forcing="adaptive", krylov_unknowns="relative",
                    predictor="secant"),
+    "rb": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative",
+               predictor="secant", krylov_system="red_black"),
 }
 METHOD_DESC = {
     "plain": "plain FP64: fused SG assembly, node-block-Jacobi BiCGStab to rtol 1e-10 on "
@@ -83,6 +85,9 @@ METHOD_DESC = {
     "fp32op": "FP64 inexact Newton as 'fp64', but the BiCGStab of the Newton steps before the "
               "update test reads an FP32 copy of the block-scaled Jacobian (FP64 vectors, dots "
               "and polishing steps)",
+    "rb": "FP64 inexact Newton as 'fp64', with the BiCGStab on the red-black Schur "
+          "complement of the block-scaled system (red nodes eliminated exactly; the full "
+          "system's stopping test)",
     "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
              "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
              "relative unknowns, adaptive forcing, secant predictor; per-instance FP64 "

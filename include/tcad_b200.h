@@ -263,11 +263,15 @@ int tcad_block_ilu_apply(const tcad_pack_t* pk, const double* J, const double* Q
 int tcad_block_spmv(const tcad_pack_t* pk, const double* J, const double* x,
                     double* y, void* stream);
 
-/* Krylov solve of A^ x = b^ for every instance of the pack (BiCGStab:
- * method 0, GMRES(restart): method 1), x starting at zero, per-instance
- * convergence ||b^ - A^ x|| <= rtol ||b^||.  iters/status/relres are
- * per-instance host arrays.  Replaces the gmres/bicgstab + block-Jacobi
- * branch of linsolve.solve_linear (pytcad/linsolve.py:941-985). */
+/* Krylov solve of A^ x = b^ for every instance of the pack, x starting at
+ * zero, per-instance convergence ||b^ - A^ x|| <= rtol ||b^||.  method 0:
+ * BiCGStab on A^; 2: BiCGStab on the red-black Schur complement of A^ (the
+ * red nodes, (i + j + k) even, eliminated exactly; the same stopping test,
+ * the full x returned; see tcad_newton_opts_t.red_black).  Any other method
+ * is TCAD_ERR_ARG (GMRES runs on the CSR form, tcad_csr_krylov).
+ * restart is unused.  iters/status/relres are per-instance host arrays.
+ * Replaces the bicgstab + block-Jacobi branch of linsolve.solve_linear
+ * (pytcad/linsolve.py:941-985). */
 int tcad_block_krylov(const tcad_pack_t* pk, const double* J, const double* b,
                       double* x, int method, double rtol, int maxiter, int restart,
                       void* work, size_t work_bytes, int32_t* iters,
@@ -374,6 +378,16 @@ typedef struct tcad_newton_opts {
   const double* p_old;
   const double* fn_old;
   const double* fp_old;
+  /* 1: the FP64 node-block-Jacobi solves run BiCGStab on the red-black Schur
+   * complement of the block-scaled system (the face-neighbour stencil has
+   * no coupling inside a colour of (i + j + k) & 1, so the red unknowns are
+   * eliminated exactly: half the unknowns, the same matrix bytes per
+   * product, about half the iterations); the stopping test stays the full
+   * system's ||b - A x|| <= eta ||b||.  Single-instance packs small enough
+   * for the one-launch solve keep it; ILU(0) solves and FP32 operators keep
+   * the full system.  0: the full system always. */
+  int32_t red_black;
+  int32_t reserved_opts;  /* 0 */
 } tcad_newton_opts_t;
 
 /* Per-instance result of a Newton solve (host memory). */

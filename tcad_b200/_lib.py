@@ -65,7 +65,8 @@ class NewtonOpts(ctypes.Structure):
                 ("eta_min", ctypes.c_double), ("scale_floor", ctypes.c_double),
                 ("polish_eta", ctypes.c_double), ("polish_scale_floor", ctypes.c_double),
                 ("dt", ctypes.c_double), ("theta", ctypes.c_double),
-                ("n_old", _p), ("p_old", _p), ("fn_old", _p), ("fp_old", _p)]
+                ("n_old", _p), ("p_old", _p), ("fn_old", _p), ("fp_old", _p),
+                ("red_black", ctypes.c_int32), ("reserved_opts", ctypes.c_int32)]
 
 
 class NewtonResult(ctypes.Structure):

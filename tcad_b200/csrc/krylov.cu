@@ -665,6 +665,10 @@ k_true_resid(const tcad_pack_t pk, const TJ* __restrict__ J, const T* __restrict
     fin_true(ks[fb.inst], tot[0], rearm);
 }
 
+}  // namespace tcad
+#include "redblack.cuh"
+namespace tcad {
+
 // ---- the whole solve in one cooperative launch (single-instance packs whose
 // flat blocks all fit on the GPU at once: one CTA per flat block)
 //
@@ -1199,6 +1203,89 @@ static WorkIlu carve_ilu(const tcad_pack_t* pk, void* base) {
   return w;
 }
 
+// Red-black Schur extension: the colour rows of the scaled J, the colours of
+// b, the red pass result, the black iterate and right-hand side (slot arrays
+// sized by n_nodes, which bounds the slot count), the full ||b||^2 and the
+// slot pack's tables
+struct WorkRb {
+  double *JR, *JB, *bR, *bB, *tR, *xb, *rhs, *bbf;
+  int32_t* shape;
+  int64_t* node_off;
+  int64_t* flat_off;
+  int32_t* flat_inst;
+  size_t bytes;
+};
+
+static WorkRb carve_rb(const tcad_pack_t* pk, void* base) {
+  Carve c{reinterpret_cast<char*>(base), 0, 0};
+  WorkRb w;
+  const size_t nn = (size_t)pk->n_nodes, v3 = 3 * nn;
+  const size_t ne = pk->dim == 2 ? TCAD_NE2 : TCAD_NE3;
+  w.JR = c.take<double>(ne * nn);
+  w.JB = c.take<double>(ne * nn);
+  w.bR = c.take<double>(v3);
+  w.bB = c.take<double>(v3);
+  w.tR = c.take<double>(v3);
+  w.xb = c.take<double>(v3);
+  w.rhs = c.take<double>(v3);
+  w.bbf = c.take<double>(pk->n_inst);
+  w.shape = c.take<int32_t>(3 * (size_t)pk->n_inst);
+  w.node_off = c.take<int64_t>((size_t)pk->n_inst + 1);
+  w.flat_off = c.take<int64_t>((size_t)pk->n_inst + 1);
+  w.flat_inst = c.take<int32_t>((size_t)pk->n_flat);
+  w.bytes = c.used;
+  return w;
+}
+
+// The slot pack of a pack (host tables; see redblack.cuh): per instance
+// (ceil(Nx/2), Ny Nz, 1) slots of each colour, flat blocks of pk->flat_nodes
+struct RbLayout {
+  tcad_pack_t pkb;
+  RbMap mp;
+  std::vector<int64_t> hfoff;
+};
+
+static int rb_layout(const tcad_pack_t* pk, const WorkRb& wr, RbLayout& L, cudaStream_t s) {
+  const int ni = pk->n_inst;
+  std::vector<int32_t> shp(3 * (size_t)ni), sb(3 * (size_t)ni), fi;
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(shp.data(), pk->shape, sizeof(int32_t) * shp.size(),
+                                  cudaMemcpyDeviceToHost, s));
+  TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+  std::vector<int64_t> noff(ni + 1), foff(ni + 1);
+  noff[0] = 0; foff[0] = 0;
+  const int64_t fn = pk->flat_nodes;
+  for (int i = 0; i < ni; ++i) {
+    const int64_t hx = (shp[3 * i] + 1) / 2, rows = (int64_t)shp[3 * i + 1] * shp[3 * i + 2];
+    sb[3 * i] = (int32_t)hx; sb[3 * i + 1] = (int32_t)rows; sb[3 * i + 2] = 1;
+    noff[i + 1] = noff[i] + hx * rows;
+    const int64_t nf = (hx * rows + fn - 1) / fn;
+    foff[i + 1] = foff[i] + nf;
+    for (int64_t b = 0; b < nf; ++b) fi.push_back(i);
+  }
+  if (noff[ni] > pk->n_nodes || foff[ni] > pk->n_flat) return TCAD_ERR_ARG;
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(wr.shape, sb.data(), sizeof(int32_t) * sb.size(),
+                                  cudaMemcpyHostToDevice, s));
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(wr.node_off, noff.data(), sizeof(int64_t) * noff.size(),
+                                  cudaMemcpyHostToDevice, s));
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(wr.flat_off, foff.data(), sizeof(int64_t) * foff.size(),
+                                  cudaMemcpyHostToDevice, s));
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(wr.flat_inst, fi.data(), sizeof(int32_t) * fi.size(),
+                                  cudaMemcpyHostToDevice, s));
+  TCAD_CUDA_CHECK(cudaStreamSynchronize(s));   // the host vectors go out of scope
+  L.pkb = *pk;
+  L.pkb.n_nodes = noff[ni];
+  L.pkb.n_flat = foff[ni];
+  L.pkb.shape = wr.shape;
+  L.pkb.node_off = wr.node_off;
+  L.pkb.flat_off = wr.flat_off;
+  L.pkb.flat_inst = wr.flat_inst;
+  L.mp.shape = pk->shape;
+  L.mp.node_off = pk->node_off;
+  L.mp.n_full = pk->n_nodes;
+  L.hfoff = foff;
+  return TCAD_OK;
+}
+
 static Work carve(const tcad_pack_t* pk, void* base, size_t cap) {
   Carve c{reinterpret_cast<char*>(base), 0, cap};
   Work w;
@@ -1277,6 +1364,64 @@ static bool fused_fits(unsigned nb) {
 // as the launch-per-step path).  Returns TCAD_OK with hks[0] filled, or 1
 // when the launch was refused or a grid barrier gave up (the caller then
 // solves with one launch per step).
+// Launch grid of a per-step Krylov loop: every flat block, or -- once the
+// instances still iterating cover under 3/4 of them -- only those instances'
+// blocks (a compact list rebuilt whenever the active set changes), so a
+// batch's stragglers do not pay for launches over finished instances.
+struct ActiveGrid {
+  unsigned nb = 0, ng = 0;
+  const int32_t* dlist = nullptr;
+  int ni = 0;
+  std::vector<int64_t> hfoff;
+  std::vector<int32_t> hlist;
+  std::vector<uint8_t> was_active;
+
+  // hfoff_host: the pack's flat_off on the host (read from the device if null)
+  int init(const tcad_pack_t* pk, cudaStream_t s, const std::vector<int64_t>* hfoff_host) {
+    nb = (unsigned)pk->n_flat;
+    ng = nb;
+    ni = pk->n_inst;
+    if (ni > 1) {
+      if (hfoff_host) {
+        hfoff = *hfoff_host;
+      } else {
+        hfoff.resize(ni + 1);
+        TCAD_CUDA_CHECK(cudaMemcpyAsync(hfoff.data(), pk->flat_off,
+                                        sizeof(int64_t) * (ni + 1), cudaMemcpyDeviceToHost, s));
+        TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+      }
+      was_active.assign(ni, 1);
+    }
+    return TCAD_OK;
+  }
+
+  int update(const std::vector<KState>& hks, int32_t* dev_list, cudaStream_t s) {
+    if (ni <= 1) return TCAD_OK;
+    bool changed = false;
+    int64_t act_blocks = 0;
+    for (int i = 0; i < ni; ++i) {
+      changed = changed || (was_active[i] != (hks[i].active ? 1 : 0));
+      if (hks[i].active) act_blocks += hfoff[i + 1] - hfoff[i];
+    }
+    if (!changed) return TCAD_OK;
+    for (int i = 0; i < ni; ++i) was_active[i] = hks[i].active ? 1 : 0;
+    if (4 * act_blocks < 3 * (int64_t)nb) {
+      hlist.clear();
+      for (int i = 0; i < ni; ++i)
+        if (hks[i].active)
+          for (int64_t b = hfoff[i]; b < hfoff[i + 1]; ++b) hlist.push_back((int32_t)b);
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(dev_list, hlist.data(), sizeof(int32_t) * hlist.size(),
+                                      cudaMemcpyHostToDevice, s));
+      ng = (unsigned)hlist.size();
+      dlist = dev_list;
+    } else {
+      ng = nb;
+      dlist = nullptr;
+    }
+    return TCAD_OK;
+  }
+};
+
 static int launch_bicgstab_fused(const tcad_pack_t* pk, const double* J, const double* b,
                                  double* x, double rtol, int maxiter, const BiVec& bi,
                                  const Work& w, const int32_t* pre_status,
@@ -1348,23 +1493,11 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const TJ* J, const T* b, T* 
   int check = 4;
   int done_iters = 0;
   int rechecks = 0;
-  // Launch grid: every flat block, or -- once the instances still iterating
-  // cover under 3/4 of them -- only those instances' blocks (a compact list
-  // rebuilt whenever the active set changes), so a batch's stragglers do
-  // not pay for launches over finished instances.
-  unsigned ng = nb;
-  const int32_t* dlist = nullptr;
-  std::vector<int64_t> hfoff;
-  std::vector<int32_t> hlist;
-  std::vector<uint8_t> was_active;
-  if (ni > 1) {
-    hfoff.resize(ni + 1);
-    TCAD_CUDA_CHECK(cudaMemcpyAsync(hfoff.data(), pk->flat_off, sizeof(int64_t) * (ni + 1),
-                                    cudaMemcpyDeviceToHost, s));
-    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
-    was_active.assign(ni, 1);
-  }
+  ActiveGrid grid;
+  if (int rc = grid.init(pk, s, nullptr)) return rc;
   for (;;) {
+    const unsigned ng = grid.ng;
+    const int32_t* dlist = grid.dlist;
     for (int q = 0; q < check; ++q) {
       k_bi_p<<<ng, NT, 0, s>>>(*pk, bi, w.ks, dlist);
       note_launch();
@@ -1403,30 +1536,8 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const TJ* J, const T* b, T* 
     TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
     bool any = false;
     for (int i = 0; i < ni; ++i) any = any || hks[i].active;
-    if (any && ni > 1) {
-      bool changed = false;
-      int64_t act_blocks = 0;
-      for (int i = 0; i < ni; ++i) {
-        changed = changed || (was_active[i] != (hks[i].active ? 1 : 0));
-        if (hks[i].active) act_blocks += hfoff[i + 1] - hfoff[i];
-      }
-      if (changed) {
-        for (int i = 0; i < ni; ++i) was_active[i] = hks[i].active ? 1 : 0;
-        if (4 * act_blocks < 3 * (int64_t)nb) {
-          hlist.clear();
-          for (int i = 0; i < ni; ++i)
-            if (hks[i].active)
-              for (int64_t b = hfoff[i]; b < hfoff[i + 1]; ++b) hlist.push_back((int32_t)b);
-          TCAD_CUDA_CHECK(cudaMemcpyAsync(w.blk, hlist.data(), sizeof(int32_t) * hlist.size(),
-                                          cudaMemcpyHostToDevice, s));
-          ng = (unsigned)hlist.size();
-          dlist = w.blk;
-        } else {
-          ng = nb;
-          dlist = nullptr;
-        }
-      }
-    }
+    if (any)
+      if (int rc = grid.update(hks, w.blk, s)) return rc;
     if (!any) {
       // true-residual check; instances whose recursive residual drifted are
       // re-armed from the true residual (bounded number of re-checks)
@@ -1447,6 +1558,111 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const TJ* J, const T* b, T* 
     if (done_iters > 64) check = 16;
     if (done_iters > 1024) check = 32;
   }
+  return TCAD_OK;
+}
+
+// BiCGStab on the red-black Schur complement of A^ (redblack.cuh): the same
+// per-instance stopping test ||b - A^ x|| <= rtol ||b|| as launch_bicgstab_t,
+// the same vector kernels on the black slot pack, and the full solution x
+// (node layout) at the end.  JR / JB must hold the colour rows of the current
+// J (k_rb_pack after the block-Jacobi set-up).
+static int launch_bicgstab_rb(const tcad_pack_t* pk, const RbLayout& L, const WorkRb& wr,
+                              const double* b, double* x, double rtol, int maxiter,
+                              const Work& w, const int32_t* pre_status,
+                              std::vector<KState>& hks, cudaStream_t s,
+                              const double* rtol_inst) {
+  const tcad_pack_t& pkb = L.pkb;
+  const unsigned nbb = (unsigned)pkb.n_flat;
+  const int ni = pk->n_inst;
+  const bool d2 = pk->dim == 2;
+  BiVec bi = w.bi;   // black vectors (stride: the slot count)
+  bi.ph = bi.p;
+  bi.sh = bi.s;
+  TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
+  if (d2) k_rb_split<2><<<nbb, NT, 0, s>>>(pkb, L.mp, b, wr.bR, wr.bB, wr.bbf, w.partial, w.ticket);
+  else    k_rb_split<3><<<nbb, NT, 0, s>>>(pkb, L.mp, b, wr.bR, wr.bB, wr.bbf, w.partial, w.ticket);
+  note_launch();
+  if (d2)
+    k_rb_init<2><<<nbb, NT, 0, s>>>(pkb, L.mp, wr.JB, wr.bR, wr.bB, wr.rhs, wr.xb, bi, wr.bbf,
+                                    w.ks, w.partial, w.ticket, rtol, maxiter, pre_status,
+                                    rtol_inst);
+  else
+    k_rb_init<3><<<nbb, NT, 0, s>>>(pkb, L.mp, wr.JB, wr.bR, wr.bB, wr.rhs, wr.xb, bi, wr.bbf,
+                                    w.ks, w.partial, w.ticket, rtol, maxiter, pre_status,
+                                    rtol_inst);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  hks.resize(ni);
+  int check = 4, done_iters = 0, rechecks = 0;
+  ActiveGrid grid;
+  if (int rc = grid.init(&pkb, s, &L.hfoff)) return rc;
+  for (;;) {
+    const unsigned ng = grid.ng;
+    const int32_t* dlist = grid.dlist;
+    for (int q = 0; q < check; ++q) {
+      k_bi_p<<<ng, NT, 0, s>>>(pkb, bi, w.ks, dlist);
+      if (d2) {
+        k_rb_red<2><<<ng, NT, 0, s>>>(pkb, L.mp, wr.JR, bi.p, wr.tR, w.ks, dlist);
+        k_rb_v<2><<<ng, NT, 0, s>>>(pkb, L.mp, wr.JB, wr.tR, bi, w.ks, w.partial, w.ticket,
+                                    dlist);
+      } else {
+        k_rb_red<3><<<ng, NT, 0, s>>>(pkb, L.mp, wr.JR, bi.p, wr.tR, w.ks, dlist);
+        k_rb_v<3><<<ng, NT, 0, s>>>(pkb, L.mp, wr.JB, wr.tR, bi, w.ks, w.partial, w.ticket,
+                                    dlist);
+      }
+      k_bi_s<<<ng, NT, 0, s>>>(pkb, bi, w.ks, w.partial, w.ticket, dlist);
+      if (d2) {
+        k_rb_red<2><<<ng, NT, 0, s>>>(pkb, L.mp, wr.JR, bi.s, wr.tR, w.ks, dlist);
+        k_rb_t<2><<<ng, NT, 0, s>>>(pkb, L.mp, wr.JB, wr.tR, bi, w.ks, w.partial, w.ticket,
+                                    dlist);
+      } else {
+        k_rb_red<3><<<ng, NT, 0, s>>>(pkb, L.mp, wr.JR, bi.s, wr.tR, w.ks, dlist);
+        k_rb_t<3><<<ng, NT, 0, s>>>(pkb, L.mp, wr.JB, wr.tR, bi, w.ks, w.partial, w.ticket,
+                                    dlist);
+      }
+      k_bi_x<<<ng, NT, 0, s>>>(pkb, wr.xb, bi, w.ks, w.partial, w.ticket, dlist);
+      for (int l = 0; l < 7; ++l) note_launch();
+    }
+    TCAD_LAUNCH_CHECK();
+    done_iters += check;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState) * ni,
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+    if (any)
+      if (int rc = grid.update(hks, w.blk, s)) return rc;
+    if (!any) {
+      // true Schur residual (= the full residual); re-arm drifted instances
+      const int rearm = rechecks < 8 ? 1 : 0;
+      if (d2) {
+        k_rb_red<2><<<nbb, NT, 0, s>>>(pkb, L.mp, wr.JR, wr.xb, wr.tR, nullptr, nullptr);
+        k_rb_true<2><<<nbb, NT, 0, s>>>(pkb, L.mp, wr.JB, wr.tR, wr.rhs, wr.xb, bi.r, w.ks,
+                                        w.partial, w.ticket, rearm);
+      } else {
+        k_rb_red<3><<<nbb, NT, 0, s>>>(pkb, L.mp, wr.JR, wr.xb, wr.tR, nullptr, nullptr);
+        k_rb_true<3><<<nbb, NT, 0, s>>>(pkb, L.mp, wr.JB, wr.tR, wr.rhs, wr.xb, bi.r, w.ks,
+                                        w.partial, w.ticket, rearm);
+      }
+      note_launch();
+      note_launch();
+      TCAD_LAUNCH_CHECK();
+      TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState) * ni,
+                                      cudaMemcpyDeviceToHost, s));
+      TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+      for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+      ++rechecks;
+      if (!any) break;
+      if (int rc = grid.update(hks, w.blk, s)) return rc;
+    }
+    if (done_iters > 64) check = 16;
+    if (done_iters > 1024) check = 32;
+  }
+  // x_r = b_r - E x_b (tR from the last true-residual pass holds E x_b)
+  if (d2) k_rb_merge<2><<<nbb, NT, 0, s>>>(pkb, L.mp, wr.bR, wr.tR, wr.xb, x, pre_status);
+  else    k_rb_merge<3><<<nbb, NT, 0, s>>>(pkb, L.mp, wr.bR, wr.tR, wr.xb, x, pre_status);
+  note_launch();
+  TCAD_LAUNCH_CHECK();
   return TCAD_OK;
 }
 
@@ -1596,15 +1812,21 @@ extern "C" int tcad_set_krylov_fused(int on) {
   return g_fused_mode.exchange(on ? 1 : 0);
 }
 
+// offsets of the workspace's extensions: FP64 work, then the FP32 extension,
+// the ILU(0) extension and the red-black Schur extension
+static size_t rnd256(size_t b) { return (b + 255) & ~(size_t)255; }
+static size_t off_w32(const tcad_pack_t* pk) { return rnd256(carve(pk, nullptr, 0).bytes); }
+static size_t off_ilu(const tcad_pack_t* pk) {
+  return off_w32(pk) + rnd256(carve32(pk, nullptr).bytes);
+}
+static size_t off_rb(const tcad_pack_t* pk) {
+  return off_ilu(pk) + rnd256(carve_ilu(pk, nullptr).bytes);
+}
+
 extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart) {
   if (!pk) return 0;
   (void)method; (void)restart;
-  Work w = carve(pk, nullptr, 0);
-  Work32 w32 = carve32(pk, nullptr);
-  WorkIlu wi = carve_ilu(pk, nullptr);
-  // FP64 work, then the FP32 extension, then the ILU(0) extension (2D)
-  return ((w.bytes + 255) & ~(size_t)255) + ((w32.bytes + 255) & ~(size_t)255) + wi.bytes +
-         512;
+  return off_rb(pk) + carve_rb(pk, nullptr).bytes + 512;
 }
 
 extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
@@ -1714,13 +1936,29 @@ extern "C" int tcad_block_krylov(const tcad_pack_t* pk, const double* J, const d
                                  int restart, void* work, size_t work_bytes, int32_t* iters,
                                  int32_t* status, double* relres, void* stream) {
   if (!pack_ok(pk) || !work) return TCAD_ERR_ARG;
-  if (method != 0) return TCAD_ERR_ARG;  // GMRES on the block layout: not in this library
+  if (method != 0 && method != 2) return TCAD_ERR_ARG;  // GMRES: the CSR entry point
   (void)restart;
   Work w = carve(pk, work, work_bytes);
   if (w.bytes > work_bytes) return TCAD_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<KState> hks;
-  const int rc = launch_bicgstab(pk, J, b, x, rtol, maxiter, w, nullptr, hks, s);
+  int rc;
+  if (method == 2) {
+    if (work_bytes < tcad_block_workspace_bytes(pk, 0, 0)) return TCAD_ERR_ARG;
+    const WorkRb wrb = carve_rb(pk, reinterpret_cast<char*>(work) + off_rb(pk));
+    RbLayout rbl;
+    if ((rc = rb_layout(pk, wrb, rbl, s)) != TCAD_OK) return rc;
+    const unsigned nbb = (unsigned)rbl.pkb.n_flat;
+    if (pk->dim == 2)
+      k_rb_pack<2><<<nbb, NT, 0, s>>>(rbl.pkb, rbl.mp, J, wrb.JR, wrb.JB);
+    else
+      k_rb_pack<3><<<nbb, NT, 0, s>>>(rbl.pkb, rbl.mp, J, wrb.JR, wrb.JB);
+    note_launch();
+    TCAD_LAUNCH_CHECK();
+    rc = launch_bicgstab_rb(pk, rbl, wrb, b, x, rtol, maxiter, w, nullptr, hks, s, nullptr);
+  } else {
+    rc = launch_bicgstab(pk, J, b, x, rtol, maxiter, w, nullptr, hks, s);
+  }
   if (rc != TCAD_OK) return rc;
   for (int i = 0; i < pk->n_inst; ++i) {
     if (iters) iters[i] = hks[i].it;
@@ -1794,6 +2032,19 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   if (use_ilu && (pk->dim != 2 || pack_max_short_side(pk, s) > kIluThreads)) {
     wilu_use.Mf = nullptr;  // node-order sweeps
     wilu_use.Mb = nullptr;
+  }
+  // red-black Schur solves: the slot pack's tables, once per call.  A
+  // single-instance pack that fits the one-launch solve keeps it (that solve
+  // is latency-bound; the Schur loop takes seven launches per iteration).
+  const bool fused_small = g_fused_mode.load() && ni == 1 &&
+                           (pk->dim == 2 ? fused_fits<2>(nb) : fused_fits<3>(nb));
+  const bool use_rb = opts->red_black != 0 && !fused_small;
+  if (use_rb && work_bytes < tcad_block_workspace_bytes(pk, 0, 0)) return TCAD_ERR_ARG;
+  WorkRb wrb{};
+  RbLayout rbl;
+  if (use_rb) {
+    wrb = carve_rb(pk, reinterpret_cast<char*>(work) + off_rb(pk));
+    if (int rc = rb_layout(pk, wrb, rbl, s)) return rc;
   }
   std::vector<int32_t> mix_it(ni), mix_st(ni), mix_grew(ni, 0), mix_steps(ni, 0);
   std::vector<double> mix_rr(ni), mix_prev(ni, -1.0);
@@ -2003,6 +2254,16 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
         rc = launch_bicgstab_t<double, float>(pk, w32.J32, F, du, opts->rtol,
                                               opts->krylov_maxiter, w.bi, w, w.status, hks, s,
                                               w.eta);
+      } else if (use_rb && !any_ilu) {
+        const unsigned nbb = (unsigned)rbl.pkb.n_flat;
+        if (pk->dim == 2)
+          k_rb_pack<2><<<nbb, NT, 0, s>>>(rbl.pkb, rbl.mp, J, wrb.JR, wrb.JB);
+        else
+          k_rb_pack<3><<<nbb, NT, 0, s>>>(rbl.pkb, rbl.mp, J, wrb.JR, wrb.JB);
+        note_launch();
+        TCAD_LAUNCH_CHECK();
+        rc = launch_bicgstab_rb(pk, rbl, wrb, F, du, opts->rtol, opts->krylov_maxiter, w,
+                                w.status, hks, s, w.eta);
       } else {
         rc = launch_bicgstab(pk, J, F, du, opts->rtol, opts->krylov_maxiter, w, w.status, hks,
                              s, w.eta, any_ilu ? &wilu_use : nullptr, nzmax);

@@ -136,6 +136,14 @@ class NewtonOptions:
     # same discrete solution either way; a predicted start that fails to
     # converge is retried from the previous state.
     predictor: str = "secant"
+    # GPU-only: the system the node-block-Jacobi BiCGStab iterates on.
+    # "red_black" eliminates the red nodes ((i + j + k) even) exactly -- the
+    # face-neighbour stencil couples no two nodes of one colour -- and
+    # iterates on the Schur complement over the black nodes: half the
+    # unknowns, the same matrix bytes per operator product, and on the
+    # tri-gate Newton systems about half the iterations; the stopping test is
+    # the full system's.  "full" iterates on the whole block-scaled system.
+    krylov_system: str = "full"
 
     def __post_init__(self):
         if self.precond not in ("auto", "block_jacobi", "schur", "ilu"):
@@ -150,6 +158,9 @@ class NewtonOptions:
             raise ValueError(f"unknown linsolve {self.linsolve!r}")
         if self.predictor not in ("none", "secant"):
             raise ValueError(f"NewtonOptions.predictor={self.predictor!r}: 'none' or 'secant'")
+        if self.krylov_system not in ("full", "red_black"):
+            raise ValueError(f"NewtonOptions.krylov_system={self.krylov_system!r}: 'full' or "
+                             "'red_black'")
         if self.precision not in ("fp64", "mixed", "fp32_operator"):
             raise ValueError(f"NewtonOptions.precision={self.precision!r}: 'fp64', 'mixed' "
                              "or 'fp32_operator'")

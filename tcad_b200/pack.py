@@ -683,6 +683,7 @@ class Pack:
         o.precond = {"ilu": 1, "auto": 2, "schur": 2}.get(pc, 0)
         o.polish_eta = float(getattr(opts, "polish_eta", 1e-10))
         o.polish_scale_floor = float(getattr(opts, "polish_scale_floor", 0.0))
+        o.red_black = 1 if getattr(opts, "krylov_system", "full") == "red_black" else 0
         return o
 
     def set_tile_z(self, tile_z):
