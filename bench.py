@@ -75,6 +75,8 @@ METHODS = {
                    predictor="secant"),
     "rb": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative",
                predictor="secant", krylov_system="red_black"),
+    "rb_bj": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative",
+                  predictor="secant", krylov_system="red_black", precond="block_jacobi"),
 }
 METHOD_DESC = {
     "plain": "plain FP64: fused SG assembly, node-block-Jacobi BiCGStab to rtol 1e-10 on "
@@ -88,6 +90,8 @@ METHOD_DESC = {
     "rb": "FP64 inexact Newton as 'fp64', with the BiCGStab on the red-black Schur "
           "complement of the block-scaled system (red nodes eliminated exactly; the full "
           "system's stopping test)",
+    "rb_bj": "as 'rb', with node-block Jacobi for every instance (2D batches included, "
+             "which otherwise take ILU(0))",
     "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
              "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
              "relative unknowns, adaptive forcing, secant predictor; per-instance FP64 "
