@@ -54,38 +54,42 @@ __device__ __forceinline__ RbGeo rb_geo(const tcad_pack_t& pkb, const RbMap& mp,
 
 struct RbNode {
   int i, j, k;
-  int64_t row;
+  int row;       // j + ny k
   int64_t node;  // index in the original pack
   bool real;     // false: a pad slot
 };
 
+// Index arithmetic is 32-bit and instance-local (an instance has far fewer
+// than 2^31 slots): 64-bit division is a long instruction sequence and its
+// registers halved the occupancy of the passes.
 __device__ __forceinline__ RbNode rb_node(const RbGeo& g, int64_t slot, int colour) {
   RbNode q;
-  const int64_t local = slot - g.soff;
-  q.row = local / g.hx;
-  const int hi = (int)(local - q.row * g.hx);
-  q.j = (int)(q.row % g.ny);
-  q.k = (int)(q.row / g.ny);
+  const unsigned local = (unsigned)(slot - g.soff);
+  const unsigned row = local / (unsigned)g.hx;
+  const int hi = (int)(local - row * (unsigned)g.hx);
+  const unsigned k = row / (unsigned)g.ny;
+  q.row = (int)row;
+  q.k = (int)k;
+  q.j = (int)(row - k * (unsigned)g.ny);
   q.i = 2 * hi + (((q.j + q.k) & 1) ^ colour);
   q.real = q.i < g.nx;
-  q.node = g.ooff + q.row * g.nx + q.i;
+  q.node = g.ooff + (int64_t)row * g.nx + q.i;
   return q;
 }
 
-// slots (in the other colour's arrays) of the face neighbours x-, x+, y-, y+,
-// z-, z+ -- the order of the Jacobian's neighbour entries; a missing
-// neighbour gets the node's own slot (its Jacobian entries are zero)
+// instance-local slots (in the other colour's arrays) of the face neighbours
+// x-, x+, y-, y+, z-, z+ -- the order of the Jacobian's neighbour entries; a
+// missing neighbour gets the node's own slot (its Jacobian entries are zero)
 template <int DIM>
-__device__ __forceinline__ void rb_nbrs(const RbGeo& g, const RbNode& q, int64_t self,
-                                        int64_t* m) {
-  const int64_t base = g.soff + q.row * g.hx;
+__device__ __forceinline__ void rb_nbrs(const RbGeo& g, const RbNode& q, int self, int* m) {
+  const int base = q.row * g.hx;
   const int h = q.i >> 1;
   m[0] = q.i > 0 ? base + ((q.i - 1) >> 1) : self;
   m[1] = q.i + 1 < g.nx ? base + ((q.i + 1) >> 1) : self;
   m[2] = q.j > 0 ? base - g.hx + h : self;
   m[3] = q.j + 1 < g.ny ? base + g.hx + h : self;
   if (DIM == 3) {
-    const int64_t plane = (int64_t)g.ny * g.hx;
+    const int plane = g.ny * g.hx;
     m[4] = q.k > 0 ? base - plane + h : self;
     m[5] = q.k + 1 < g.nz ? base + plane + h : self;
   }
@@ -93,17 +97,18 @@ __device__ __forceinline__ void rb_nbrs(const RbGeo& g, const RbNode& q, int64_t
 
 // y = D (sum_d A_d x_m(d)) at one slot of a colour array Jc ([NE][NS]; the
 // set-up's D^-1 in entries 0..8, the raw neighbour entries after them): the
-// coupling part of A^ on the other colour's values x
+// coupling part of A^ on the other colour's values; xi = that colour's
+// vector from the instance's first slot, m instance-local
 template <int DIM>
 __device__ __forceinline__ void rb_couple(const double* __restrict__ Jc,
-                                          const double* __restrict__ x, int64_t slot,
-                                          int64_t NS, const int64_t* m, double& y0,
-                                          double& y1, double& y2) {
+                                          const double* __restrict__ xi, int64_t slot,
+                                          int64_t NS, const int* m, double& y0, double& y1,
+                                          double& y2) {
   double t0 = 0.0, t1 = 0.0, t2 = 0.0;
 #pragma unroll
   for (int d = 0; d < 2 * DIM; ++d) {
     const int e = 9 + 5 * d;
-    const double xs = x[m[d]], xn = x[NS + m[d]], xp = x[2 * NS + m[d]];
+    const double xs = xi[m[d]], xn = xi[NS + m[d]], xp = xi[2 * NS + m[d]];
     t0 += Jc[(int64_t)e * NS + slot] * xs;
     t1 += Jc[(int64_t)(e + 1) * NS + slot] * xs + Jc[(int64_t)(e + 2) * NS + slot] * xn;
     t2 += Jc[(int64_t)(e + 3) * NS + slot] * xs + Jc[(int64_t)(e + 4) * NS + slot] * xp;
@@ -169,7 +174,7 @@ k_rb_split(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ b,
 // red pass: Tr = E x (the red rows' coupling to black values x); every
 // instance when ks is null, else only those still iterating
 template <int DIM>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 3)
 k_rb_red(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JR,
          const double* __restrict__ x, double* __restrict__ Tr, const KState* ks,
          const int32_t* __restrict__ blk) {
@@ -182,9 +187,9 @@ k_rb_red(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JR,
     const RbNode q = rb_node(g, slot, 0);
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
     if (q.real) {
-      int64_t m[6];
-      rb_nbrs<DIM>(g, q, slot, m);
-      rb_couple<DIM>(JR, x, slot, NS, m, y0, y1, y2);
+      int m[6];
+      rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
+      rb_couple<DIM>(JR, x + g.soff, slot, NS, m, y0, y1, y2);
     }
     Tr[slot] = y0; Tr[NS + slot] = y1; Tr[2 * NS + slot] = y2;
   }
@@ -199,10 +204,10 @@ __device__ __forceinline__ void rb_black(const RbGeo& g, const double* __restric
   const RbNode q = rb_node(g, slot, 1);
   y0 = 0.0; y1 = 0.0; y2 = 0.0;
   if (!q.real) return;
-  int64_t m[6];
-  rb_nbrs<DIM>(g, q, slot, m);
+  int m[6];
+  rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
   double u0, u1, u2;
-  rb_couple<DIM>(JB, Tr, slot, NS, m, u0, u1, u2);
+  rb_couple<DIM>(JB, Tr + g.soff, slot, NS, m, u0, u1, u2);
   y0 = X[slot] - u0;
   y1 = X[NS + slot] - u1;
   y2 = X[2 * NS + slot] - u2;
@@ -211,7 +216,7 @@ __device__ __forceinline__ void rb_black(const RbGeo& g, const double* __restric
 // Schur right-hand side and BiCGStab start: rhs = bB - F bR; x = 0,
 // r = rh = rhs, p = v = 0; the tolerance is on the full ||b|| (bbf)
 template <int DIM>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 3)
 k_rb_init(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
           const double* __restrict__ bR, const double* __restrict__ bB,
           double* __restrict__ rhs, double* __restrict__ x, BiVec w,
@@ -252,7 +257,7 @@ k_rb_init(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
 
 // v = S p (S = I - F E; Tr = E p from the red pass); (rh, v)
 template <int DIM>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 3)
 k_rb_v(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
        const double* __restrict__ Tr, BiVec w, KState* ks, double* partial, unsigned* ticket,
        const int32_t* __restrict__ blk) {
@@ -279,7 +284,7 @@ k_rb_v(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
 
 // t = S s (Tr = E s); (t, s), (t, t)
 template <int DIM>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 3)
 k_rb_t(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
        const double* __restrict__ Tr, BiVec w, KState* ks, double* partial, unsigned* ticket,
        const int32_t* __restrict__ blk) {
@@ -307,7 +312,7 @@ k_rb_t(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
 // true Schur residual r = rhs - S x (Tr = E x), which is the black part of
 // the full residual (its red part is zero); (r, r); re-arm as k_true_resid
 template <int DIM>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 3)
 k_rb_true(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
           const double* __restrict__ Tr, const double* __restrict__ rhs,
           const double* __restrict__ x, double* __restrict__ r, KState* ks, double* partial,
