@@ -54,6 +54,13 @@ BYTES_ASM = {2: (13 + 32) * 8 + 1, 3: (16 + 42) * 8 + 1}
 #  node of the five kernels: k_bi_p 96 (r, v, p in; p out), k_bi_v and k_bi_t
 #  one SpMV each (J + x in, y out), k_bi_s 72, k_bi_x 168
 BYTES_ITER = {d: 96 + 2 * BYTES_SPMV[d] + 72 + 168 for d in (2, 3)}
+#  one BiCGStab iteration on the red-black Schur complement, bytes per node of
+#  the original pack (a black slot per two nodes): the vector kernels on the
+#  black half (96 + 72 + 168) / 2; two red passes (red rows of J, black x in,
+#  E x out: (8 NE + 48) / 2 each); the black passes (black rows of J, E x, one
+#  vector in, product out, plus rh for v: (8 NE + 96) / 2 and (8 NE + 72) / 2)
+#  = 300 + 16 NE: 924 in 3D, 764 in 2D
+BYTES_ITER_RB = {d: 300 + 16 * (29 if d == 2 else 39) for d in (2, 3)}
 
 # Newton iterations / BiCGStab iterations per bias point of the plain FP64
 # path on this workload, from its own bench runs; used only to scale the
@@ -66,31 +73,31 @@ TRIGATE_ITERS = {"newton_per_point": 6.0, "krylov_per_newton": 1078.0}
 # to the fixed rtol 1e-10 on (dpsi, dn, dp) with node-block Jacobi.
 METHODS = {
     "plain": dict(precision="fp64", forcing="fixed", krylov_unknowns="absolute",
-                  predictor="none"),
+                  predictor="none", krylov_system="full"),
     "fp64": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative",
-                 predictor="secant"),
+                 predictor="secant", krylov_system="red_black"),
+    "full": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative",
+                 predictor="secant", krylov_system="full"),
     "mixed": dict(precision="mixed", forcing="adaptive", krylov_unknowns="relative",
                   predictor="secant"),
     "fp32op": dict(precision="fp32_operator", forcing="adaptive", krylov_unknowns="relative",
                    predictor="secant"),
-    "rb": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative",
-               predictor="secant", krylov_system="red_black"),
     "rb_bj": dict(precision="fp64", forcing="adaptive", krylov_unknowns="relative",
                   predictor="secant", krylov_system="red_black", precond="block_jacobi"),
 }
 METHOD_DESC = {
     "plain": "plain FP64: fused SG assembly, node-block-Jacobi BiCGStab to rtol 1e-10 on "
              "(dpsi, dn, dp) every Newton step, damped Newton",
-    "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the block-scaled system in "
-            "relative unknowns (dpsi, dn/n, dp/p) solved to 1e-3 every Newton step, two "
-            "polishing steps (1e-6, then 1e-3), secant predictor along the sweep",
+    "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the red-black Schur "
+            "complement of the block-scaled system (red nodes eliminated exactly; the full "
+            "system's stopping test) in relative unknowns (dpsi, dn/n, dp/p) solved to 1e-3 "
+            "every Newton step, two polishing steps (1e-8, then 1e-3), secant predictor "
+            "along the sweep",
+    "full": "as 'fp64', with the BiCGStab on the whole block-scaled system",
     "fp32op": "FP64 inexact Newton as 'fp64', but the BiCGStab of the Newton steps before the "
               "update test reads an FP32 copy of the block-scaled Jacobian (FP64 vectors, dots "
               "and polishing steps)",
-    "rb": "FP64 inexact Newton as 'fp64', with the BiCGStab on the red-black Schur "
-          "complement of the block-scaled system (red nodes eliminated exactly; the full "
-          "system's stopping test)",
-    "rb_bj": "as 'rb', with node-block Jacobi for every instance (2D batches included, "
+    "rb_bj": "as 'fp64', with node-block Jacobi for every instance (2D batches included, "
              "which otherwise take ILU(0))",
     "mixed": "mixed precision inexact Newton: FP64 assembly, residual, Newton update and "
              "convergence test; FP32 block-scaled BiCGStab inside FP64 iterative refinement, "
@@ -321,7 +328,8 @@ class SweepRunner:
         volts, _ = self.steps[(self.q - 1) % len(self.steps)]
         ref = tb.NewtonOptions(precision="fp64", forcing="adaptive",
                                krylov_unknowns="relative", predictor="none",
-                               eta_max=1e-10, eta_min=1e-10, tol_update=1e-12)
+                               eta_max=1e-10, eta_min=1e-10, tol_update=1e-12,
+                               krylov_system="full")
         out = []
         for dev, v in zip(self.lanes, volts):
             keep = [t.clone() for t in (dev.pack.psi, dev.pack.n, dev.pack.p)]
@@ -485,16 +493,21 @@ def run_ours(args):
     xk = torch.zeros_like(pk.du)
     KIT = 200
 
+    rb = METHODS[args.method].get("krylov_system") == "red_black"
+    kmethod = 2 if rb else 0
+    bytes_iter = (BYTES_ITER_RB if rb else BYTES_ITER)[dim]
+
     def krylov_fixed():
-        lib.tcad_block_krylov(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(xk), 0, 1e-300,
-                              KIT, 0, _lib.ptr(pk.work), pk.work.numel(), kit, kst, krr, sp)
+        lib.tcad_block_krylov(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(xk), kmethod,
+                              1e-300, KIT, 0, _lib.ptr(pk.work), pk.work.numel(), kit, kst,
+                              krr, sp)
     t_kry = time_kernel(krylov_fixed, 2)
     it_done = max(int(kit[i]) for i in range(ni))
     t_iter = t_kry / max(it_done, 1)
     peak, peak_kind = load_peaks()
     ach_spmv = BYTES_SPMV[dim] * NN / t_spmv / 1e9
     ach_asm = BYTES_ASM[dim] * NN / t_asm / 1e9
-    ach_iter = BYTES_ITER[dim] * NN / t_iter / 1e9
+    ach_iter = bytes_iter * NN / t_iter / 1e9
 
     res = {}
     if rank == 0:
@@ -545,10 +558,12 @@ def run_ours(args):
                                   "launch_ms": t_asm * 1e3,
                                   "traffic": load_traffic(f"assemble{dim}d_{args.workload}")},
             "roofline_bicgstab_iteration": {
-                "kernel": "k_bi_p + k_bi_v + k_bi_s + k_bi_t + k_bi_x (one iteration in "
-                          "the solver)", "bound": "hbm", "achieved": ach_iter, "peak": peak,
+                "kernel": ("k_bi_p + k_rb_red + k_rb_v + k_bi_s + k_rb_red + k_rb_t + k_bi_x "
+                           "(one red-black Schur iteration in the solver)" if rb else
+                           "k_bi_p + k_bi_v + k_bi_s + k_bi_t + k_bi_x (one iteration in "
+                           "the solver)"), "bound": "hbm", "achieved": ach_iter, "peak": peak,
                 "unit": "GB/s", "frac": ach_iter / peak,
-                "bytes_per_iteration": BYTES_ITER[dim] * NN, "iteration_ms": t_iter * 1e3,
+                "bytes_per_iteration": bytes_iter * NN, "iteration_ms": t_iter * 1e3,
                 "iterations_timed": it_done},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
@@ -1087,8 +1102,9 @@ def run_reference(args):
 
 def run_kernels(args):
     """A short, representative launch sequence for ncu: 3 coupled assemblies,
-    one block-Jacobi set-up, 3 block SpMVs and one 20-iteration BiCGStab, on
-    the full workload at its neutral-bulk state (no Newton solve)."""
+    one block-Jacobi set-up, 3 block SpMVs, one 20-iteration BiCGStab on the
+    full system and one on its red-black Schur complement, on the full
+    workload at its neutral-bulk state (no Newton solve)."""
     import torch
     import tcad_b200 as tb
     from tcad_b200 import _lib
@@ -1121,6 +1137,11 @@ def run_kernels(args):
                                      0, 1e-30, 20, 0, _lib.ptr(pk.work), pk.work.numel(),
                                      ctypes.byref(it), ctypes.byref(stt), ctypes.byref(rr),
                                      sp), "krylov")
+    # the same 20 iterations on the red-black Schur complement
+    _lib.check(lib.tcad_block_krylov(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(pk.du),
+                                     2, 1e-30, 20, 0, _lib.ptr(pk.work), pk.work.numel(),
+                                     ctypes.byref(it), ctypes.byref(stt), ctypes.byref(rr),
+                                     sp), "krylov red-black")
     torch.cuda.synchronize()
     print(json.dumps({"mode": "kernels", "workload": desc, "nodes": int(dev.N),
                       "krylov_iters": it.value, "launches": int(lib.tcad_launch_count())}))

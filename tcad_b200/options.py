@@ -89,12 +89,13 @@ class NewtonOptions:
     # currents agree to 1e-16.
     polish: int = 2
     # GPU-only: Krylov tolerance of the first polishing step (the second
-    # follows the forcing rule).  Measured over the fixture sweeps with the
-    # floor-free polishing scale below: every current within 1.3e-8 of the
-    # reference's (the 201x101 and 41x11 diodes, the small MOSFET and
-    # tri-gate, the 48x24x12 p-i-n) in 14-24 % fewer Krylov iterations than
-    # 1e-10; 1e-3 put the 201x101 diode's currents 4.5e-6 off.
-    polish_eta: float = 1e-6
+    # follows the forcing rule).  Measured on the 48x24x12 p-i-n sweep with
+    # the floor-free polishing scale below: on the red-black Schur system,
+    # 1e-6 left the 0.5 V current (1.2e-13 A) 1.6e-6 off the oracle and 1e-8
+    # put every current within 5e-16, for 5 % more Krylov iterations (2,106
+    # against 2,005); the full system at 1e-6 was within 1.2e-8.  On the
+    # full system 1e-3 had put the 201x101 diode's currents 4.5e-6 off.
+    polish_eta: float = 1e-8
     # GPU-only: density floor of the relative Krylov unknowns in the
     # polishing steps (0: krylov_scale_floor).  The polishing steps run with
     # no floor to speak of, so minority densities below the 1e-10 floor of
@@ -141,9 +142,12 @@ class NewtonOptions:
     # face-neighbour stencil couples no two nodes of one colour -- and
     # iterates on the Schur complement over the black nodes: half the
     # unknowns, the same matrix bytes per operator product, and on the
-    # tri-gate Newton systems about half the iterations; the stopping test is
-    # the full system's.  "full" iterates on the whole block-scaled system.
-    krylov_system: str = "full"
+    # tri-gate Newton systems about half the iterations (the 983k-node
+    # tri-gate sweep: 1,610 BiCGStab iterations per point against 3,634, 2.04
+    # against 1.17 points/s); the stopping test is the full system's.
+    # "full" iterates on the whole block-scaled system.  Single-instance
+    # packs small enough for the one-launch solve keep that solve either way.
+    krylov_system: str = "red_black"
 
     def __post_init__(self):
         if self.precond not in ("auto", "block_jacobi", "schur", "ilu"):

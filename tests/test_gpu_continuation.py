@@ -57,16 +57,22 @@ def test_adaptive_sweep_backs_off_and_matches_ordered_solves():
 def test_arc_length_sweep_lies_on_the_oracle_branch():
     """Pseudo-arclength continuation (the bordered corrector on the GPU
     Jacobian) along the 41x11 diode's forward branch 0 -> 0.6 V: every
-    traced (V, I) lies on the oracle's voltage-controlled solution at that
-    V (exact Newton to 1e-12), within 1e-6 relative (on 1e-9 x the
-    branch's largest current); the branch has no
-    fold, so V increases monotonically, and the trace reaches v_end."""
+    traced state lies on the oracle's voltage-controlled solution at that V
+    (exact Newton to 1e-12): psi within 1e-9 V and the quasi-Fermi levels
+    within 1e-8 V at every node, and the current within 1e-6 relative where
+    it exceeds 1e-4 x the branch's largest.  Below that the current of this
+    device is a difference of contact fluxes so much larger that it is set by
+    the last bits of the state: at 0.07 V the bias-controlled GPU Newton and
+    the oracle reach states within 4e-15 (psi, relative n) and currents
+    7.7e-4 apart (5.06e-12 A/cm), and the oracle's own current sum at the
+    GPU state gives the GPU's value.  The branch has no fold, so V increases
+    monotonically, and the trace reaches v_end."""
     import numpy as np
     import fixtures as fx
     from tcad_b200.continuation import arc_length_sweep
     dev = _diode()
     dev.solve_equilibrium()
-    recs = arc_length_sweep(dev, "anode", 0.0, 0.6, 0.05)
+    recs = arc_length_sweep(dev, "anode", 0.0, 0.6, 0.05, keep_states=True)
     V = np.array([r["V"] for r in recs])
     assert V[-1] >= 0.6 and np.all(np.diff(V) > 0)
     assert len(recs) >= 6
@@ -77,13 +83,15 @@ def test_arc_length_sweep_lies_on_the_oracle_branch():
     for r in recs:
         ora.solve_bias({"anode": r["V"]}, tol=1e-12)
         Iref.append(ora.terminal_current("anode"))
-    # on 1e-9 x the branch's largest current: near 0 V the current (~1e-13
-    # A/cm against ~1e-3 at 0.6 V) is a difference of large fluxes
+        e_psi, e_n, e_p = fx.field_errs(r["psi"], r["n"], r["p"], ora.psi, ora.n, ora.p)
+        assert e_psi * dev.VT < 1e-9, (r["V"], e_psi * dev.VT)
+        assert max(e_n, e_p) * dev.VT < 1e-8, (r["V"], e_n * dev.VT, e_p * dev.VT)
     Iref = np.array(Iref)
     I = np.array([r["I"] for r in recs])
-    scale = np.maximum(np.abs(Iref), 1e-9 * np.abs(Iref).max())
-    err = np.abs(I - Iref) / scale
-    assert err.max() < 1e-6, (V[err.argmax()], I[err.argmax()], Iref[err.argmax()])
+    big = np.abs(Iref) >= 1e-4 * np.abs(Iref).max()
+    assert big.sum() >= 3
+    err = np.abs(I[big] - Iref[big]) / np.abs(Iref[big])
+    assert err.max() < 1e-6, (V[big][err.argmax()], I[big][err.argmax()], Iref[big][err.argmax()])
 
 
 def test_arc_length_sweep_stalls_loudly():
