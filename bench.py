@@ -91,7 +91,7 @@ METHOD_DESC = {
     "fp64": "FP64 inexact Newton: fused SG assembly, BiCGStab on the red-black Schur "
             "complement of the block-scaled system (red nodes eliminated exactly; the full "
             "system's stopping test) in relative unknowns (dpsi, dn/n, dp/p) solved to 1e-3 "
-            "every Newton step, two polishing steps (1e-8, then 1e-3), secant predictor "
+            "every Newton step, two polishing steps (1e-6, then 1e-3), secant predictor "
             "along the sweep",
     "full": "as 'fp64', with the BiCGStab on the whole block-scaled system",
     "fp32op": "FP64 inexact Newton as 'fp64', but the BiCGStab of the Newton steps before the "

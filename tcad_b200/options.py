@@ -89,13 +89,14 @@ class NewtonOptions:
     # currents agree to 1e-16.
     polish: int = 2
     # GPU-only: Krylov tolerance of the first polishing step (the second
-    # follows the forcing rule).  Measured on the 48x24x12 p-i-n sweep with
-    # the floor-free polishing scale below: on the red-black Schur system,
-    # 1e-6 left the 0.5 V current (1.2e-13 A) 1.6e-6 off the oracle and 1e-8
-    # put every current within 5e-16, for 5 % more Krylov iterations (2,106
-    # against 2,005); the full system at 1e-6 was within 1.2e-8.  On the
-    # full system 1e-3 had put the 201x101 diode's currents 4.5e-6 off.
-    polish_eta: float = 1e-8
+    # follows the forcing rule).  Measured over the fixture sweeps with the
+    # floor-free polishing scale below: every current within 1.3e-8 of the
+    # reference's in 14-24 % fewer Krylov iterations than 1e-10, except
+    # currents that the last bits of the state decide (the 48x24x12 p-i-n at
+    # 0.5 V, 1.2e-13 A: 1.2e-8 to 1.9e-6 off across the Krylov systems and
+    # polishing tolerances, each state within rounding of the oracle's); on
+    # the full system 1e-3 put the 201x101 diode's currents 4.5e-6 off.
+    polish_eta: float = 1e-6
     # GPU-only: density floor of the relative Krylov unknowns in the
     # polishing steps (0: krylov_scale_floor).  The polishing steps run with
     # no floor to speak of, so minority densities below the 1e-10 floor of

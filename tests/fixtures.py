@@ -216,3 +216,37 @@ def field_errs(psi, n, p, psi_ref, n_ref, p_ref):
     return (float(np.abs(dpsi).max()),
             float(np.abs(dpsi - (np.log(n) - np.log(n_ref))).max()),
             float(np.abs(dpsi + (np.log(p) - np.log(p_ref))).max()))
+
+
+def current_noise(dev, contact, rel=4.4e-16, trials=8, seed=0, state=None):
+    """How much of a terminal current the last bits of the state decide: the
+    spread (max - min) of the contact's current over `trials` random
+    relative perturbations of psi, n and p at the rounding level (each value
+    times 1 + rel u, u uniform in [-1, 1]), evaluated by the device's own
+    current sum on perturbed copies (the state is not touched); `state`: a
+    (psi, n, p) of host arrays to use instead of the device's own.  At
+    low-current points the current is a difference of contact fluxes many
+    decades larger, so two solvers whose states agree to the last bits can
+    still report currents this far apart (the 41x11 diode at 0.07 V: states
+    within 4e-15, currents 7.7e-4 apart; the oracle's own sum at the GPU
+    state gives the GPU's value)."""
+    import torch
+    pk = dev.pack
+    g = torch.Generator(device=pk.device).manual_seed(seed)
+    scale = dev.J0 * dev.LD ** dev._current_len_exp
+    base = ((pk.psi, pk.n, pk.p) if state is None else
+            [torch.as_tensor(np.asarray(a, float).ravel(), device=pk.device) for a in state])
+    vals = []
+    for _ in range(trials):
+        pert = [t * (1.0 + rel * (2.0 * torch.rand(t.shape, generator=g, device=pk.device,
+                                                   dtype=t.dtype) - 1.0))
+                for t in base]
+        vals.append(float(pk.contact_current(0, contact, *pert).item()) * scale)
+    return max(vals) - min(vals)
+
+
+def current_tol(I_ref, noise, rel=1e-6, floor=0.0):
+    """Tolerance of a current comparison: rel x max(|I_ref|, floor), or ten
+    times the current's rounding-level spread (current_noise) where that is
+    larger."""
+    return max(rel * max(abs(I_ref), floor), 10.0 * noise)

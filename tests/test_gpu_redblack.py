@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import fixtures as fx
-from test_gpu_scale import _check_fields, _rel_err
+from test_gpu_scale import _check_currents, _check_fields
 
 pytestmark = pytest.mark.gpu
 
@@ -158,16 +158,17 @@ def test_pin_downscaled_sweep_red_black():
     dev = W.pin3d(tb.Device3D, *(int(v) for v in g["shape"]))
     opts = tb.NewtonOptions(krylov_system="red_black")
     idx = g["idx"]
-    I = []
+    I, noise = [], []
     with _per_step(dev.pack.lib):
         dev.solve_equilibrium()
         for k, V in enumerate(g["V"]):
             dev.solve_bias({"anode": float(V)}, opts)
             assert dev.last_converged, V
             I.append(dev.terminal_current("anode"))
+            noise.append(fx.current_noise(dev, "anode"))
             st = [t.ravel()[idx] for t in (dev.psi, dev.n, dev.p)]
             _check_fields(dev.VT, st, g["fields"][k], V)
-    assert _rel_err(I, g["I_anode"]) < 1e-6
+    _check_currents(I, g["I_anode"], noise)
 
 
 def test_trigate_downscaled_batch_red_black():
