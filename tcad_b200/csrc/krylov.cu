@@ -1213,8 +1213,21 @@ struct WorkRb {
   int64_t* node_off;
   int64_t* flat_off;
   int32_t* flat_inst;
+  int32_t* blk;  // compact list of the slot pack's flat blocks still iterating
   size_t bytes;
 };
+
+// Slot-pack flat blocks hold half as many slots as the pack's blocks hold
+// nodes (a slot is half a node pair's work), so the passes keep the pack's
+// block count: with 512-slot blocks the 983k-node tri-gate's passes ran 2.2
+// waves of 960 blocks at 3 CTAs per SM.  The count is bounded by
+// slots / rb_flat + n_inst <= n_nodes / rb_flat + n_inst.
+static int64_t rb_flat(const tcad_pack_t* pk) {
+  return pk->flat_nodes > 1 ? pk->flat_nodes / 2 : 1;
+}
+static size_t rb_flat_cap(const tcad_pack_t* pk) {
+  return (size_t)(pk->n_nodes / rb_flat(pk)) + (size_t)pk->n_inst + 1;
+}
 
 static WorkRb carve_rb(const tcad_pack_t* pk, void* base) {
   Carve c{reinterpret_cast<char*>(base), 0, 0};
@@ -1232,7 +1245,8 @@ static WorkRb carve_rb(const tcad_pack_t* pk, void* base) {
   w.shape = c.take<int32_t>(3 * (size_t)pk->n_inst);
   w.node_off = c.take<int64_t>((size_t)pk->n_inst + 1);
   w.flat_off = c.take<int64_t>((size_t)pk->n_inst + 1);
-  w.flat_inst = c.take<int32_t>((size_t)pk->n_flat);
+  w.flat_inst = c.take<int32_t>(rb_flat_cap(pk));
+  w.blk = c.take<int32_t>(rb_flat_cap(pk));
   w.bytes = c.used;
   return w;
 }
@@ -1253,7 +1267,7 @@ static int rb_layout(const tcad_pack_t* pk, const WorkRb& wr, RbLayout& L, cudaS
   TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
   std::vector<int64_t> noff(ni + 1), foff(ni + 1);
   noff[0] = 0; foff[0] = 0;
-  const int64_t fn = pk->flat_nodes;
+  const int64_t fn = rb_flat(pk);
   for (int i = 0; i < ni; ++i) {
     const int64_t hx = (shp[3 * i] + 1) / 2, rows = (int64_t)shp[3 * i + 1] * shp[3 * i + 2];
     sb[3 * i] = (int32_t)hx; sb[3 * i + 1] = (int32_t)rows; sb[3 * i + 2] = 1;
@@ -1262,7 +1276,11 @@ static int rb_layout(const tcad_pack_t* pk, const WorkRb& wr, RbLayout& L, cudaS
     foff[i + 1] = foff[i] + nf;
     for (int64_t b = 0; b < nf; ++b) fi.push_back(i);
   }
-  if (noff[ni] > pk->n_nodes || foff[ni] > pk->n_flat) return TCAD_ERR_ARG;
+  // (the Krylov partials hold 8 n_flat doubles: 4 per slot block fit, as
+  // n_flat >= max(n_inst, n_nodes / flat_nodes))
+  if (noff[ni] > pk->n_nodes || (size_t)foff[ni] > rb_flat_cap(pk) ||
+      4 * foff[ni] > 8 * pk->n_flat)
+    return TCAD_ERR_ARG;
   TCAD_CUDA_CHECK(cudaMemcpyAsync(wr.shape, sb.data(), sizeof(int32_t) * sb.size(),
                                   cudaMemcpyHostToDevice, s));
   TCAD_CUDA_CHECK(cudaMemcpyAsync(wr.node_off, noff.data(), sizeof(int64_t) * noff.size(),
@@ -1279,6 +1297,7 @@ static int rb_layout(const tcad_pack_t* pk, const WorkRb& wr, RbLayout& L, cudaS
   L.pkb.node_off = wr.node_off;
   L.pkb.flat_off = wr.flat_off;
   L.pkb.flat_inst = wr.flat_inst;
+  L.pkb.flat_nodes = (int32_t)fn;
   L.mp.shape = pk->shape;
   L.mp.node_off = pk->node_off;
   L.mp.n_full = pk->n_nodes;
@@ -1631,7 +1650,7 @@ static int launch_bicgstab_rb(const tcad_pack_t* pk, const RbLayout& L, const Wo
     bool any = false;
     for (int i = 0; i < ni; ++i) any = any || hks[i].active;
     if (any)
-      if (int rc = grid.update(hks, w.blk, s)) return rc;
+      if (int rc = grid.update(hks, wr.blk, s)) return rc;
     if (!any) {
       // true Schur residual (= the full residual); re-arm drifted instances
       const int rearm = rechecks < 8 ? 1 : 0;
@@ -1653,7 +1672,7 @@ static int launch_bicgstab_rb(const tcad_pack_t* pk, const RbLayout& L, const Wo
       for (int i = 0; i < ni; ++i) any = any || hks[i].active;
       ++rechecks;
       if (!any) break;
-      if (int rc = grid.update(hks, w.blk, s)) return rc;
+      if (int rc = grid.update(hks, wr.blk, s)) return rc;
     }
     if (done_iters > 64) check = 16;
     if (done_iters > 1024) check = 32;
