@@ -135,6 +135,10 @@ def parse():
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--asm-stage", type=int, default=0, choices=(0, 1),
                     help="--kernels: the 3D assembly's plane staging (pack asm_stage)")
+    ap.add_argument("--no-fused", action="store_true",
+                    help="solve single-instance packs one launch per Krylov step (the "
+                         "red-black Schur loop for FP64 block-Jacobi solves) instead of "
+                         "the one-launch BiCGStab")
     ap.add_argument("--kernels", action="store_true",
                     help="profiling mode: assembly, block-Jacobi set-up and 20 BiCGStab "
                          "iterations on the full-size workload at its bulk-guess state")
@@ -524,6 +528,7 @@ def run_ours(args):
                       "fp32op": "f64 (FP32 operator copy)"}.get(args.method, "f64"),
             "data": "synthetic device (analytic doping profiles, explicit mesh)",
             "config": {"workload": chosen.desc, "method": method_desc,
+                       "single_launch_bicgstab": not args.no_fused,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (J alone is "
                              f"{8 * _lib.NE[dim] * N / 1e6:.0f} MB)"},
@@ -1149,6 +1154,9 @@ def run_kernels(args):
 
 def main():
     args = parse()
+    if args.no_fused and args.impl != "reference":
+        from tcad_b200 import _lib
+        _lib.load().tcad_set_krylov_fused(0)
     if args.kernels:
         run_kernels(args)
         return
