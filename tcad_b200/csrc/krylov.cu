@@ -1217,14 +1217,12 @@ struct WorkRb {
   size_t bytes;
 };
 
-// Slot-pack flat blocks hold half as many slots as the pack's blocks hold
-// nodes (a slot is half a node pair's work), so the passes keep the pack's
-// block count: with 512-slot blocks the 983k-node tri-gate's passes ran 2.2
-// waves of 960 blocks at 3 CTAs per SM.  The count is bounded by
-// slots / rb_flat + n_inst <= n_nodes / rb_flat + n_inst.
-static int64_t rb_flat(const tcad_pack_t* pk) {
-  return pk->flat_nodes > 1 ? pk->flat_nodes / 2 : 1;
-}
+// Slot-pack flat blocks hold pk->flat_nodes slots (measured, 200-iteration
+// solves on the two-lane 983k-node tri-gate: 419 us per iteration at 512
+// slots and 5 CTAs per SM, 450 at 256 slots, 511 at 256 slots and 4 CTAs,
+// 774 at 128).  The count is bounded by slots / rb_flat + n_inst <=
+// n_nodes / rb_flat + n_inst.
+static int64_t rb_flat(const tcad_pack_t* pk) { return pk->flat_nodes; }
 static size_t rb_flat_cap(const tcad_pack_t* pk) {
   return (size_t)(pk->n_nodes / rb_flat(pk)) + (size_t)pk->n_inst + 1;
 }

@@ -62,9 +62,10 @@ struct RbNode {
 // Index arithmetic is 32-bit and instance-local (an instance has far fewer
 // than 2^31 slots): 64-bit division is a long instruction sequence and its
 // registers halved the occupancy of the passes.  The passes that run every
-// iteration fit 64 registers (4 CTAs per SM): under ncu the 3-CTA black pass
-// was latency-bound, 33 long-scoreboard stalls per issue at 34 % warps
-// active, DRAM 33 % busy.
+// iteration are held to 5 CTAs per SM (51 registers; the black passes spill
+// 44 bytes): they are latency-bound -- under ncu the 3-CTA black pass waited
+// 33 long-scoreboard stalls per issue at 34 % warps active, DRAM 33 % busy
+// -- and a whole iteration went from 511 us at 4 CTAs to 419 at 5.
 __device__ __forceinline__ RbNode rb_node(const RbGeo& g, int64_t slot, int colour) {
   RbNode q;
   const unsigned local = (unsigned)(slot - g.soff);
@@ -177,7 +178,7 @@ k_rb_split(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ b,
 // red pass: Tr = E x (the red rows' coupling to black values x); every
 // instance when ks is null, else only those still iterating
 template <int DIM>
-__global__ void __launch_bounds__(NT, 4)
+__global__ void __launch_bounds__(NT, 5)
 k_rb_red(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JR,
          const double* __restrict__ x, double* __restrict__ Tr, const KState* ks,
          const int32_t* __restrict__ blk) {
@@ -260,7 +261,7 @@ k_rb_init(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
 
 // v = S p (S = I - F E; Tr = E p from the red pass); (rh, v)
 template <int DIM>
-__global__ void __launch_bounds__(NT, 4)
+__global__ void __launch_bounds__(NT, 5)
 k_rb_v(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
        const double* __restrict__ Tr, BiVec w, KState* ks, double* partial, unsigned* ticket,
        const int32_t* __restrict__ blk) {
@@ -287,7 +288,7 @@ k_rb_v(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
 
 // t = S s (Tr = E s); (t, s), (t, t)
 template <int DIM>
-__global__ void __launch_bounds__(NT, 4)
+__global__ void __launch_bounds__(NT, 5)
 k_rb_t(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
        const double* __restrict__ Tr, BiVec w, KState* ks, double* partial, unsigned* ticket,
        const int32_t* __restrict__ blk) {
