@@ -3,7 +3,7 @@
 // All kernels are "flat": block b owns pk.flat_nodes consecutive nodes of
 // one instance (flat_block()).  Reductions are per instance and
 // deterministic: each block writes its partial sums, and the LAST block of
-// the instance to finish (atomic tickets, two levels) sums them in a fixed order and
+// the instance to finish (atomic ticket) sums the partials in block order and
 // updates the instance's scalar state (alpha, omega, ...).  The host only
 // looks at the per-instance state every few iterations, so the iteration
 // itself runs without host round trips; blocks of finished instances return
@@ -46,133 +46,53 @@ __device__ __forceinline__ void nbr_offsets(const Inst& g, int64_t* off) {
 }
 
 // --------------------------------------------------------------------------
-// partial sums -> per-instance totals, in a fixed order (deterministic).
-// store(): this block's sums into partial[b * 4 + q].  The instance's blocks
-// form groups of kRedGroup consecutive blocks; a group's sum is the lane-order
-// warp tree of its block partials (group_sum), and the instance total is the
-// warp tree of lane sums, lane l adding groups l, l + 32, ... in order
-// (groups_total).  run(): the LAST block of each group (atomic ticket in the
-// group's slot of the second half of `partial`) stores the group sum there,
-// and the last group of the instance (ticket[inst]) forms the total -- two
-// short serial steps on one warp each, instead of one block summing every
-// block partial of the instance at the kernel's tail.  total(): the same
-// total computed by every CTA of the single-launch solve (its instance has
-// at most kFusedGroups groups).  run() needs the group tickets zero: the
-// solve launchers clear `partial` before a solve.
-constexpr int kRedGroup = 32;
-constexpr int kFusedGroups = 16;
-
-__device__ __forceinline__ double warp_tree(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// sum of the partials q of blocks [g0, g0 + cnt), cnt <= 32: one full warp
-// (every lane returns it)
-__device__ __forceinline__ double group_sum(const double* partial, int64_t g0, int cnt, int q) {
-  const int lane = threadIdx.x & 31;
-  const double v = lane < cnt ? __ldcg(&partial[(g0 + lane) * 4 + q]) : 0.0;
-  return warp_tree(v);
-}
-
+// partial sums -> per-instance totals.  store(): this block's sums into
+// partial[b * 4 + q]; total(): the instance's block partials summed in block
+// order (valid in thread 0).  run(): both, the total taken by the LAST block
+// of the instance to finish (atomic ticket); true in every thread of that
+// block.
 template <int NS>
 struct Reduce {
   __device__ static void store(int64_t b, double (&v)[NS], double* partial) {
-    __shared__ double sm[NS][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ double sm[32];
+    __shared__ double st[NS];
 #pragma unroll
     for (int q = 0; q < NS; ++q) {
-      double x = v[q];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-      if (lane == 0) sm[q][warp] = x;
+      const double r = block_sum<NT>(v[q], sm);
+      if (threadIdx.x == 0) st[q] = r;
     }
-    __syncthreads();
-    if (warp == 0) {
+    if (threadIdx.x == 0) {
 #pragma unroll
-      for (int q = 0; q < NS; ++q) {
-        double r = lane < NT / 32 ? sm[q][lane] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
-        if (lane == 0) partial[b * 4 + q] = r;
-      }
+      for (int q = 0; q < NS; ++q) partial[b * 4 + q] = st[q];
     }
-    __syncthreads();
   }
-  // every CTA: the instance's total into tot (valid in thread 0); at most
-  // kFusedGroups groups
   __device__ static void total(const tcad_pack_t& pk, int inst, const double* partial,
                                double* tot) {
-    __shared__ double gs[NS][kFusedGroups];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t b0 = pk.flat_off[inst], nb = pk.flat_off[inst + 1] - b0;
-    const int ng = (int)((nb + kRedGroup - 1) / kRedGroup);
-    for (int j = warp; j < ng; j += NT / 32) {
-      const int cnt = (int)min((int64_t)kRedGroup, nb - (int64_t)j * kRedGroup);
+    __shared__ double sm[32];
+    const int64_t b0 = pk.flat_off[inst], b1 = pk.flat_off[inst + 1];
 #pragma unroll
-      for (int q = 0; q < NS; ++q) {
-        const double g = group_sum(partial, b0 + (int64_t)j * kRedGroup, cnt, q);
-        if (lane == 0) gs[q][j] = g;
-      }
+    for (int q = 0; q < NS; ++q) {
+      double s = 0.0;
+      for (int64_t bb = b0 + threadIdx.x; bb < b1; bb += NT) s += __ldcg(&partial[bb * 4 + q]);
+      const double r = block_sum<NT>(s, sm);
+      if (threadIdx.x == 0) tot[q] = r;
     }
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-      for (int q = 0; q < NS; ++q) {
-        double x = 0.0;
-        for (int j = lane; j < ng; j += 32) x += gs[q][j];
-        x = warp_tree(x);
-        if (lane == 0) tot[q] = x;
-      }
-    }
-    __syncthreads();
   }
   __device__ static bool run(const tcad_pack_t& pk, int64_t b, int inst, double (&v)[NS],
                              double* partial, unsigned* ticket, double* tot) {
     __shared__ int last;
     store(b, v, partial);
-    const int64_t b0 = pk.flat_off[inst], nb = pk.flat_off[inst + 1] - b0;
-    const int64_t gi = (b - b0) / kRedGroup;
-    const int64_t gfirst = b0 + gi * kRedGroup;
-    const int cnt = (int)min((int64_t)kRedGroup, nb - gi * kRedGroup);
-    double* gpart = partial + 4 * pk.n_flat;
-    unsigned* gtick = reinterpret_cast<unsigned*>(&gpart[gfirst * 4 + 3]);
     if (threadIdx.x == 0) {
       __threadfence();
-      last = atomicAdd(gtick, 1u) == (unsigned)(cnt - 1);
+      const int64_t nb = pk.flat_off[inst + 1] - pk.flat_off[inst];
+      const unsigned prev = atomicAdd(&ticket[inst], 1u);
+      last = (prev == (unsigned)(nb - 1));
     }
     __syncthreads();
     if (!last) return false;
-    const int ng = (int)((nb + kRedGroup - 1) / kRedGroup);
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      __threadfence();
-#pragma unroll
-      for (int q = 0; q < NS; ++q) {
-        const double g = group_sum(partial, gfirst, cnt, q);
-        if (threadIdx.x == 0) gpart[gfirst * 4 + q] = g;
-      }
-      if (threadIdx.x == 0) {
-        *gtick = 0u;
-        __threadfence();
-        last = atomicAdd(&ticket[inst], 1u) == (unsigned)(ng - 1);
-      }
-    }
-    __syncthreads();
-    if (!last) return false;
-    if (threadIdx.x < 32) {
-      __threadfence();
-#pragma unroll
-      for (int q = 0; q < NS; ++q) {
-        double x = 0.0;
-        for (int j = threadIdx.x; j < ng; j += 32)
-          x += __ldcg(&gpart[(b0 + (int64_t)j * kRedGroup) * 4 + q]);
-        x = warp_tree(x);
-        if (threadIdx.x == 0) tot[q] = x;
-      }
-      if (threadIdx.x == 0) ticket[inst] = 0u;
-    }
+    __threadfence();
+    total(pk, inst, partial, tot);
+    if (threadIdx.x == 0) ticket[inst] = 0u;
     return true;
   }
 };
@@ -1454,8 +1374,7 @@ static bool fused_fits(unsigned nb) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bicgstab_fused<DIM>, NT, 0) !=
       cudaSuccess)
     return false;
-  return nb >= 1 && (long long)nb <= (long long)per * sms &&
-         nb <= (unsigned)(kFusedGroups * kRedGroup);   // Reduce::total's group bound
+  return nb >= 1 && (long long)nb <= (long long)per * sms;
 }
 
 // The whole solve of a single-instance pack in one launch (same arithmetic
@@ -1583,7 +1502,6 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const TJ* J, const T* b, T* 
       return TCAD_OK;
   }
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
-  TCAD_CUDA_CHECK(cudaMemsetAsync(w.partial, 0, 8 * sizeof(double) * (size_t)pk->n_flat, s));
   k_bi_init<<<nb, NT, 0, s>>>(*pk, b, x, bi, w.ks, w.partial, w.ticket, rtol, maxiter,
                               pre_status, rtol_inst);
   note_launch();
@@ -1678,7 +1596,6 @@ static int launch_bicgstab_rb(const tcad_pack_t* pk, const RbLayout& L, const Wo
   bi.ph = bi.p;
   bi.sh = bi.s;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
-  TCAD_CUDA_CHECK(cudaMemsetAsync(w.partial, 0, 8 * sizeof(double) * (size_t)pk->n_flat, s));
   if (d2) k_rb_split<2><<<nbb, NT, 0, s>>>(pkb, L.mp, b, wr.bR, wr.bB, wr.bbf, w.partial, w.ticket);
   else    k_rb_split<3><<<nbb, NT, 0, s>>>(pkb, L.mp, b, wr.bR, wr.bB, wr.bbf, w.partial, w.ticket);
   note_launch();
@@ -1799,7 +1716,6 @@ static int solve_mixed(const tcad_pack_t* pk, const double* J, const double* b, 
   k_to_f32<<<fl ? nfl : nb, NT, 0, s>>>(*pk, ne, J, w32.J32, fl);
   note_launch();
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
-  TCAD_CUDA_CHECK(cudaMemsetAsync(w.partial, 0, 8 * sizeof(double) * (size_t)pk->n_flat, s));
   k_ir_init<<<nb, NT, 0, s>>>(*pk, b, x, w32.irs, w.partial, w.ticket);
   note_launch();
   TCAD_LAUNCH_CHECK();
@@ -1867,7 +1783,6 @@ static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, do
   const unsigned nb = (unsigned)pk->n_flat;
   const int ni = pk->n_inst;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
-  TCAD_CUDA_CHECK(cudaMemsetAsync(w.partial, 0, 8 * sizeof(double) * (size_t)pk->n_flat, s));
   k_cg_init<<<nb, NT, 0, s>>>(*pk, J, b, x, w.cg, w.ks, w.partial, w.ticket, rtol, maxiter,
                               active, rtol_inst);
   note_launch();
@@ -2587,7 +2502,6 @@ extern "C" int tcad_block_krylov_noalloc(const tcad_pack_t* pk, const double* J,
   const int ni = pk->n_inst;
   KState hks[TCAD_STATIC_MAX_INST];  // host mirror on the stack, no heap
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
-  TCAD_CUDA_CHECK(cudaMemsetAsync(w.partial, 0, 8 * sizeof(double) * (size_t)pk->n_flat, s));
   k_bi_init<<<nb, NT, 0, s>>>(*pk, b, x, w.bi, w.ks, w.partial, w.ticket, rtol, maxiter,
                               nullptr, nullptr);
   note_launch();
