@@ -1232,8 +1232,8 @@ static WorkRb carve_rb(const tcad_pack_t* pk, void* base) {
   WorkRb w;
   const size_t nn = (size_t)pk->n_nodes, v3 = 3 * nn;
   const size_t ne = pk->dim == 2 ? TCAD_NE2 : TCAD_NE3;
-  w.JR = c.take<double>(ne * nn);
-  w.JB = c.take<double>(ne * nn);
+  w.JR = c.take<double>(ne * (nn + 32));   // warp tiles of 32 slots
+  w.JB = c.take<double>(ne * (nn + 32));
   w.bR = c.take<double>(v3);
   w.bB = c.take<double>(v3);
   w.tR = c.take<double>(v3);

@@ -99,7 +99,17 @@ __device__ __forceinline__ void rb_nbrs(const RbGeo& g, const RbNode& q, int sel
   }
 }
 
-// y = D (sum_d A_d x_m(d)) at one slot of a colour array Jc ([NE][NS]; the
+// Colour rows of J are stored in warp tiles: the NE entries of 32
+// consecutive slots are one contiguous run of NE x 32 doubles (entry e of
+// slot s at ((s / 32) NE + e) 32 + s % 32), so a warp's loads of a slot row
+// stay inside one 10 KB (3D) span instead of touching NE arrays a whole
+// colour apart.
+template <int NE>
+__device__ __forceinline__ int64_t rb_jidx(int e, int64_t slot) {
+  return (((slot >> 5) * NE + e) << 5) + (slot & 31);
+}
+
+// y = D (sum_d A_d x_m(d)) at one slot of a colour array Jc (warp tiles; the
 // set-up's D^-1 in entries 0..8, the raw neighbour entries after them): the
 // coupling part of A^ on the other colour's values; xi = that colour's
 // vector from the instance's first slot, m instance-local
@@ -108,24 +118,27 @@ __device__ __forceinline__ void rb_couple(const double* __restrict__ Jc,
                                           const double* __restrict__ xi, int64_t slot,
                                           int64_t NS, const int* m, double& y0, double& y1,
                                           double& y2) {
+  constexpr int NE = Stencil<DIM>::NE;
+  const double* __restrict__ Jt = Jc + rb_jidx<NE>(0, slot);   // entry e at Jt[32 e]
   double t0 = 0.0, t1 = 0.0, t2 = 0.0;
 #pragma unroll
   for (int d = 0; d < 2 * DIM; ++d) {
     const int e = 9 + 5 * d;
     const double xs = xi[m[d]], xn = xi[NS + m[d]], xp = xi[2 * NS + m[d]];
-    t0 += Jc[(int64_t)e * NS + slot] * xs;
-    t1 += Jc[(int64_t)(e + 1) * NS + slot] * xs + Jc[(int64_t)(e + 2) * NS + slot] * xn;
-    t2 += Jc[(int64_t)(e + 3) * NS + slot] * xs + Jc[(int64_t)(e + 4) * NS + slot] * xp;
+    t0 += Jt[32 * e] * xs;
+    t1 += Jt[32 * (e + 1)] * xs + Jt[32 * (e + 2)] * xn;
+    t2 += Jt[32 * (e + 3)] * xs + Jt[32 * (e + 4)] * xp;
   }
   double d[9];
 #pragma unroll
-  for (int e = 0; e < 9; ++e) d[e] = Jc[(int64_t)e * NS + slot];
+  for (int e = 0; e < 9; ++e) d[e] = Jt[32 * e];
   y0 = d[0] * t0 + d[1] * t1 + d[2] * t2;
   y1 = d[3] * t0 + d[4] * t1 + d[5] * t2;
   y2 = d[6] * t0 + d[7] * t1 + d[8] * t2;
 }
 
-// JR, JB <- the red and black rows of the block-scaled J (zeros at pads)
+// JR, JB <- the red and black rows of the block-scaled J in warp tiles
+// (zeros at pads; the tile tail past the last slot is never read)
 template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_rb_pack(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ J,
@@ -141,7 +154,7 @@ k_rb_pack(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ J,
       double* __restrict__ out = c ? JB : JR;
 #pragma unroll 13
       for (int e = 0; e < NE; ++e)
-        out[(int64_t)e * NS + slot] = q.real ? J[(int64_t)e * NN + q.node] : 0.0;
+        out[rb_jidx<NE>(e, slot)] = q.real ? J[(int64_t)e * NN + q.node] : 0.0;
     }
   }
 }
