@@ -383,9 +383,10 @@ typedef struct tcad_newton_opts {
    * no coupling inside a colour of (i + j + k) & 1, so the red unknowns are
    * eliminated exactly: half the unknowns, the same matrix bytes per
    * product, about half the iterations); the stopping test stays the full
-   * system's ||b - A x|| <= eta ||b||.  Single-instance packs small enough
-   * for the one-launch solve keep it; ILU(0) solves and FP32 operators keep
-   * the full system.  0: the full system always. */
+   * system's ||b - A x|| <= eta ||b||.  A single-instance pack whose slot
+   * blocks fit on the GPU at once is solved in one cooperative launch (the
+   * same arithmetic).  ILU(0) solves and FP32 operators keep the full
+   * system.  0: the full system always. */
   int32_t red_black;
   int32_t reserved_opts;  /* 0 */
 } tcad_newton_opts_t;

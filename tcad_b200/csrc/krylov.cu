@@ -816,6 +816,115 @@ k_bicgstab_fused(const tcad_pack_t pk, const double* __restrict__ J,
   if (blockIdx.x == 0 && threadIdx.x == 0) ks[inst] = S;
 }
 
+// ---- the red-black Schur solve in one cooperative launch (single-instance
+// packs whose slot blocks all fit on the GPU at once: one CTA per slot
+// block).  The search direction and s are formed on the fly by the red
+// passes (RbFormP / RbFormS) and stored by the black passes, so an iteration
+// takes five grid barriers: red(p); p + v (alpha); red(s); s + t (early,
+// omega); x (rho, beta, convergence).  Bodies, scalar updates and reduction
+// order are the per-step kernels' own, so the result is bit-identical to
+// launch_bicgstab_rb's one launch per step.  Every wait is bounded as in
+// k_bicgstab_fused; a CTA that gives up returns and the host solves again
+// one launch per step.
+template <int DIM>
+__global__ void __launch_bounds__(NT, 2)
+k_bicgstab_rb_fused(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JR,
+                    const double* __restrict__ JB, const double* __restrict__ b,
+                    double* __restrict__ x, double* __restrict__ bR, double* __restrict__ bB,
+                    double* __restrict__ Tr, double* __restrict__ xb,
+                    double* __restrict__ rhs, BiVec w, KState* ks, double* partial,
+                    unsigned* bar, double rtol, int maxit,
+                    const int32_t* __restrict__ pre_status,
+                    const double* __restrict__ rtol_inst, int max_rechecks) {
+  __shared__ KState S;
+  const unsigned G = gridDim.x;
+  const FlatBlock fb = flat_block(pkb, blockIdx.x);
+  const int inst = fb.inst;
+  const int64_t NS = pkb.n_nodes;
+  double* const half[2] = {partial, partial + 4 * (int64_t)pkb.n_flat};
+  int ph = 0;
+  unsigned round = 0;
+  double tot[3];
+  double bb = 0.0;
+  {
+    double v[1] = {rb_split_body<DIM>(pkb, mp, fb, b, bR, bB)};
+    Reduce<1>::store(blockIdx.x, v, half[ph]);
+    if (!grid_barrier(bar, G, round)) return;
+    Reduce<1>::total(pkb, inst, half[ph], tot);
+    ph ^= 1;
+    bb = tot[0];
+  }
+  {
+    double v[1] = {rb_init_body<DIM>(pkb, mp, fb, JB, bR, bB, rhs, xb, w)};
+    Reduce<1>::store(blockIdx.x, v, half[ph]);
+    if (!grid_barrier(bar, G, round)) return;
+    Reduce<1>::total(pkb, inst, half[ph], tot);
+    ph ^= 1;
+    if (threadIdx.x == 0)
+      rb_fin_init(S, tot[0], bb, rtol_inst ? rtol_inst[inst] : rtol, maxit,
+                  pre_status ? pre_status[inst] : TCAD_OK);
+    __syncthreads();
+  }
+  for (int rechecks = 0;; ++rechecks) {
+    while (S.active) {
+      rb_red_body<DIM>(pkb, mp, fb, JR,
+                       RbMakeP{w.r, w.p, w.v, NS, S.beta, S.omega, S.restart}, Tr);
+      if (!grid_barrier(bar, G, round)) return;
+      {
+        double v[1] = {rb_v_body<DIM, true>(pkb, mp, fb, JB, Tr, w, S.beta, S.omega,
+                                            S.restart)};
+        Reduce<1>::store(blockIdx.x, v, half[ph]);
+        if (!grid_barrier(bar, G, round)) return;
+        Reduce<1>::total(pkb, inst, half[ph], tot);
+        ph ^= 1;
+        if (threadIdx.x == 0) fin_v(S, tot[0]);
+        __syncthreads();
+      }
+      if (!S.active) break;
+      rb_red_body<DIM>(pkb, mp, fb, JR, RbMakeS{w.r, w.v, NS, S.alpha}, Tr);
+      if (!grid_barrier(bar, G, round)) return;
+      {
+        double v[3];
+        rb_t_body<DIM, true>(pkb, mp, fb, JB, Tr, w, S.alpha, v);
+        Reduce<3>::store(blockIdx.x, v, half[ph]);
+        if (!grid_barrier(bar, G, round)) return;
+        Reduce<3>::total(pkb, inst, half[ph], tot);
+        ph ^= 1;
+        if (threadIdx.x == 0) {
+          fin_s(S, tot[0]);
+          fin_t(S, tot[1], tot[2]);
+        }
+        __syncthreads();
+      }
+      {
+        double v[3];
+        bi_x_body<double>(pkb, fb, xb, w, S.alpha, S.omega, v);
+        Reduce<3>::store(blockIdx.x, v, half[ph]);
+        if (!grid_barrier(bar, G, round)) return;
+        Reduce<3>::total(pkb, inst, half[ph], tot);
+        ph ^= 1;
+        if (threadIdx.x == 0) fin_x(S, tot[0], tot[1], tot[2]);
+        __syncthreads();
+      }
+    }
+    rb_red_body<DIM>(pkb, mp, fb, JR, RbMakeVal{xb, NS}, Tr);
+    if (!grid_barrier(bar, G, round)) return;
+    {
+      double v[1] = {rb_true_body<DIM>(pkb, mp, fb, JB, Tr, rhs, xb, w.r)};
+      Reduce<1>::store(blockIdx.x, v, half[ph]);
+      if (!grid_barrier(bar, G, round)) return;
+      Reduce<1>::total(pkb, inst, half[ph], tot);
+      ph ^= 1;
+      if (threadIdx.x == 0) fin_true(S, tot[0], rechecks < max_rechecks ? 1 : 0);
+      __syncthreads();
+    }
+    if (!S.active) break;
+  }
+  rb_merge_body<DIM>(pkb, mp, fb, bR, Tr, xb, x,
+                     pre_status && pre_status[inst] != TCAD_OK);
+  if (blockIdx.x == 0 && threadIdx.x == 0) ks[inst] = S;
+}
+
 // --------------------------------------------------------------------------
 // Newton update (device2d.py:2079-2100): per-instance max update into err
 __global__ void __launch_bounds__(NT)
@@ -1578,6 +1687,73 @@ static int launch_bicgstab_t(const tcad_pack_t* pk, const TJ* J, const T* b, T* 
   return TCAD_OK;
 }
 
+template <int DIM>
+static bool rb_fused_fits(unsigned nb) {
+  int dev = 0, coop = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+    return false;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return false;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bicgstab_rb_fused<DIM>, NT, 0) !=
+      cudaSuccess)
+    return false;
+  return nb >= 1 && (long long)nb <= (long long)per * sms;
+}
+
+// The whole red-black solve of a single-instance pack in one launch (same
+// arithmetic as launch_bicgstab_rb's per-step loop).  Returns TCAD_OK with
+// hks[0] filled, or 1 when the launch was refused or a grid barrier gave up
+// (the caller then solves one launch per step).
+static int launch_bicgstab_rb_fused(const tcad_pack_t* pk, const RbLayout& L,
+                                    const WorkRb& wr, const double* b, double* x,
+                                    double rtol, int maxiter, const BiVec& bi, const Work& w,
+                                    const int32_t* pre_status, std::vector<KState>& hks,
+                                    cudaStream_t s, const double* rtol_inst) {
+  TCAD_CUDA_CHECK(cudaMemsetAsync(w.bar, 0, 4 * sizeof(unsigned), s));
+  if (g_fused_test_hold.load()) {
+    static const unsigned kPhantom = 1u;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(w.bar + 3, &kPhantom, sizeof(unsigned),
+                                    cudaMemcpyHostToDevice, s));
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)L.pkb.n_flat);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const int rechecks = 8;
+  cudaError_t e =
+      pk->dim == 2
+          ? cudaLaunchKernelEx(&cfg, k_bicgstab_rb_fused<2>, L.pkb, L.mp, (const double*)wr.JR,
+                               (const double*)wr.JB, b, x, wr.bR, wr.bB, wr.tR, wr.xb, wr.rhs,
+                               bi, w.ks, w.partial, w.bar, rtol, maxiter, pre_status,
+                               rtol_inst, rechecks)
+          : cudaLaunchKernelEx(&cfg, k_bicgstab_rb_fused<3>, L.pkb, L.mp, (const double*)wr.JR,
+                               (const double*)wr.JB, b, x, wr.bR, wr.bB, wr.tR, wr.xb, wr.rhs,
+                               bi, w.ks, w.partial, w.bar, rtol, maxiter, pre_status,
+                               rtol_inst, rechecks);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 1;
+  }
+  note_launch();
+  hks.resize(1);
+  unsigned hbar[4] = {0u, 0u, 0u, 0u};
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState), cudaMemcpyDeviceToHost, s));
+  TCAD_CUDA_CHECK(cudaMemcpyAsync(hbar, w.bar, sizeof(hbar), cudaMemcpyDeviceToHost, s));
+  TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (hbar[2] != 0u) {
+    g_fused_gave_up.fetch_add(1);
+    return 1;
+  }
+  return TCAD_OK;
+}
+
 // BiCGStab on the red-black Schur complement of A^ (redblack.cuh): the same
 // per-instance stopping test ||b - A^ x|| <= rtol ||b|| as launch_bicgstab_t,
 // the same vector kernels on the black slot pack, and the full solution x
@@ -1595,6 +1771,11 @@ static int launch_bicgstab_rb(const tcad_pack_t* pk, const RbLayout& L, const Wo
   BiVec bi = w.bi;   // black vectors (stride: the slot count)
   bi.ph = bi.p;
   bi.sh = bi.s;
+  if (g_fused_mode.load() && ni == 1 &&
+      (d2 ? rb_fused_fits<2>(nbb) : rb_fused_fits<3>(nbb)) &&
+      launch_bicgstab_rb_fused(pk, L, wr, b, x, rtol, maxiter, bi, w, pre_status, hks, s,
+                               rtol_inst) == TCAD_OK)
+    return TCAD_OK;
   TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
   if (d2) k_rb_split<2><<<nbb, NT, 0, s>>>(pkb, L.mp, b, wr.bR, wr.bB, wr.bbf, w.partial, w.ticket);
   else    k_rb_split<3><<<nbb, NT, 0, s>>>(pkb, L.mp, b, wr.bR, wr.bB, wr.bbf, w.partial, w.ticket);
@@ -2050,12 +2231,10 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
     wilu_use.Mf = nullptr;  // node-order sweeps
     wilu_use.Mb = nullptr;
   }
-  // red-black Schur solves: the slot pack's tables, once per call.  A
-  // single-instance pack that fits the one-launch solve keeps it (that solve
-  // is latency-bound; the Schur loop takes seven launches per iteration).
-  const bool fused_small = g_fused_mode.load() && ni == 1 &&
-                           (pk->dim == 2 ? fused_fits<2>(nb) : fused_fits<3>(nb));
-  const bool use_rb = opts->red_black != 0 && !fused_small;
+  // red-black Schur solves: the slot pack's tables, once per call (a
+  // single-instance pack small enough is solved in one cooperative launch,
+  // k_bicgstab_rb_fused, by launch_bicgstab_rb itself)
+  const bool use_rb = opts->red_black != 0;
   if (use_rb && work_bytes < tcad_block_workspace_bytes(pk, 0, 0)) return TCAD_ERR_ARG;
   WorkRb wrb{};
   RbLayout rbl;

@@ -111,20 +111,18 @@ __device__ __forceinline__ int64_t rb_jidx(int e, int64_t slot) {
 
 // y = D (sum_d A_d x_m(d)) at one slot of a colour array Jc (warp tiles; the
 // set-up's D^-1 in entries 0..8, the raw neighbour entries after them): the
-// coupling part of A^ on the other colour's values; xi = that colour's
-// vector from the instance's first slot, m instance-local
-template <int DIM>
-__device__ __forceinline__ void rb_couple(const double* __restrict__ Jc,
-                                          const double* __restrict__ xi, int64_t slot,
-                                          int64_t NS, const int* m, double& y0, double& y1,
-                                          double& y2) {
+// coupling part of A^ on the other colour's values X(m, c), m instance-local
+template <int DIM, class XF>
+__device__ __forceinline__ void rb_couple_f(const double* __restrict__ Jc, const XF& X,
+                                            int64_t slot, const int* m, double& y0,
+                                            double& y1, double& y2) {
   constexpr int NE = Stencil<DIM>::NE;
   const double* __restrict__ Jt = Jc + rb_jidx<NE>(0, slot);   // entry e at Jt[32 e]
   double t0 = 0.0, t1 = 0.0, t2 = 0.0;
 #pragma unroll
   for (int d = 0; d < 2 * DIM; ++d) {
     const int e = 9 + 5 * d;
-    const double xs = xi[m[d]], xn = xi[NS + m[d]], xp = xi[2 * NS + m[d]];
+    const double xs = X(m[d], 0), xn = X(m[d], 1), xp = X(m[d], 2);
     t0 += Jt[32 * e] * xs;
     t1 += Jt[32 * (e + 1)] * xs + Jt[32 * (e + 2)] * xn;
     t2 += Jt[32 * (e + 3)] * xs + Jt[32 * (e + 4)] * xp;
@@ -137,6 +135,296 @@ __device__ __forceinline__ void rb_couple(const double* __restrict__ Jc,
   y2 = d[6] * t0 + d[7] * t1 + d[8] * t2;
 }
 
+// a stored vector of the other colour (xi: from the instance's first slot)
+struct RbVal {
+  const double* __restrict__ xi;
+  int64_t NS;
+  __device__ __forceinline__ double operator()(int m, int c) const { return xi[c * NS + m]; }
+};
+
+// The search direction p = r + beta (p - omega v) (p = r on a restart) and
+// s = r - alpha v formed on the fly at the other colour's slots, from vectors
+// no CTA writes meanwhile -- the expressions of bi_p_body and bi_s_body (the
+// single-launch solve forms them where the per-step solve stores them)
+struct RbFormP {
+  const double* __restrict__ r;
+  const double* __restrict__ p;
+  const double* __restrict__ v;
+  int64_t NS;
+  double beta, omega;
+  int restart;
+  __device__ __forceinline__ double operator()(int m, int c) const {
+    const double rv = r[c * NS + m];
+    return restart ? rv : rv + beta * (p[c * NS + m] - omega * v[c * NS + m]);
+  }
+};
+struct RbFormS {
+  const double* __restrict__ r;
+  const double* __restrict__ v;
+  int64_t NS;
+  double alpha;
+  __device__ __forceinline__ double operator()(int m, int c) const {
+    return r[c * NS + m] - alpha * v[c * NS + m];
+  }
+};
+
+template <int DIM>
+__device__ __forceinline__ void rb_couple(const double* __restrict__ Jc,
+                                          const double* __restrict__ xi, int64_t slot,
+                                          int64_t NS, const int* m, double& y0, double& y1,
+                                          double& y2) {
+  rb_couple_f<DIM>(Jc, RbVal{xi, NS}, slot, m, y0, y1, y2);
+}
+
+// ---- per-block bodies, shared by the per-step kernels below and the
+// single-launch solve (k_bicgstab_rb_fused), so both run the same
+// arithmetic in the same order
+
+// bR, bB <- the colours of b at the block's slots; returns the thread's
+// share of (b, b)
+template <int DIM>
+__device__ __forceinline__ double rb_split_body(const tcad_pack_t& pkb, const RbMap& mp,
+                                                const FlatBlock& fb,
+                                                const double* __restrict__ b,
+                                                double* __restrict__ bR,
+                                                double* __restrict__ bB) {
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes, NN = mp.n_full;
+  double v = 0.0;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const RbNode q = rb_node(g, slot, c);
+      double* __restrict__ out = c ? bB : bR;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const double bv = q.real ? b[r * NN + q.node] : 0.0;
+        out[r * NS + slot] = bv;
+        v += bv * bv;
+      }
+    }
+  }
+  return v;
+}
+
+// black pass coupling at one slot: u = F Tr; false at a pad (u = 0).  The
+// callers load the slot's own vectors after it (y = X - u), which keeps them
+// out of the registers the gathers need.
+template <int DIM>
+__device__ __forceinline__ bool rb_black_u(const RbGeo& g, const double* __restrict__ JB,
+                                           const double* __restrict__ Tr, int64_t slot,
+                                           int64_t NS, double* u) {
+  const RbNode q = rb_node(g, slot, 1);
+  u[0] = 0.0; u[1] = 0.0; u[2] = 0.0;
+  if (!q.real) return false;
+  int m[6];
+  rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
+  rb_couple<DIM>(JB, Tr + g.soff, slot, NS, m, u[0], u[1], u[2]);
+  return true;
+}
+
+// rhs = bB - F bR; x = 0, r = rh = rhs, p = v = 0; returns (rhs, rhs) share
+template <int DIM>
+__device__ __forceinline__ double rb_init_body(const tcad_pack_t& pkb, const RbMap& mp,
+                                               const FlatBlock& fb,
+                                               const double* __restrict__ JB,
+                                               const double* __restrict__ bR,
+                                               const double* __restrict__ bB,
+                                               double* __restrict__ rhs,
+                                               double* __restrict__ x, const BiVec& w) {
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  double v = 0.0;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    double u[3];
+    const bool real = rb_black_u<DIM>(g, JB, bR, slot, NS, u);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t q = c * NS + slot;
+      const double y = real ? bB[q] - u[c] : 0.0;
+      rhs[q] = y;
+      x[q] = 0.0; w.r[q] = y; w.rh[q] = y; w.p[q] = 0.0; w.v[q] = 0.0;
+      v += y * y;
+    }
+  }
+  return v;
+}
+
+// red pass: Tr = E X at the block's red slots, X a value functor factory
+// (instance base offset -> functor)
+template <int DIM, class MK>
+__device__ __forceinline__ void rb_red_body(const tcad_pack_t& pkb, const RbMap& mp,
+                                            const FlatBlock& fb,
+                                            const double* __restrict__ JR, const MK& make,
+                                            double* __restrict__ Tr) {
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  const auto X = make(g.soff);
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    const RbNode q = rb_node(g, slot, 0);
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+    if (q.real) {
+      int m[6];
+      rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
+      rb_couple_f<DIM>(JR, X, slot, m, y0, y1, y2);
+    }
+    Tr[slot] = y0; Tr[NS + slot] = y1; Tr[2 * NS + slot] = y2;
+  }
+}
+
+// v = S p (Tr = E p); FORM: p formed and stored first (p = r + beta (p -
+// omega v); restart: rh = p = r), else p as stored; returns (rh, v) share
+template <int DIM, bool FORM>
+__device__ __forceinline__ double rb_v_body(const tcad_pack_t& pkb, const RbMap& mp,
+                                            const FlatBlock& fb,
+                                            const double* __restrict__ JB,
+                                            const double* __restrict__ Tr, const BiVec& w,
+                                            double beta, double omega, int restart) {
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  double* __restrict__ P = w.p;
+  double* __restrict__ RH = w.rh;
+  double* __restrict__ Vo = w.v;
+  const double* __restrict__ R = w.r;
+  double v = 0.0;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    double u[3];
+    const bool real = rb_black_u<DIM>(g, JB, Tr, slot, NS, u);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t i = c * NS + slot;
+      double pn, h;
+      if (FORM) {
+        const double rv = R[i];
+        pn = restart ? rv : rv + beta * (P[i] - omega * Vo[i]);
+        P[i] = pn;
+        if (restart) RH[i] = rv;
+        h = restart ? rv : RH[i];
+      } else {
+        pn = P[i];
+        h = RH[i];
+      }
+      const double y = real ? pn - u[c] : 0.0;
+      Vo[i] = y;
+      v += h * y;
+    }
+  }
+  return v;
+}
+
+// t = S s (Tr = E s); FORM: s = r - alpha v formed and stored first (its
+// (s, s) share in v[0], accumulated as bi_s_body does), else s as stored;
+// v[1] = (t, s), v[2] = (t, t) shares
+template <int DIM, bool FORM>
+__device__ __forceinline__ void rb_t_body(const tcad_pack_t& pkb, const RbMap& mp,
+                                          const FlatBlock& fb, const double* __restrict__ JB,
+                                          const double* __restrict__ Tr, const BiVec& w,
+                                          double alpha, double (&v)[3]) {
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  double* __restrict__ S = w.s;
+  double* __restrict__ To = w.t;
+  const double* __restrict__ R = w.r;
+  const double* __restrict__ V = w.v;
+  v[0] = 0.0; v[1] = 0.0; v[2] = 0.0;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    double u[3];
+    const bool real = rb_black_u<DIM>(g, JB, Tr, slot, NS, u);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t i = c * NS + slot;
+      double sv;
+      if (FORM) {
+        sv = R[i] - alpha * V[i];
+        v[0] += sv * sv;
+        S[i] = sv;
+      } else {
+        sv = S[i];
+      }
+      const double y = real ? sv - u[c] : 0.0;
+      To[i] = y;
+      v[1] += y * sv;
+      v[2] += y * y;
+    }
+  }
+}
+
+// true Schur residual r = rhs - S x (Tr = E x), the black part of the full
+// residual (its red part is zero); returns (r, r) share
+template <int DIM>
+__device__ __forceinline__ double rb_true_body(const tcad_pack_t& pkb, const RbMap& mp,
+                                               const FlatBlock& fb,
+                                               const double* __restrict__ JB,
+                                               const double* __restrict__ Tr,
+                                               const double* __restrict__ rhs,
+                                               const double* __restrict__ x,
+                                               double* __restrict__ r) {
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  double v = 0.0;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    double u[3];
+    const bool real = rb_black_u<DIM>(g, JB, Tr, slot, NS, u);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double y = real ? x[c * NS + slot] - u[c] : 0.0;
+      const double a = rhs[c * NS + slot] - y;
+      r[c * NS + slot] = a;
+      v += a * a;
+    }
+  }
+  return v;
+}
+
+// full solution at the block's slots: x_r = bR - Tr (Tr = E x_b), x_b; zero
+// when idle
+template <int DIM>
+__device__ __forceinline__ void rb_merge_body(const tcad_pack_t& pkb, const RbMap& mp,
+                                              const FlatBlock& fb,
+                                              const double* __restrict__ bR,
+                                              const double* __restrict__ Tr,
+                                              const double* __restrict__ xb,
+                                              double* __restrict__ x, bool idle) {
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes, NN = mp.n_full;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    const RbNode qr = rb_node(g, slot, 0);
+    const RbNode qb = rb_node(g, slot, 1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t q = c * NS + slot;
+      if (qr.real) x[c * NN + qr.node] = idle ? 0.0 : bR[q] - Tr[q];
+      if (qb.real) x[c * NN + qb.node] = idle ? 0.0 : xb[q];
+    }
+  }
+}
+
+// functor factories for rb_red_body
+struct RbMakeVal {
+  const double* x;
+  int64_t NS;
+  __device__ __forceinline__ RbVal operator()(int64_t soff) const { return RbVal{x + soff, NS}; }
+};
+struct RbMakeP {
+  const double *r, *p, *v;
+  int64_t NS;
+  double beta, omega;
+  int restart;
+  __device__ __forceinline__ RbFormP operator()(int64_t soff) const {
+    return RbFormP{r + soff, p + soff, v + soff, NS, beta, omega, restart};
+  }
+};
+struct RbMakeS {
+  const double *r, *v;
+  int64_t NS;
+  double alpha;
+  __device__ __forceinline__ RbFormS operator()(int64_t soff) const {
+    return RbFormS{r + soff, v + soff, NS, alpha};
+  }
+};
+
+// ---- one launch per step
+
 // JR, JB <- the red and black rows of the block-scaled J in warp tiles
 // (zeros at pads; the tile tail past the last slot is never read)
 template <int DIM>
@@ -146,7 +434,7 @@ k_rb_pack(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ J,
   constexpr int NE = Stencil<DIM>::NE;
   const FlatBlock fb = flat_block(pkb, blockIdx.x);
   const RbGeo g = rb_geo(pkb, mp, fb.inst);
-  const int64_t NS = pkb.n_nodes, NN = mp.n_full;
+  const int64_t NN = mp.n_full;
   for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
@@ -166,26 +454,38 @@ k_rb_split(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ b,
            double* __restrict__ bR, double* __restrict__ bB, double* __restrict__ bbf,
            double* partial, unsigned* ticket) {
   const FlatBlock fb = flat_block(pkb, blockIdx.x);
-  const RbGeo g = rb_geo(pkb, mp, fb.inst);
-  const int64_t NS = pkb.n_nodes, NN = mp.n_full;
-  double v = 0.0;
-  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const RbNode q = rb_node(g, slot, c);
-      double* __restrict__ out = c ? bB : bR;
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        const double bv = q.real ? b[r * NN + q.node] : 0.0;
-        out[r * NS + slot] = bv;
-        v += bv * bv;
-      }
-    }
-  }
-  double vv[1] = {v};
+  double vv[1] = {rb_split_body<DIM>(pkb, mp, fb, b, bR, bB)};
   double tot[1];
   if (Reduce<1>::run(pkb, blockIdx.x, fb.inst, vv, partial, ticket, tot) && threadIdx.x == 0)
     bbf[fb.inst] = tot[0];
+}
+
+// the Schur start: the tolerance is on the full ||b|| (bbf)
+__device__ __forceinline__ void rb_fin_init(KState& s, double tot, double bb, double rt,
+                                            int maxit, int pre) {
+  fin_init(s, tot, rt, maxit, pre);
+  s.bb = bb;
+  s.tol2 = rt * rt * bb;
+  if (s.status == TCAD_OK && !isfinite(bb)) {
+    s.status = TCAD_ERR_NONFINITE;
+    s.active = 0;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(NT, 3)
+k_rb_init(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
+          const double* __restrict__ bR, const double* __restrict__ bB,
+          double* __restrict__ rhs, double* __restrict__ x, BiVec w,
+          const double* __restrict__ bbf, KState* ks, double* partial, unsigned* ticket,
+          double rtol, int maxit, const int32_t* __restrict__ pre_status,
+          const double* __restrict__ rtol_inst) {
+  const FlatBlock fb = flat_block(pkb, blockIdx.x);
+  double vv[1] = {rb_init_body<DIM>(pkb, mp, fb, JB, bR, bB, rhs, x, w)};
+  double tot[1];
+  if (Reduce<1>::run(pkb, blockIdx.x, fb.inst, vv, partial, ticket, tot) && threadIdx.x == 0)
+    rb_fin_init(ks[fb.inst], tot[0], bbf[fb.inst], rtol_inst ? rtol_inst[fb.inst] : rtol,
+                maxit, pre_status ? pre_status[fb.inst] : TCAD_OK);
 }
 
 // red pass: Tr = E x (the red rows' coupling to black values x); every
@@ -198,81 +498,10 @@ k_rb_red(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JR,
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
   const FlatBlock fb = flat_block(pkb, fbi);
   if (ks && !ks[fb.inst].active) return;
-  const RbGeo g = rb_geo(pkb, mp, fb.inst);
-  const int64_t NS = pkb.n_nodes;
-  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
-    const RbNode q = rb_node(g, slot, 0);
-    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    if (q.real) {
-      int m[6];
-      rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
-      rb_couple<DIM>(JR, x + g.soff, slot, NS, m, y0, y1, y2);
-    }
-    Tr[slot] = y0; Tr[NS + slot] = y1; Tr[2 * NS + slot] = y2;
-  }
+  rb_red_body<DIM>(pkb, mp, fb, JR, RbMakeVal{x, pkb.n_nodes}, Tr);
 }
 
-// black pass at one slot: y = x_b - F Tr (0 at a pad)
-template <int DIM>
-__device__ __forceinline__ void rb_black(const RbGeo& g, const double* __restrict__ JB,
-                                         const double* __restrict__ Tr,
-                                         const double* __restrict__ X, int64_t slot,
-                                         int64_t NS, double& y0, double& y1, double& y2) {
-  const RbNode q = rb_node(g, slot, 1);
-  y0 = 0.0; y1 = 0.0; y2 = 0.0;
-  if (!q.real) return;
-  int m[6];
-  rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
-  double u0, u1, u2;
-  rb_couple<DIM>(JB, Tr + g.soff, slot, NS, m, u0, u1, u2);
-  y0 = X[slot] - u0;
-  y1 = X[NS + slot] - u1;
-  y2 = X[2 * NS + slot] - u2;
-}
-
-// Schur right-hand side and BiCGStab start: rhs = bB - F bR; x = 0,
-// r = rh = rhs, p = v = 0; the tolerance is on the full ||b|| (bbf)
-template <int DIM>
-__global__ void __launch_bounds__(NT, 3)
-k_rb_init(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
-          const double* __restrict__ bR, const double* __restrict__ bB,
-          double* __restrict__ rhs, double* __restrict__ x, BiVec w,
-          const double* __restrict__ bbf, KState* ks, double* partial, unsigned* ticket,
-          double rtol, int maxit, const int32_t* __restrict__ pre_status,
-          const double* __restrict__ rtol_inst) {
-  const FlatBlock fb = flat_block(pkb, blockIdx.x);
-  const RbGeo g = rb_geo(pkb, mp, fb.inst);
-  const int64_t NS = pkb.n_nodes;
-  double v = 0.0;
-  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
-    double y[3];
-    rb_black<DIM>(g, JB, bR, bB, slot, NS, y[0], y[1], y[2]);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t q = c * NS + slot;
-      rhs[q] = y[c];
-      x[q] = 0.0; w.r[q] = y[c]; w.rh[q] = y[c]; w.p[q] = 0.0; w.v[q] = 0.0;
-      v += y[c] * y[c];
-    }
-  }
-  double vv[1] = {v};
-  double tot[1];
-  if (Reduce<1>::run(pkb, blockIdx.x, fb.inst, vv, partial, ticket, tot) &&
-      threadIdx.x == 0) {
-    KState& s = ks[fb.inst];
-    const double rt = rtol_inst ? rtol_inst[fb.inst] : rtol;
-    fin_init(s, tot[0], rt, maxit, pre_status ? pre_status[fb.inst] : TCAD_OK);
-    const double bb = bbf[fb.inst];
-    s.bb = bb;
-    s.tol2 = rt * rt * bb;
-    if (s.status == TCAD_OK && !isfinite(bb)) {
-      s.status = TCAD_ERR_NONFINITE;
-      s.active = 0;
-    }
-  }
-}
-
-// v = S p (S = I - F E; Tr = E p from the red pass); (rh, v)
+// v = S p (Tr = E p from the red pass); (rh, v)
 template <int DIM>
 __global__ void __launch_bounds__(NT, 5)
 k_rb_v(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
@@ -281,19 +510,7 @@ k_rb_v(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
   const FlatBlock fb = flat_block(pkb, fbi);
   if (!ks[fb.inst].active) return;
-  const RbGeo g = rb_geo(pkb, mp, fb.inst);
-  const int64_t NS = pkb.n_nodes;
-  const double* __restrict__ RH = w.rh;
-  double* __restrict__ Vo = w.v;
-  double v = 0.0;
-  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
-    double y0, y1, y2;
-    rb_black<DIM>(g, JB, Tr, w.p, slot, NS, y0, y1, y2);
-    const double h0 = RH[slot], h1 = RH[NS + slot], h2 = RH[2 * NS + slot];
-    Vo[slot] = y0; Vo[NS + slot] = y1; Vo[2 * NS + slot] = y2;
-    v += h0 * y0 + h1 * y1 + h2 * y2;
-  }
-  double vv[1] = {v};
+  double vv[1] = {rb_v_body<DIM, false>(pkb, mp, fb, JB, Tr, w, 0.0, 0.0, 0)};
   double tot[1];
   if (Reduce<1>::run(pkb, fbi, fb.inst, vv, partial, ticket, tot) && threadIdx.x == 0)
     fin_v(ks[fb.inst], tot[0]);
@@ -308,26 +525,15 @@ k_rb_t(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
   const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
   const FlatBlock fb = flat_block(pkb, fbi);
   if (!ks[fb.inst].active) return;
-  const RbGeo g = rb_geo(pkb, mp, fb.inst);
-  const int64_t NS = pkb.n_nodes;
-  const double* __restrict__ S = w.s;
-  double* __restrict__ To = w.t;
-  double v[2] = {0.0, 0.0};
-  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
-    double y0, y1, y2;
-    rb_black<DIM>(g, JB, Tr, S, slot, NS, y0, y1, y2);
-    const double s0 = S[slot], s1 = S[NS + slot], s2 = S[2 * NS + slot];
-    To[slot] = y0; To[NS + slot] = y1; To[2 * NS + slot] = y2;
-    v[0] += y0 * s0 + y1 * s1 + y2 * s2;
-    v[1] += y0 * y0 + y1 * y1 + y2 * y2;
-  }
+  double v3[3];
+  rb_t_body<DIM, false>(pkb, mp, fb, JB, Tr, w, 0.0, v3);
+  double v[2] = {v3[1], v3[2]};
   double tot[2];
   if (Reduce<2>::run(pkb, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0)
     fin_t(ks[fb.inst], tot[0], tot[1]);
 }
 
-// true Schur residual r = rhs - S x (Tr = E x), which is the black part of
-// the full residual (its red part is zero); (r, r); re-arm as k_true_resid
+// true Schur residual; (r, r); re-arm as k_true_resid
 template <int DIM>
 __global__ void __launch_bounds__(NT, 3)
 k_rb_true(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
@@ -335,20 +541,7 @@ k_rb_true(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JB,
           const double* __restrict__ x, double* __restrict__ r, KState* ks, double* partial,
           unsigned* ticket, int rearm) {
   const FlatBlock fb = flat_block(pkb, blockIdx.x);
-  const RbGeo g = rb_geo(pkb, mp, fb.inst);
-  const int64_t NS = pkb.n_nodes;
-  double v = 0.0;
-  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
-    double y[3];
-    rb_black<DIM>(g, JB, Tr, x, slot, NS, y[0], y[1], y[2]);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const double a = rhs[c * NS + slot] - y[c];
-      r[c * NS + slot] = a;
-      v += a * a;
-    }
-  }
-  double vv[1] = {v};
+  double vv[1] = {rb_true_body<DIM>(pkb, mp, fb, JB, Tr, rhs, x, r)};
   double tot[1];
   if (Reduce<1>::run(pkb, blockIdx.x, fb.inst, vv, partial, ticket, tot) && threadIdx.x == 0)
     fin_true(ks[fb.inst], tot[0], rearm);
@@ -362,19 +555,8 @@ k_rb_merge(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ bR,
            const double* __restrict__ Tr, const double* __restrict__ xb,
            double* __restrict__ x, const int32_t* __restrict__ pre_status) {
   const FlatBlock fb = flat_block(pkb, blockIdx.x);
-  const RbGeo g = rb_geo(pkb, mp, fb.inst);
-  const int64_t NS = pkb.n_nodes, NN = mp.n_full;
-  const bool idle = pre_status && pre_status[fb.inst] != TCAD_OK;
-  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
-    const RbNode qr = rb_node(g, slot, 0);
-    const RbNode qb = rb_node(g, slot, 1);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t q = c * NS + slot;
-      if (qr.real) x[c * NN + qr.node] = idle ? 0.0 : bR[q] - Tr[q];
-      if (qb.real) x[c * NN + qb.node] = idle ? 0.0 : xb[q];
-    }
-  }
+  rb_merge_body<DIM>(pkb, mp, fb, bR, Tr, xb, x,
+                     pre_status && pre_status[fb.inst] != TCAD_OK);
 }
 
 }  // namespace tcad

@@ -227,3 +227,84 @@ def test_ragged_2d_batch_red_black_equals_alone():
     for a in range(len(PARAMS)):
         assert abs(I[a] - alone_I[a]) <= 1e-6 * abs(alone_I[a]), (a, I[a], alone_I[a])
         assert np.abs(batch.state(a)[0] - alone_psi[a]).max() * batch.devices[a].VT < 1e-9
+
+
+def _solve_counted(pk, method, rtol, maxit, fused):
+    import torch
+    from tcad_b200 import _lib
+    lib = pk.lib
+    prev = lib.tcad_set_krylov_fused(1 if fused else 0)
+    try:
+        x = torch.full_like(pk.du, float("nan"))
+        it, st, rr = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_double(0.0)
+        torch.cuda.synchronize()
+        n0 = lib.tcad_launch_count()
+        _lib.check(lib.tcad_block_krylov(pk.pref, _lib.ptr(pk.J), _lib.ptr(pk.F), _lib.ptr(x),
+                                         method, rtol, maxit, 0, _lib.ptr(pk.work),
+                                         pk.work.numel(), ctypes.byref(it), ctypes.byref(st),
+                                         ctypes.byref(rr), pk.sp()), "krylov")
+        torch.cuda.synchronize()
+        n = lib.tcad_launch_count() - n0
+    finally:
+        lib.tcad_set_krylov_fused(prev)
+    return x, it.value, st.value, rr.value, n
+
+
+@pytest.mark.parametrize("name", ["diode2d_201x101", "trigate3d_40x24x20", "trigate3d_41x23x19"])
+@pytest.mark.parametrize("rtol,maxit", [(1e-10, 4000), (1e-30, 60)])
+def test_schur_single_launch_bit_identical_to_per_step(name, rtol, maxit):
+    """The red-black solve of a small single-instance pack in one
+    cooperative launch (p and s formed on the fly by the red passes, five
+    grid barriers per iteration) against its one-launch-per-step loop: the
+    same bodies, scalar updates and reduction order, so solution, iteration
+    count, status and residual are bit-identical."""
+    pk = _scaled_system(_devices()[name]())
+    xa, ita, sta, rra, na = _solve_counted(pk, 2, rtol, maxit, fused=False)
+    xb, itb, stb, rrb, nb = _solve_counted(pk, 2, rtol, maxit, fused=True)
+    assert (ita, sta, rra) == (itb, stb, rrb)
+    assert np.array_equal(xa.cpu().numpy(), xb.cpu().numpy())
+    assert nb == 2 and na > 10          # colour repack + the single launch
+
+
+def test_schur_single_launch_give_up_falls_back():
+    """With the test hook the single launch's first grid barrier runs out
+    its time limit; the host solves again one launch per step, bit for bit
+    the per-step answer, and the next single launch succeeds."""
+    pk = _scaled_system(_devices()["trigate3d_40x24x20"]())
+    lib = pk.lib
+    x0, it0, st0, rr0, _ = _solve_counted(pk, 2, 1e-10, 4000, fused=False)
+    g0 = lib.tcad_krylov_fused_gave_up()
+    prev = lib.tcad_set_krylov_fused_test(1)
+    try:
+        x1, it1, st1, rr1, n1 = _solve_counted(pk, 2, 1e-10, 4000, fused=True)
+    finally:
+        lib.tcad_set_krylov_fused_test(prev)
+    assert lib.tcad_krylov_fused_gave_up() == g0 + 1
+    assert n1 > 3
+    assert (it1, st1, rr1) == (it0, st0, rr0)
+    assert np.array_equal(x1.cpu().numpy(), x0.cpu().numpy())
+    x2, it2, st2, rr2, n2 = _solve_counted(pk, 2, 1e-10, 4000, fused=True)
+    assert n2 == 2 and lib.tcad_krylov_fused_gave_up() == g0 + 1
+    assert np.array_equal(x2.cpu().numpy(), x0.cpu().numpy())
+
+
+def test_newton_sweep_single_launch_equals_per_step():
+    """A whole 201x101 diode sweep with the red-black default: single
+    launch and one launch per step give bit-identical states."""
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    states = []
+    for fused in (False, True):
+        dev = W.diode2d(tb.Device2D, 201, 101)
+        lib = dev.pack.lib
+        prev = lib.tcad_set_krylov_fused(1 if fused else 0)
+        try:
+            dev.solve_equilibrium()
+            for v in (0.2, 0.4, 0.6):
+                dev.solve_bias({"anode": v}, tb.NewtonOptions())
+                assert dev.last_converged
+            states.append([t.copy() for t in (dev.psi, dev.n, dev.p)])
+        finally:
+            lib.tcad_set_krylov_fused(prev)
+    for a, b in zip(*states):
+        assert np.array_equal(a, b)
