@@ -1017,8 +1017,9 @@ k_cg_init(const tcad_pack_t pk, const double* __restrict__ J, const double* __re
 template <int DIM>
 __global__ void __launch_bounds__(NT)
 k_cg_q(const tcad_pack_t pk, const double* __restrict__ J, CgVec w, KState* ks,
-       double* partial, unsigned* ticket) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+       double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
   if (!ks[fb.inst].active) return;
   const Inst g = load_inst(pk, fb.inst);
   int64_t off[6];
@@ -1031,7 +1032,7 @@ k_cg_q(const tcad_pack_t pk, const double* __restrict__ J, CgVec w, KState* ks,
     v[0] += w.p[k] * q;
   }
   double tot[1];
-  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+  if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     KState& s = ks[fb.inst];
     if (!(tot[0] > 0.0) || !isfinite(tot[0])) {
       s.status = TCAD_ERR_BREAKDOWN;
@@ -1044,8 +1045,9 @@ k_cg_q(const tcad_pack_t pk, const double* __restrict__ J, CgVec w, KState* ks,
 
 __global__ void __launch_bounds__(NT)
 k_cg_x(const tcad_pack_t pk, const double* __restrict__ J, double* __restrict__ x, CgVec w,
-       KState* ks, double* partial, unsigned* ticket) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+       KState* ks, double* partial, unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pk, fbi);
   const KState s0 = ks[fb.inst];
   if (!s0.active) return;
   double v[1] = {0.0};
@@ -1058,7 +1060,7 @@ k_cg_x(const tcad_pack_t pk, const double* __restrict__ J, double* __restrict__ 
     v[0] += r * z;
   }
   double tot[1];
-  if (Reduce<1>::run(pk, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+  if (Reduce<1>::run(pk, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
     KState& s = ks[fb.inst];
     s.it += 1;
     s.rho_prev = s.rho;
@@ -1079,8 +1081,8 @@ k_cg_x(const tcad_pack_t pk, const double* __restrict__ J, double* __restrict__ 
 }
 
 __global__ void __launch_bounds__(NT)
-k_cg_p(const tcad_pack_t pk, CgVec w, const KState* ks) {
-  const FlatBlock fb = flat_block(pk, blockIdx.x);
+k_cg_p(const tcad_pack_t pk, CgVec w, const KState* ks, const int32_t* __restrict__ blk) {
+  const FlatBlock fb = flat_block(pk, blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x);
   const KState s = ks[fb.inst];
   if (!s.active) return;
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) w.p[k] = w.z[k] + s.beta * w.p[k];
@@ -1971,16 +1973,22 @@ static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, do
   hks.resize(ni);
   int check = 8;
   int done_iters = 0;
+  // a batch's stragglers (the graded-mesh devices of a serving round can
+  // need tens of thousands of iterations) launch only their own blocks
+  ActiveGrid grid;
+  if (int rc = grid.init(pk, s, nullptr)) return rc;
   for (;;) {
+    const unsigned ng = grid.ng;
+    const int32_t* dlist = grid.dlist;
     for (int q = 0; q < check; ++q) {
       if (pk->dim == 2)
-        k_cg_q<2><<<nb, NT, 0, s>>>(*pk, J, w.cg, w.ks, w.partial, w.ticket);
+        k_cg_q<2><<<ng, NT, 0, s>>>(*pk, J, w.cg, w.ks, w.partial, w.ticket, dlist);
       else
-        k_cg_q<3><<<nb, NT, 0, s>>>(*pk, J, w.cg, w.ks, w.partial, w.ticket);
+        k_cg_q<3><<<ng, NT, 0, s>>>(*pk, J, w.cg, w.ks, w.partial, w.ticket, dlist);
       note_launch();
-      k_cg_x<<<nb, NT, 0, s>>>(*pk, J, x, w.cg, w.ks, w.partial, w.ticket);
+      k_cg_x<<<ng, NT, 0, s>>>(*pk, J, x, w.cg, w.ks, w.partial, w.ticket, dlist);
       note_launch();
-      k_cg_p<<<nb, NT, 0, s>>>(*pk, w.cg, w.ks);
+      k_cg_p<<<ng, NT, 0, s>>>(*pk, w.cg, w.ks, dlist);
       note_launch();
     }
     TCAD_LAUNCH_CHECK();
@@ -1991,6 +1999,7 @@ static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, do
     bool any = false;
     for (int i = 0; i < ni; ++i) any = any || hks[i].active;
     if (!any) break;
+    if (int rc = grid.update(hks, w.blk, s)) return rc;
     if (done_iters > 64) check = 32;
   }
   return TCAD_OK;
