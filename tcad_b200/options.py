@@ -146,8 +146,10 @@ class NewtonOptions:
     # tri-gate Newton systems about half the iterations (the 983k-node
     # tri-gate sweep: 1,610 BiCGStab iterations per point against 3,634, 2.04
     # against 1.17 points/s); the stopping test is the full system's.
-    # "full" iterates on the whole block-scaled system.  Single-instance
-    # packs small enough for the one-launch solve keep that solve either way.
+    # "full" iterates on the whole block-scaled system.  Either system runs
+    # in one cooperative launch per solve on a single-instance pack small
+    # enough to be resident at once (the 201x101 diode: 33.7 points/s
+    # red-black, 21.3 whole system).
     krylov_system: str = "red_black"
 
     def __post_init__(self):

@@ -19,8 +19,8 @@ pytestmark = pytest.mark.gpu
 
 @contextlib.contextmanager
 def _per_step(lib):
-    """Single-instance packs small enough for the one-launch solve keep it;
-    turning that solve off sends them through the Schur loop."""
+    """Single-instance packs small enough are solved in one cooperative
+    launch; turning that off sends them through the per-step Schur loop."""
     prev = lib.tcad_set_krylov_fused(0)
     try:
         yield
