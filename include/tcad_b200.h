@@ -204,7 +204,11 @@ int tcad_state_extrapolate(const tcad_pack_t* pk, double* psi, double* n, double
                            const double* ratio, void* stream);
 
 /* ---- linear algebra on the node-block layout ---------------------------
- * Workspace size in bytes for tcad_block_krylov / tcad_newton_solve. */
+ * Workspace size in bytes for tcad_block_krylov / tcad_newton_solve.
+ * method 2 includes the red-black Schur extension (two colour copies of the
+ * Jacobian and five slot vectors), which tcad_block_krylov method 2 needs
+ * and tcad_newton_opts_t.red_black uses; a tcad_newton_solve workspace
+ * sized without it (method 0) solves the whole system.  restart is unused. */
 size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart);
 
 /* Launch shape of the node-block-Jacobi BiCGStab (an implementation switch;
@@ -385,8 +389,9 @@ typedef struct tcad_newton_opts {
    * product, about half the iterations); the stopping test stays the full
    * system's ||b - A x|| <= eta ||b||.  A single-instance pack whose slot
    * blocks fit on the GPU at once is solved in one cooperative launch (the
-   * same arithmetic).  ILU(0) solves and FP32 operators keep the full
-   * system.  0: the full system always. */
+   * same arithmetic).  ILU(0) solves, FP32 operators and a workspace sized
+   * without the red-black extension (tcad_block_workspace_bytes method 0)
+   * keep the full system.  0: the full system always. */
   int32_t red_black;
   int32_t reserved_opts;  /* 0 */
 } tcad_newton_opts_t;

@@ -2032,8 +2032,10 @@ static size_t off_rb(const tcad_pack_t* pk) {
 
 extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart) {
   if (!pk) return 0;
-  (void)method; (void)restart;
-  return off_rb(pk) + carve_rb(pk, nullptr).bytes + 512;
+  (void)restart;
+  // the red-black extension (two colour copies of J and five slot vectors,
+  // about as much again as J) only for method 2
+  return off_rb(pk) + (method == 2 ? carve_rb(pk, nullptr).bytes : 0) + 512;
 }
 
 extern "C" int tcad_block_jacobi_setup(const tcad_pack_t* pk, double* J, double* F,
@@ -2151,7 +2153,7 @@ extern "C" int tcad_block_krylov(const tcad_pack_t* pk, const double* J, const d
   std::vector<KState> hks;
   int rc;
   if (method == 2) {
-    if (work_bytes < tcad_block_workspace_bytes(pk, 0, 0)) return TCAD_ERR_ARG;
+    if (work_bytes < tcad_block_workspace_bytes(pk, 2, 0)) return TCAD_ERR_ARG;
     const WorkRb wrb = carve_rb(pk, reinterpret_cast<char*>(work) + off_rb(pk));
     RbLayout rbl;
     if ((rc = rb_layout(pk, wrb, rbl, s)) != TCAD_OK) return rc;
@@ -2243,8 +2245,9 @@ extern "C" int tcad_newton_solve(const tcad_pack_t* pk, double* psi, double* n, 
   // red-black Schur solves: the slot pack's tables, once per call (a
   // single-instance pack small enough is solved in one cooperative launch,
   // k_bicgstab_rb_fused, by launch_bicgstab_rb itself)
-  const bool use_rb = opts->red_black != 0;
-  if (use_rb && work_bytes < tcad_block_workspace_bytes(pk, 0, 0)) return TCAD_ERR_ARG;
+  // (a workspace sized without the red-black extension -- method 0 -- solves
+  // the whole system)
+  const bool use_rb = opts->red_black != 0 && work_bytes >= tcad_block_workspace_bytes(pk, 2, 0);
   WorkRb wrb{};
   RbLayout rbl;
   if (use_rb) {

@@ -401,7 +401,7 @@ class Pack:
         self.F = z(3 * self.N)
         self.J = z(_lib.NE[dim] * self.N)
         self.du = z(3 * self.N)
-        wb = int(self.lib.tcad_block_workspace_bytes(self.pref, 0, 0))
+        wb = int(self.lib.tcad_block_workspace_bytes(self.pref, 2, 0))
         self.work = torch.empty(wb, dtype=torch.uint8, device=self.device)
         self.active = torch.ones(len(self.setups), dtype=torch.uint8, device=self.device)
         self.refresh_bcs()
@@ -700,7 +700,7 @@ class Pack:
         P.tile = self.t["tile"].data_ptr()
         P.n_tiles = self.n_tiles
         P.tile_z = self.tile_z = int(tile_z)
-        wb = int(self.lib.tcad_block_workspace_bytes(self.pref, 0, 0))
+        wb = int(self.lib.tcad_block_workspace_bytes(self.pref, 2, 0))
         if wb > self.work.numel():
             self.work = self.torch.empty(wb, dtype=self.torch.uint8, device=self.device)
 

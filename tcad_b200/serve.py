@@ -153,6 +153,9 @@ class Arena:
         P.n_flat = cap // 256 + self.max_inst    # any flat_nodes >= 256
         P.flat_nodes = _lib.FLAT_NODES
         P.tile_z = TILE_Z
+        # sized without the red-black extension (method 0): served solves run
+        # on the whole system -- the mixed-precision default does anyway --
+        # and the arena keeps its nodes for devices
         wb = int(self.lib.tcad_block_workspace_bytes(ctypes_ref(P), 0, 0))
         self.work = torch.empty(wb, dtype=torch.uint8, device=self.device)
         self.nodes = RangeAllocator(cap, ALIGN)
