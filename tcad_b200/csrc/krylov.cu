@@ -1088,6 +1088,236 @@ k_cg_p(const tcad_pack_t pk, CgVec w, const KState* ks, const int32_t* __restric
   for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) w.p[k] = w.z[k] + s.beta * w.p[k];
 }
 
+// ---- equilibrium PCG on the red-black Schur complement (scalar Poisson)
+//
+// The equilibrium Newton step solves A d = F with A = -J (SPD: the box-
+// integration Laplacian plus the diagonal charge derivative; eliminated
+// Dirichlet rows are identity rows).  Its 5-/7-point stencil has no coupling
+// inside a colour, so with the colour slot layout of redblack.cuh
+//     A = [ A_rr  A_rb ]      S = A_bb - A_br A_rr^-1 A_rb   (SPD, black slots)
+//         [ A_br  A_bb ]      S d_b = F_b - A_br A_rr^-1 F_r,
+//                             d_r = A_rr^-1 (F_r - A_rb d_b),
+// A_rr diagonal.  PCG runs on S with its exact diagonal as the Jacobi
+// preconditioner: half the unknowns, the same matrix bytes per product
+// (a red pass t = A_rr^-1 A_rb p and a black pass q = A_bb p - A_br t).
+// The colour rows of J (1 + 2 DIM entries, the diagonal first) are stored
+// entry-major per colour: JRe / JBe [1 + 2 DIM][slots].
+
+// JRe, JBe <- colour rows of the equilibrium J; bR, bB <- colours of F
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eqrb_pack(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ J,
+            const double* __restrict__ F, double* __restrict__ JRe, double* __restrict__ JBe,
+            double* __restrict__ bR, double* __restrict__ bB) {
+  constexpr int NE = 1 + 2 * DIM;
+  const FlatBlock fb = flat_block(pkb, blockIdx.x);
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes, NN = mp.n_full;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const RbNode q = rb_node(g, slot, c);
+      double* __restrict__ out = c ? JBe : JRe;
+#pragma unroll
+      for (int e = 0; e < NE; ++e)
+        out[(int64_t)e * NS + slot] = q.real ? J[(int64_t)e * NN + q.node] : 0.0;
+      (c ? bB : bR)[slot] = q.real ? F[q.node] : 0.0;
+    }
+  }
+}
+
+// red pass: Tr = A_rr^-1 (v_r - A_rb x) at the block's red slots (v null:
+// -A_rr^-1 A_rb x); every instance when ks is null
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eqrb_red(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JRe,
+           const double* __restrict__ x, const double* __restrict__ vr,
+           double* __restrict__ Tr, const KState* ks, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pkb, fbi);
+  if (ks && !ks[fb.inst].active) return;
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  const double* __restrict__ xi = x + g.soff;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    const RbNode q = rb_node(g, slot, 0);
+    double t = 0.0;
+    if (q.real) {
+      int m[6];
+      rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
+      double a = 0.0;                         // (J_rb x): A_rb = -J_rb
+#pragma unroll
+      for (int d = 0; d < 2 * DIM; ++d) a += JRe[(int64_t)(1 + d) * NS + slot] * xi[m[d]];
+      const double arr = -JRe[slot];
+      t = ((vr ? vr[slot] : 0.0) + a) / arr;  // A_rr^-1 (v_r - A_rb x)
+    }
+    Tr[slot] = t;
+  }
+}
+
+// black coupling at one slot: sum_d A_bd Tr(m_d) = -sum_d J_bd Tr(m_d)
+template <int DIM>
+__device__ __forceinline__ double eqrb_black_u(const RbGeo& g, const double* __restrict__ JBe,
+                                               const double* __restrict__ Tr, int64_t slot,
+                                               int64_t NS, const RbNode& q) {
+  int m[6];
+  rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
+  const double* __restrict__ ti = Tr + g.soff;
+  double a = 0.0;
+#pragma unroll
+  for (int d = 0; d < 2 * DIM; ++d) a += JBe[(int64_t)(1 + d) * NS + slot] * ti[m[d]];
+  return -a;
+}
+
+// Sinv = 1 / diag(S): diag(S)_b = A_bb - sum_d A_bd A_{r(d) b} / A_{r(d)}
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eqrb_diag(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JRe,
+            const double* __restrict__ JBe, double* __restrict__ Sinv) {
+  const FlatBlock fb = flat_block(pkb, blockIdx.x);
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    const RbNode q = rb_node(g, slot, 1);
+    double sd = 0.0;
+    if (q.real) {
+      int m[6];
+      rb_nbrs<DIM>(g, q, (int)(slot - g.soff), m);
+      sd = -JBe[slot];
+#pragma unroll
+      for (int d = 0; d < 2 * DIM; ++d) {
+        const double jbd = JBe[(int64_t)(1 + d) * NS + slot];
+        if (jbd != 0.0) {                     // a real neighbour: its row holds
+          const int64_t r = g.soff + m[d];    //   the coupling back, direction d ^ 1
+          const double jrb = JRe[(int64_t)(1 + (d ^ 1)) * NS + r];
+          sd -= (jbd * jrb) / (-JRe[r]);
+        }
+      }
+    }
+    Sinv[slot] = (q.real && sd != 0.0) ? 1.0 / sd : 0.0;
+  }
+}
+
+// Schur start: rhs = F_b - A_br A_rr^-1 F_r (Tr = A_rr^-1 F_r from the red
+// pass), x = 0, r = rhs, z = Sinv r, p = z; (r, z), (r, r) as k_cg_init
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eqrb_init(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JBe,
+            const double* __restrict__ bB, const double* __restrict__ Tr,
+            const double* __restrict__ Sinv, double* __restrict__ x, CgVec w, KState* ks,
+            double* partial, unsigned* ticket, double rtol, int maxit,
+            const uint8_t* __restrict__ active, const double* __restrict__ rtol_inst) {
+  const FlatBlock fb = flat_block(pkb, blockIdx.x);
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  double v[2] = {0.0, 0.0};
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    const RbNode q = rb_node(g, slot, 1);
+    const double bv = q.real ? bB[slot] - eqrb_black_u<DIM>(g, JBe, Tr, slot, NS, q) : 0.0;
+    const double z = bv * Sinv[slot];
+    x[slot] = 0.0; w.r[slot] = bv; w.z[slot] = z; w.p[slot] = z;
+    v[0] += bv * z;
+    v[1] += bv * bv;
+  }
+  double tot[2];
+  if (Reduce<2>::run(pkb, blockIdx.x, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.bb = tot[0]; s.rho = tot[0]; s.rr = tot[0];
+    const double rt = rtol_inst ? rtol_inst[fb.inst] : rtol;
+    s.tol2 = rt * rt * tot[0];
+    s.it = 0; s.maxit = maxit; s.status = TCAD_OK; s.restart = 0; s.early = 0;
+    if (!isfinite(tot[0]) || !isfinite(tot[1])) s.status = TCAD_ERR_NONFINITE;
+    s.active = (s.status == TCAD_OK && tot[0] > 0.0 && (!active || active[fb.inst])) ? 1 : 0;
+  }
+}
+
+// q = S p (Tr from the red pass of p); alpha = rho / (p, q)
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eqrb_q(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ JBe,
+         const double* __restrict__ Tr, CgVec w, KState* ks, double* partial,
+         unsigned* ticket, const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pkb, fbi);
+  if (!ks[fb.inst].active) return;
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  const int64_t NS = pkb.n_nodes;
+  double v[1] = {0.0};
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    const RbNode q = rb_node(g, slot, 1);
+    const double pv = w.p[slot];
+    // S p = A_bb p + A_br t, t = -A_rr^-1 A_rb p
+    const double qv = q.real ? -JBe[slot] * pv + eqrb_black_u<DIM>(g, JBe, Tr, slot, NS, q)
+                             : 0.0;
+    w.q[slot] = qv;
+    v[0] += pv * qv;
+  }
+  double tot[1];
+  if (Reduce<1>::run(pkb, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    if (!(tot[0] > 0.0) || !isfinite(tot[0])) {
+      s.status = TCAD_ERR_BREAKDOWN;
+      s.active = 0;
+    } else {
+      s.alpha = s.rho / tot[0];
+    }
+  }
+}
+
+// x += alpha p, r -= alpha q, z = Sinv r; (r, z), convergence as k_cg_x
+__global__ void __launch_bounds__(NT)
+k_eqrb_x(const tcad_pack_t pkb, const double* __restrict__ Sinv, double* __restrict__ x,
+         CgVec w, KState* ks, double* partial, unsigned* ticket,
+         const int32_t* __restrict__ blk) {
+  const int64_t fbi = blk ? (int64_t)blk[blockIdx.x] : (int64_t)blockIdx.x;
+  const FlatBlock fb = flat_block(pkb, fbi);
+  const KState s0 = ks[fb.inst];
+  if (!s0.active) return;
+  double v[1] = {0.0};
+  for (int64_t k = fb.begin + threadIdx.x; k < fb.end; k += NT) {
+    x[k] = x[k] + s0.alpha * w.p[k];
+    const double r = w.r[k] - s0.alpha * w.q[k];
+    w.r[k] = r;
+    const double z = r * Sinv[k];
+    w.z[k] = z;
+    v[0] += r * z;
+  }
+  double tot[1];
+  if (Reduce<1>::run(pkb, fbi, fb.inst, v, partial, ticket, tot) && threadIdx.x == 0) {
+    KState& s = ks[fb.inst];
+    s.it += 1;
+    s.rho_prev = s.rho;
+    s.rho = tot[0];
+    s.rr = tot[0];
+    if (!isfinite(tot[0])) {
+      s.status = TCAD_ERR_NONFINITE;
+      s.active = 0;
+    } else if (tot[0] <= s.tol2) {
+      s.active = 0;
+    } else if (s.it >= s.maxit) {
+      s.status = TCAD_ERR_NOCONV;
+      s.active = 0;
+    } else {
+      s.beta = s.rho / s.rho_prev;
+    }
+  }
+}
+
+// full update: d_r = Tr (= A_rr^-1 (F_r - A_rb d_b) from the red pass), d_b = x
+template <int DIM>
+__global__ void __launch_bounds__(NT)
+k_eqrb_merge(const tcad_pack_t pkb, const RbMap mp, const double* __restrict__ Tr,
+             const double* __restrict__ xb, double* __restrict__ d) {
+  const FlatBlock fb = flat_block(pkb, blockIdx.x);
+  const RbGeo g = rb_geo(pkb, mp, fb.inst);
+  for (int64_t slot = fb.begin + threadIdx.x; slot < fb.end; slot += NT) {
+    const RbNode qr = rb_node(g, slot, 0);
+    const RbNode qb = rb_node(g, slot, 1);
+    if (qr.real) d[qr.node] = Tr[slot];
+    if (qb.real) d[qb.node] = xb[slot];
+  }
+}
+
 // equilibrium update: clip to +-max_dpsi, psi += d, err = max |d|
 __global__ void __launch_bounds__(NT)
 k_eq_update(const tcad_pack_t pk, double* __restrict__ psi, const double* __restrict__ d,
@@ -1360,6 +1590,41 @@ static WorkRb carve_rb(const tcad_pack_t* pk, void* base) {
   return w;
 }
 
+// Equilibrium red-black extension: the colour rows of the Poisson J, the
+// Schur diagonal's inverse, the colours of F, the red pass result, the black
+// iterate (slot arrays sized by n_nodes) and the slot pack's tables.  Part of
+// every workspace (about 15 doubles a node in 3D).
+struct WorkEq {
+  double *JRe, *JBe, *Sinv, *bR, *bB, *tR, *xb;
+  int32_t* shape;
+  int64_t* node_off;
+  int64_t* flat_off;
+  int32_t* flat_inst;
+  int32_t* blk;
+  size_t bytes;
+};
+
+static WorkEq carve_eq(const tcad_pack_t* pk, void* base) {
+  Carve c{reinterpret_cast<char*>(base), 0, 0};
+  WorkEq w;
+  const size_t nn = (size_t)pk->n_nodes;
+  const size_t ne = 1 + 2 * (size_t)pk->dim;
+  w.JRe = c.take<double>(ne * nn);
+  w.JBe = c.take<double>(ne * nn);
+  w.Sinv = c.take<double>(nn);
+  w.bR = c.take<double>(nn);
+  w.bB = c.take<double>(nn);
+  w.tR = c.take<double>(nn);
+  w.xb = c.take<double>(nn);
+  w.shape = c.take<int32_t>(3 * (size_t)pk->n_inst);
+  w.node_off = c.take<int64_t>((size_t)pk->n_inst + 1);
+  w.flat_off = c.take<int64_t>((size_t)pk->n_inst + 1);
+  w.flat_inst = c.take<int32_t>(rb_flat_cap(pk));
+  w.blk = c.take<int32_t>(rb_flat_cap(pk));
+  w.bytes = c.used;
+  return w;
+}
+
 // The slot pack of a pack (host tables; see redblack.cuh): per instance
 // (ceil(Nx/2), Ny Nz, 1) slots of each colour, flat blocks of pk->flat_nodes
 struct RbLayout {
@@ -1368,7 +1633,8 @@ struct RbLayout {
   std::vector<int64_t> hfoff;
 };
 
-static int rb_layout(const tcad_pack_t* pk, const WorkRb& wr, RbLayout& L, cudaStream_t s) {
+template <class W>   // WorkRb or WorkEq: the slot pack's table arrays
+static int rb_layout(const tcad_pack_t* pk, const W& wr, RbLayout& L, cudaStream_t s) {
   const int ni = pk->n_inst;
   std::vector<int32_t> shp(3 * (size_t)ni), sb(3 * (size_t)ni), fi;
   TCAD_CUDA_CHECK(cudaMemcpyAsync(shp.data(), pk->shape, sizeof(int32_t) * shp.size(),
@@ -2005,6 +2271,85 @@ static int launch_cg(const tcad_pack_t* pk, const double* J, const double* b, do
   return TCAD_OK;
 }
 
+// Equilibrium PCG on the red-black Schur complement (k_eqrb_*): the same
+// per-instance loop, masks and compaction as launch_cg, on the black slots;
+// d is the full update.  L: the slot pack (rb_layout over we's tables).
+static int launch_cg_rb(const tcad_pack_t* pk, const RbLayout& L, const WorkEq& we,
+                        const double* J, const double* b, double* d, double rtol,
+                        int maxiter, const Work& w, const uint8_t* active,
+                        std::vector<KState>& hks, cudaStream_t s,
+                        const double* rtol_inst = nullptr) {
+  const tcad_pack_t& pkb = L.pkb;
+  const unsigned nbb = (unsigned)pkb.n_flat;
+  const int ni = pk->n_inst;
+  const bool d2 = pk->dim == 2;
+  CgVec cg = w.cg;   // black slot vectors
+  TCAD_CUDA_CHECK(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned) * ni, s));
+  TCAD_CUDA_CHECK(cudaMemsetAsync(we.xb, 0, sizeof(double) * (size_t)pkb.n_nodes, s));
+  if (d2) {
+    k_eqrb_pack<2><<<nbb, NT, 0, s>>>(pkb, L.mp, J, b, we.JRe, we.JBe, we.bR, we.bB);
+    k_eqrb_diag<2><<<nbb, NT, 0, s>>>(pkb, L.mp, we.JRe, we.JBe, we.Sinv);
+    k_eqrb_red<2><<<nbb, NT, 0, s>>>(pkb, L.mp, we.JRe, we.xb, we.bR, we.tR, nullptr, nullptr);
+    k_eqrb_init<2><<<nbb, NT, 0, s>>>(pkb, L.mp, we.JBe, we.bB, we.tR, we.Sinv, we.xb, cg,
+                                      w.ks, w.partial, w.ticket, rtol, maxiter, active,
+                                      rtol_inst);
+  } else {
+    k_eqrb_pack<3><<<nbb, NT, 0, s>>>(pkb, L.mp, J, b, we.JRe, we.JBe, we.bR, we.bB);
+    k_eqrb_diag<3><<<nbb, NT, 0, s>>>(pkb, L.mp, we.JRe, we.JBe, we.Sinv);
+    k_eqrb_red<3><<<nbb, NT, 0, s>>>(pkb, L.mp, we.JRe, we.xb, we.bR, we.tR, nullptr, nullptr);
+    k_eqrb_init<3><<<nbb, NT, 0, s>>>(pkb, L.mp, we.JBe, we.bB, we.tR, we.Sinv, we.xb, cg,
+                                      w.ks, w.partial, w.ticket, rtol, maxiter, active,
+                                      rtol_inst);
+  }
+  for (int l = 0; l < 4; ++l) note_launch();
+  TCAD_LAUNCH_CHECK();
+  hks.resize(ni);
+  int check = 8;
+  int done_iters = 0;
+  ActiveGrid grid;
+  if (int rc = grid.init(&pkb, s, &L.hfoff)) return rc;
+  for (;;) {
+    const unsigned ng = grid.ng;
+    const int32_t* dlist = grid.dlist;
+    for (int q = 0; q < check; ++q) {
+      if (d2) {
+        k_eqrb_red<2><<<ng, NT, 0, s>>>(pkb, L.mp, we.JRe, cg.p, nullptr, we.tR, w.ks, dlist);
+        k_eqrb_q<2><<<ng, NT, 0, s>>>(pkb, L.mp, we.JBe, we.tR, cg, w.ks, w.partial, w.ticket,
+                                      dlist);
+      } else {
+        k_eqrb_red<3><<<ng, NT, 0, s>>>(pkb, L.mp, we.JRe, cg.p, nullptr, we.tR, w.ks, dlist);
+        k_eqrb_q<3><<<ng, NT, 0, s>>>(pkb, L.mp, we.JBe, we.tR, cg, w.ks, w.partial, w.ticket,
+                                      dlist);
+      }
+      k_eqrb_x<<<ng, NT, 0, s>>>(pkb, we.Sinv, we.xb, cg, w.ks, w.partial, w.ticket, dlist);
+      k_cg_p<<<ng, NT, 0, s>>>(pkb, cg, w.ks, dlist);
+      for (int l = 0; l < 4; ++l) note_launch();
+    }
+    TCAD_LAUNCH_CHECK();
+    done_iters += check;
+    TCAD_CUDA_CHECK(cudaMemcpyAsync(hks.data(), w.ks, sizeof(KState) * ni,
+                                    cudaMemcpyDeviceToHost, s));
+    TCAD_CUDA_CHECK(cudaStreamSynchronize(s));
+    bool any = false;
+    for (int i = 0; i < ni; ++i) any = any || hks[i].active;
+    if (!any) break;
+    if (int rc = grid.update(hks, we.blk, s)) return rc;
+    if (done_iters > 64) check = 32;
+  }
+  // d_r = A_rr^-1 (F_r - A_rb d_b), then the full update
+  if (d2) {
+    k_eqrb_red<2><<<nbb, NT, 0, s>>>(pkb, L.mp, we.JRe, we.xb, we.bR, we.tR, nullptr, nullptr);
+    k_eqrb_merge<2><<<nbb, NT, 0, s>>>(pkb, L.mp, we.tR, we.xb, d);
+  } else {
+    k_eqrb_red<3><<<nbb, NT, 0, s>>>(pkb, L.mp, we.JRe, we.xb, we.bR, we.tR, nullptr, nullptr);
+    k_eqrb_merge<3><<<nbb, NT, 0, s>>>(pkb, L.mp, we.tR, we.xb, d);
+  }
+  note_launch();
+  note_launch();
+  TCAD_LAUNCH_CHECK();
+  return TCAD_OK;
+}
+
 }  // namespace tcad
 
 using namespace tcad;
@@ -2020,14 +2365,18 @@ extern "C" int tcad_set_krylov_fused(int on) {
 }
 
 // offsets of the workspace's extensions: FP64 work, then the FP32 extension,
-// the ILU(0) extension and the red-black Schur extension
+// the ILU(0) extension, the equilibrium red-black extension and the
+// red-black Schur extension of the coupled solves
 static size_t rnd256(size_t b) { return (b + 255) & ~(size_t)255; }
 static size_t off_w32(const tcad_pack_t* pk) { return rnd256(carve(pk, nullptr, 0).bytes); }
 static size_t off_ilu(const tcad_pack_t* pk) {
   return off_w32(pk) + rnd256(carve32(pk, nullptr).bytes);
 }
-static size_t off_rb(const tcad_pack_t* pk) {
+static size_t off_eq(const tcad_pack_t* pk) {
   return off_ilu(pk) + rnd256(carve_ilu(pk, nullptr).bytes);
+}
+static size_t off_rb(const tcad_pack_t* pk) {
+  return off_eq(pk) + rnd256(carve_eq(pk, nullptr).bytes);
 }
 
 extern "C" size_t tcad_block_workspace_bytes(const tcad_pack_t* pk, int method, int restart) {
@@ -2580,13 +2929,25 @@ extern "C" int tcad_equilibrium_solve(const tcad_pack_t* pk, double* psi, double
   // test, are solved to rtol; quadratic convergence is kept and the
   // converged potential is the same discrete solution
   std::vector<double> heta(ni, opts->forcing ? std::max(opts->eta_max, opts->rtol) : opts->rtol);
+  // PCG on the red-black Schur complement (opts->red_black; the workspace's
+  // equilibrium extension): the slot pack's tables once per call
+  const bool use_rb = opts->red_black != 0 && work_bytes >= tcad_block_workspace_bytes(pk, 0, 0);
+  WorkEq we{};
+  RbLayout rbl;
+  if (use_rb) {
+    we = carve_eq(pk, reinterpret_cast<char*>(work) + off_eq(pk));
+    if (int rc = rb_layout(pk, we, rbl, s)) return rc;
+  }
   for (int it = 0; it < opts->max_iter; ++it) {
     TCAD_CUDA_CHECK(cudaMemcpyAsync(dact, hact.data(), ni, cudaMemcpyHostToDevice, s));
     TCAD_CUDA_CHECK(cudaMemcpyAsync(w.eta, heta.data(), sizeof(double) * ni,
                                     cudaMemcpyHostToDevice, s));
     int rc = tcad_poisson_assemble(pk, psi, F, J, TCAD_MODE_ELIMINATE, stream);
     if (rc != TCAD_OK) return rc;
-    rc = launch_cg(pk, J, F, d, opts->rtol, opts->krylov_maxiter, w, dact, hks, s, w.eta);
+    rc = use_rb ? launch_cg_rb(pk, rbl, we, J, F, d, opts->rtol, opts->krylov_maxiter, w, dact,
+                               hks, s, w.eta)
+                : launch_cg(pk, J, F, d, opts->rtol, opts->krylov_maxiter, w, dact, hks, s,
+                            w.eta);
     if (rc != TCAD_OK) return rc;
     TCAD_CUDA_CHECK(cudaMemsetAsync(w.err, 0, sizeof(unsigned long long) * ni, s));
     k_eq_update<<<nb, NT, 0, s>>>(*pk, psi, d, opts->max_dpsi, dact, w.err);

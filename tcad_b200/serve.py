@@ -47,8 +47,9 @@ def bytes_per_node(dim):
     """HBM bytes one resident node costs: coefficients, BC arrays, state, F,
     the node-block Jacobian, the Newton update and the Krylov workspace
     (FP64 BiCGStab vectors and the FP32 extension of the mixed-precision
-    path), the ILU(0) preconditioner, and the previous state the
-    sweep predictor extrapolates from."""
+    path), the ILU(0) preconditioner, the equilibrium PCG's red-black
+    extension, and the previous state the sweep predictor extrapolates
+    from."""
     ne = _lib.NE[dim]
     doubles = len(NODE_ARRAYS) + 3 * dim + len(BC_ARRAYS) + 3 + 3 + 3 + ne + 3
     work64 = 6 * 3 * 8 + 4 * 8 / 256
@@ -56,7 +57,8 @@ def bytes_per_node(dim):
     ilu = (9 + 6) * 8                        # ILU(0) factor and two vectors
     if dim == 2:                             # slot-order sweep data (FP32) and vectors
         ilu += 2 * (27 + 18) * 4 + 2 * 2 * 3 * 8
-    return int(np.ceil(doubles * 8 + 1 + work64 + work32 + ilu))
+    eq = (2 * (1 + 2 * dim) + 5) * 8 + 2 * 4 / 256   # equilibrium red-black extension
+    return int(np.ceil(doubles * 8 + 1 + work64 + work32 + ilu + eq))
 
 
 class RangeAllocator:

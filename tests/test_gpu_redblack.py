@@ -308,3 +308,38 @@ def test_newton_sweep_single_launch_equals_per_step():
             lib.tcad_set_krylov_fused(prev)
     for a, b in zip(*states):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["mosfet2d_128x64", "trigate3d_41x23x19"])
+def test_equilibrium_pcg_red_black_matches_whole_system(name):
+    """The equilibrium Newton with its PCG on the red-black Schur complement
+    (the default) lands on the whole-system PCG's potential (within 1e-10 V)
+    in fewer PCG iterations."""
+    import tcad_b200 as tb
+    res = {}
+    for system in ("full", "red_black"):
+        dev = _devices()[name]()
+        dev.solve_equilibrium(tb.NewtonOptions(krylov_system=system))
+        eq = dev.last_equilibrium
+        assert eq["converged"], system
+        res[system] = (dev.psi.copy(), eq["krylov_iters"], dev.VT)
+    (pa, ka, vt), (pb, kb, _) = res["full"], res["red_black"]
+    assert np.abs(pa - pb).max() * vt < 1e-10
+    assert kb < ka, (kb, ka)
+
+
+def test_equilibrium_pcg_red_black_batch_equals_alone():
+    """Ragged 2D batch (odd Nx) equilibrium through the red-black PCG: each
+    instance's potential equals its solo solve's within 1e-10 V."""
+    import tcad_b200 as tb
+    from tcad_b200.batch import DeviceBatch
+    from test_gpu_batch import PARAMS, _build
+    alone = []
+    for q in PARAMS:
+        dev = _build(q)
+        dev.solve_equilibrium()
+        alone.append(dev.psi.copy())
+    b = DeviceBatch([_build(q) for q in PARAMS])
+    b.solve_equilibrium()
+    for a in range(len(PARAMS)):
+        assert np.abs(b.state(a)[0] - alone[a]).max() * b.devices[a].VT < 1e-10

@@ -149,6 +149,24 @@ def test_range_allocator_first_fit_and_coalescing():
 def test_arena_bytes_per_node():
     from tcad_b200.serve import bytes_per_node
     # coefficients + BC + state + previous state + F + J + du (doubles),
-    # bcflag, FP64 and FP32 Krylov workspace, ILU(0) factor and vectors
-    assert 1370 <= bytes_per_node(2) <= 1460
-    assert 1060 <= bytes_per_node(3) <= 1140
+    # bcflag, FP64 and FP32 Krylov workspace, ILU(0) factor and vectors,
+    # the equilibrium PCG's red-black extension
+    assert 1490 <= bytes_per_node(2) <= 1580
+    assert 1210 <= bytes_per_node(3) <= 1300
+
+
+def test_arena_estimate_covers_the_workspace():
+    """The serving arena's per-node estimate holds the library's own
+    workspace (sized without the coupled red-black extension) with the node
+    arrays it does not count."""
+    import ctypes
+    from tcad_b200 import _lib
+    from tcad_b200.serve import bytes_per_node
+    lib = _lib.load(require_gpu=False)
+    for dim in (2, 3):
+        P = _lib.TcadPack()
+        P.dim, P.n_inst, P.n_nodes = dim, 64, 1 << 20
+        P.n_flat, P.flat_nodes, P.tile_z = (1 << 20) // 256 + 64, _lib.FLAT_NODES, 2
+        wb = lib.tcad_block_workspace_bytes(ctypes.byref(P), 0, 0)
+        arrays = (1 + 3 * dim + 3 + 3 + 3 + 3 + _lib.NE[dim] + 3) * 8   # not in wb
+        assert wb / P.n_nodes <= bytes_per_node(dim) - arrays + 64, (dim, wb / P.n_nodes)
