@@ -391,7 +391,9 @@ typedef struct tcad_newton_opts {
    * blocks fit on the GPU at once is solved in one cooperative launch (the
    * same arithmetic).  ILU(0) solves, FP32 operators and a workspace sized
    * without the red-black extension (tcad_block_workspace_bytes method 0)
-   * keep the full system.  0: the full system always. */
+   * keep the full system.  tcad_equilibrium_solve: its PCG runs on the
+   * red-black Schur complement of the scalar Poisson system (every
+   * workspace holds that extension).  0: the full systems always. */
   int32_t red_black;
   int32_t reserved_opts;  /* 0 */
 } tcad_newton_opts_t;
