@@ -62,10 +62,11 @@ struct RbNode {
 // Index arithmetic is 32-bit and instance-local (an instance has far fewer
 // than 2^31 slots): 64-bit division is a long instruction sequence and its
 // registers halved the occupancy of the passes.  The passes that run every
-// iteration are held to 5 CTAs per SM (51 registers; the black passes spill
-// 44 bytes): they are latency-bound -- under ncu the 3-CTA black pass waited
-// 33 long-scoreboard stalls per issue at 34 % warps active, DRAM 33 % busy
-// -- and a whole iteration went from 511 us at 4 CTAs to 419 at 5.
+// iteration are held to 5 CTAs per SM (48 registers; the t pass spills 72
+// bytes): they are latency-bound -- under ncu the 3-CTA black pass waited 33
+// long-scoreboard stalls per issue at 34 % warps active, DRAM 33 % busy --
+// and a two-lane tri-gate iteration went from 511 us at 4 CTAs to 419 at 5
+// (about 410 with J in warp tiles).
 __device__ __forceinline__ RbNode rb_node(const RbGeo& g, int64_t slot, int colour) {
   RbNode q;
   const unsigned local = (unsigned)(slot - g.soff);
