@@ -32,7 +32,12 @@ update test saturates at the 1e-10 density floor).  Each fixture holds the
 terminal currents and (psi, n, p) at a seeded sample of nodes (the whole
 fields would be several MB).
 
-Usage:  python tests/golden/make_oracle_sweeps.py [mosfets] [trigate] [pin]
+* ``trigate_mid.npz`` -- the tri-gate at 64 x 40 x 28 (71,680 nodes), the
+  down-scaled size of the headline sweep: equilibrium, then Vg = 0 and
+  0.05 V at Vd = 0.05 V and Vg = 0 at Vd = 0.7 V, each branch from
+  equilibrium (a few points: each SuperLU step takes minutes at this size).
+
+Usage:  python tests/golden/make_oracle_sweeps.py [mosfets] [trigate] [pin] [trigate_mid]
 """
 import multiprocessing as mp
 import os
@@ -198,11 +203,58 @@ def job_pin():
                         fields=np.array(F), iters=np.array(iters))
 
 
-JOBS = {"mosfets": job_mosfets, "trigate": job_trigate_both, "pin": job_pin}
+MID_SHAPE = (64, 40, 28)
+MID_POINTS = {0: [0.0, 0.05], 1: [0.0]}    # Vd index -> Vg values, from equilibrium
+
+
+def job_trigate_mid_branch(vd_index):
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    dev = W.trigate3d(tb.Device3D, *MID_SHAPE)
+    ora = _oracle(dev)
+    idx = sample_nodes(ora.N, N_SAMPLE_3D, 642816)
+    t = time.time()
+    ora.solve_equilibrium()
+    _log(f"trigate-mid equilibrium {time.time() - t:.1f} s ({ora.eq_iters} steps)")
+    psi_eq = ora.psi.ravel()[idx].copy()
+    vd = W.TRIGATE_VD[vd_index]
+    out = []
+    for vg in MID_POINTS[vd_index]:
+        t = time.time()
+        ora.solve_bias(W.trigate_bias(vd, vg), tol=TOL)
+        assert ora.last_converged, (vd, vg)
+        out.append(dict(vd=vd, vg=vg, I_drain=ora.terminal_current("drain"),
+                        I_source=ora.terminal_current("source"),
+                        I_body=ora.terminal_current("body"),
+                        fields=np.stack(_fields(ora, idx)), iters=ora.newton_iters))
+        _log(f"trigate-mid Vd={vd} Vg={vg}: {ora.newton_iters} steps, {time.time() - t:.1f} s, "
+             f"Id={out[-1]['I_drain']:.9e}")
+    return dict(idx=idx, psi_eq=psi_eq, points=out)
+
+
+def job_trigate_mid():
+    """The tri-gate at 64 x 40 x 28 (71,680 nodes; a SuperLU step takes
+    minutes here): equilibrium, then the first points of each Vd branch."""
+    with mp.get_context("spawn").Pool(2) as pool:
+        a, b = pool.map(job_trigate_mid_branch, [0, 1])
+    assert np.array_equal(a["idx"], b["idx"])
+    pts = a["points"] + b["points"]
+    np.savez_compressed(
+        os.path.join(HERE, "trigate_mid.npz"), shape=np.array(MID_SHAPE), tol=TOL,
+        idx=a["idx"], psi_eq=a["psi_eq"], vd=np.array([q["vd"] for q in pts]),
+        vg=np.array([q["vg"] for q in pts]),
+        I_drain=np.array([q["I_drain"] for q in pts]),
+        I_source=np.array([q["I_source"] for q in pts]),
+        I_body=np.array([q["I_body"] for q in pts]),
+        fields=np.stack([q["fields"] for q in pts]), iters=np.array([q["iters"] for q in pts]))
+
+
+JOBS = {"mosfets": job_mosfets, "trigate": job_trigate_both, "pin": job_pin,
+        "trigate_mid": job_trigate_mid}
 
 
 if __name__ == "__main__":
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
-    names = [a for a in sys.argv[1:] if a in JOBS] or list(JOBS)
+    names = [a for a in sys.argv[1:] if a in JOBS] or [j for j in JOBS if j != "trigate_mid"]
     for name in names:
         JOBS[name]()
