@@ -18,24 +18,25 @@ committed as small .npz files:
   and largest meshes, the extreme body and source/drain dopings, the
   shortest gate and the highest bias; each from equilibrium through the
   same 4-step ramp (tcad_b200.workloads.ramp) as the batched GPU solve,
-  Newton steps solved by SuperLU.
+  Newton steps solved by SuperLU;
+* ``trigate_mid.npz`` -- the tri-gate at 64 x 40 x 28 (71,680 nodes), the
+  down-scaled size of the headline sweep: equilibrium, then Vg = 0 and
+  0.05 V at Vd = 0.05 V and Vg = 0 at Vd = 0.7 V, each branch from
+  equilibrium -- three points, not a sweep: a coupled Newton step took
+  ~12 minutes here (equilibrium 5 min; the three points 1.0, 1.2 and 2.6 h
+  with two branches in parallel).
 
-The 3D meshes are the largest whose sweeps the oracle's direct solves finish
+The sweep meshes are the largest whose sweeps the oracle's direct solves finish
 in minutes per point on one host core: a SuperLU factorisation of the coupled
 3D system grows from 0.5 s at 3,840 nodes to about a minute at 30k and
-several minutes (9 GB of factors) at the 71,680-node 64 x 40 x 28 mesh,
-where a 42-point sweep of ~6 Newton steps per point would take most of a day.
+several minutes at the 71,680-node 64 x 40 x 28 mesh,
+where a 42-point sweep would take days.
 
 Every converged state is solved to the update test 1e-12 (a stock
 NewtonOptions value, as for the reference-run sweep fixtures: at 1e-8 the
 update test saturates at the 1e-10 density floor).  Each fixture holds the
 terminal currents and (psi, n, p) at a seeded sample of nodes (the whole
 fields would be several MB).
-
-* ``trigate_mid.npz`` -- the tri-gate at 64 x 40 x 28 (71,680 nodes), the
-  down-scaled size of the headline sweep: equilibrium, then Vg = 0 and
-  0.05 V at Vd = 0.05 V and Vg = 0 at Vd = 0.7 V, each branch from
-  equilibrium (a few points: each SuperLU step takes minutes at this size).
 
 Usage:  python tests/golden/make_oracle_sweeps.py [mosfets] [trigate] [pin] [trigate_mid]
 """

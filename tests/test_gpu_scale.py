@@ -171,3 +171,34 @@ def test_pin_downscaled_sweep_matches_oracle():
         st = [t.ravel()[idx] for t in (dev.psi, dev.n, dev.p)]
         _check_fields(dev.VT, st, g["fields"][k], V)
     _check_currents(I, g["I_anode"], noise)
+
+
+def test_trigate_mid_points_match_oracle():
+    """The tri-gate at 64 x 40 x 28 (71,680 nodes), the down-scaled size of
+    the headline sweep (tests/golden/trigate_mid.npz, the oracle's exact
+    Newton, tests/golden/make_oracle_sweeps.py): equilibrium psi within
+    1e-9 V; then each Vd branch from equilibrium through its points with the
+    default options: drain, source and body currents within 1e-6 (on 1e-9 x
+    the largest terminal current, or ten times the rounding-level spread),
+    psi within 1e-9 V and the quasi-Fermi levels within 1e-8 V at the
+    sampled nodes."""
+    import tcad_b200 as tb
+    from tcad_b200 import workloads as W
+    g = fx.load("trigate_mid")
+    shape = tuple(int(v) for v in g["shape"])
+    idx = g["idx"]
+    top = max(np.abs(g["I_" + c]).max() for c in ("drain", "source", "body"))
+    for vd in sorted(set(float(v) for v in g["vd"])):
+        dev = W.trigate3d(tb.Device3D, *shape)
+        dev.solve_equilibrium()
+        assert np.abs(dev.psi.ravel()[idx] - g["psi_eq"]).max() * dev.VT < 1e-9
+        for k in np.flatnonzero(np.asarray(g["vd"]) == vd):
+            vg = float(g["vg"][k])
+            dev.solve_bias(W.trigate_bias(vd, vg))
+            assert dev.last_converged, (vd, vg)
+            for c in ("drain", "source", "body"):
+                I, ref = dev.terminal_current(c), float(g["I_" + c][k])
+                tol = fx.current_tol(ref, fx.current_noise(dev, c), floor=1e-9 * top)
+                assert abs(I - ref) <= tol, (vd, vg, c, I, ref)
+            st = [t.ravel()[idx] for t in (dev.psi, dev.n, dev.p)]
+            _check_fields(dev.VT, st, g["fields"][k], (vd, vg))
